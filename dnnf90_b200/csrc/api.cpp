@@ -1,0 +1,1162 @@
+// api.cpp - the C ABI: handle registries and the entry points of dnnf90.h
+// and dnnf90_b200.h.
+//
+// The registry model is the reference's (lib/c_api_module.f90:38-62): 64
+// slots per kind, handles are slot numbers > 0, a freed network slot
+// advances a generation counter and every dependent object built for an
+// earlier occupant is refused (-1).  Unlike the reference, no error stops
+// the process: every failure is a negative return code.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/dnnf90.h"
+#include "../../include/dnnf90_b200.h"
+#include "engine.hpp"
+#include "gemm_tc.hpp"
+
+using namespace dnnf90;
+
+namespace {
+
+constexpr int MAXH = 64;
+constexpr int QCAP = 8192;  // grad_point queue length before a flush
+
+struct NetH {
+  bool used = false;
+  TableSet ts;
+  int nlayer = 0;
+  std::vector<int> dims;
+  std::vector<double> w;  // flat layer layout
+  uint64_t wver = 1;      // bumped on every host-side weight change
+  int prec = PREC_F64;
+  bool dt_ok = false;
+  DevTables dt;
+  DevNet dn;
+};
+
+struct WorkH {
+  bool used = false;
+  int nid = 0, gen = 0;
+  Planes p;
+  cudaStream_t st = nullptr;
+  int chunk = 0;
+  // planes kept by a keep=1 forward
+  bool kept = false;
+  const double *kept_x = nullptr;
+  int kept_n = 0;
+  uint64_t kept_ver = 0;
+  // grad_point queue
+  std::vector<double> qx, qs;
+  int qn = 0, qgid = 0;
+  double *dX = nullptr, *dS = nullptr;
+  size_t dcap = 0;
+};
+
+struct GradH {
+  bool used = false;
+  int nid = 0, gen = 0;
+  double *d = nullptr, *m = nullptr, *v = nullptr;
+  int nw = 0;
+};
+
+struct TabH {
+  bool used = false;
+  TableSet ts;
+};
+
+struct RuleH {
+  bool used = false;
+  SeedRuleHost r;
+  bool up = false;
+  DevRule d;
+};
+
+std::recursive_mutex g_mu;
+TabH g_tab[MAXH + 1];
+NetH g_net[MAXH + 1];
+int g_gen[MAXH + 1];
+WorkH g_wrk[MAXH + 1];
+WorkH g_twk[MAXH + 1];
+GradH g_grd[MAXH + 1];
+RuleH g_rule[MAXH + 1];
+TableSet g_cur;
+bool g_cur_ready = false;
+
+template <typename T>
+int free_slot(T *reg) {
+  for (int i = 1; i <= MAXH; ++i)
+    if (!reg[i].used) return i;
+  return -1;
+}
+
+bool bad_net(int nid) { return nid < 1 || nid > MAXH || !g_net[nid].used; }
+
+int ck(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return RC_OK;
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? RC_NOMEM : RC_DEVICE;
+}
+
+int weight_count(const std::vector<int> &dims) {
+  int n = 0;
+  for (size_t l = 1; l < dims.size(); ++l) n += dims[l] * (dims[l - 1] + 1);
+  return n;
+}
+
+// net_init contract checks (lib/net_module.f90:109-136)
+int init_net(NetH &n, const TableSet &ts, int nlayer, const int *dims) {
+  if (nlayer < 2) return RC_BAD_ARG;
+  for (int l = 0; l < nlayer; ++l)
+    if (dims[l] < 1) return RC_BAD_ARG;
+  if (dims[0] != ts.d0) {
+    set_error("input width does not match the table set d0");
+    return RC_BAD_ARG;
+  }
+  n = NetH();
+  n.used = true;
+  n.ts = ts;
+  n.nlayer = nlayer;
+  n.dims.assign(dims, dims + nlayer);
+  n.w.assign(weight_count(n.dims), 0.0);
+  return RC_OK;
+}
+
+size_t layer_off(const NetH &n, int l) {  // 1-based l in 2..nlayer
+  size_t o = 0;
+  for (int ll = 2; ll < l; ++ll) o += (size_t)n.dims[ll - 1] * (n.dims[ll - 2] + 1);
+  return o;
+}
+
+// device copies of the network's tables and weights, refreshed when stale
+int net_device(NetH &n, cudaStream_t st) {
+  int rc = device_ready();
+  if (rc) return rc;
+  if (n.ts.iact > 2) {
+    set_error("the Bessel activations are not on the device path");
+    return RC_UNSUPPORTED;
+  }
+  if (!n.dt_ok) {
+    if ((rc = upload_tables(n.ts, n.dt))) return rc;
+    n.dt_ok = true;
+  }
+  if (n.dn.uploaded != n.wver) {
+    DevNet &d = n.dn;
+    if (!d.w64) {
+      d.nlayer = n.nlayer;
+      d.dims = n.dims;
+      d.nw = (int)n.w.size();
+      d.woff.assign(n.nlayer, 0);
+      for (int l = 2; l <= n.nlayer; ++l) d.woff[l - 1] = layer_off(n, l);
+      if ((rc = ck(cudaMalloc(&d.w64, n.w.size() * sizeof(double)), "cudaMalloc"))) return rc;
+      if ((rc = ck(cudaMalloc(&d.w32, n.w.size() * sizeof(float)), "cudaMalloc"))) return rc;
+    }
+    if ((rc = ck(cudaMemcpyAsync(d.w64, n.w.data(), n.w.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, st), "weights H2D")))
+      return rc;
+    if ((rc = weights_to_f32(d.w64, d.w32, n.w.size(), st))) return rc;
+    if ((rc = gemm_tc_prepare(&d, st))) return rc;
+    d.uploaded = n.wver;
+  }
+  return RC_OK;
+}
+
+int work_stream(WorkH &w) {
+  if (!w.st) {
+    int rc = ck(cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking), "stream");
+    if (rc) return rc;
+  }
+  return RC_OK;
+}
+
+// planes for up to want points (bounded by a device memory budget)
+int work_planes(WorkH &w, NetH &n, int want, bool exact) {
+  const size_t rsz = n.prec == PREC_F64 ? 8 : 4;
+  size_t per = 0;
+  int nmax = 0;
+  for (int l = 1; l < n.nlayer; ++l) nmax = std::max(nmax, n.dims[l]);
+  for (int l = 2; l < n.nlayer; ++l) per += 2 * (size_t)n.ts.na * n.dims[l - 1] * rsz;
+  per += 3 * (size_t)n.ts.na * nmax * rsz;
+  per += 2 * (size_t)n.ts.na * n.dims[n.nlayer - 1] * 8 + n.ts.d0 * 8 + 1024;
+  size_t freeb = 0, totb = 0;
+  cudaMemGetInfo(&freeb, &totb);
+  size_t budget = std::min<size_t>((size_t)48 << 30, freeb / 2);
+  if (w.p.base) budget += w.p.bytes;
+  int cap = (int)std::max<size_t>(1, budget / per);
+  if (w.chunk > 0) cap = std::min(cap, w.chunk);
+  int need = std::min(want, cap);
+  if (exact && want > cap) {
+    set_error("the kept forward does not fit the device memory budget");
+    return RC_NOMEM;
+  }
+  if (w.p.base && w.p.prec == n.prec && w.p.cap_pts >= need) return RC_OK;
+  w.kept = false;
+  return ensure_planes(n.dt, n.dn, n.prec, std::max(need, 1), w.p);
+}
+
+int grad_alloc(GradH &g) {
+  if (g.d) return RC_OK;
+  int rc = device_ready();
+  if (rc) return rc;
+  if ((rc = ck(cudaMalloc(&g.d, sizeof(double) * std::max(1, g.nw)), "cudaMalloc"))) return rc;
+  return ck(cudaMemset(g.d, 0, sizeof(double) * std::max(1, g.nw)), "cudaMemset");
+}
+
+int rule_device(RuleH &r, const TableSet &ts) {
+  for (int s : r.r.ind)
+    if (s < 0 || s >= ts.na) {
+      set_error("seed rule names a slot the table set does not carry");
+      return RC_BAD_ARG;
+    }
+  if (!r.up) {
+    int rc = upload_rule(r.r, r.d);
+    if (rc) return rc;
+    r.up = true;
+  }
+  return RC_OK;
+}
+
+// Run the queued grad_point points of one training work space.
+int flush_queue(int tid) {
+  WorkH &w = g_twk[tid];
+  if (!w.qn) return RC_OK;
+  const int nid = w.nid, gid = w.qgid, np = w.qn;
+  w.qn = 0;
+  if (bad_net(nid) || g_gen[nid] != w.gen) return RC_OK;  // net gone: points dropped
+  if (gid < 1 || gid > MAXH || !g_grd[gid].used) return RC_OK;
+  NetH &n = g_net[nid];
+  GradH &g = g_grd[gid];
+  int rc;
+  if ((rc = work_stream(w))) return rc;
+  if ((rc = net_device(n, w.st))) return rc;
+  if ((rc = grad_alloc(g))) return rc;
+  const int nout = n.dims[n.nlayer - 1], na = n.ts.na, d0 = n.ts.d0;
+  size_t need = (size_t)np * (d0 + (size_t)nout * na);
+  if (w.dcap < need) {
+    if (w.dX) cudaFree(w.dX);
+    w.dX = nullptr;
+    w.dcap = 0;
+    if ((rc = ck(cudaMalloc(&w.dX, need * sizeof(double)), "cudaMalloc"))) return rc;
+    w.dcap = need;
+  }
+  w.dS = w.dX + (size_t)np * d0;
+  std::vector<double> sm((size_t)np * nout * na, 0.0);
+  for (int p = 0; p < np; ++p)
+    std::memcpy(&sm[(size_t)p * nout * na], &w.qs[(size_t)p * na], sizeof(double) * na);
+  if ((rc = ck(cudaMemcpyAsync(w.dX, w.qx.data(), sizeof(double) * np * d0,
+                               cudaMemcpyHostToDevice, w.st), "H2D")))
+    return rc;
+  if ((rc = ck(cudaMemcpyAsync(w.dS, sm.data(), sizeof(double) * sm.size(),
+                               cudaMemcpyHostToDevice, w.st), "H2D")))
+    return rc;
+  if ((rc = work_planes(w, n, np, false))) return rc;
+  DevRule given;
+  given.kind = SEED_GIVEN;
+  BatchArgs a;
+  a.npts = np; a.X = w.dX; a.seeds = w.dS; a.grad = g.d; a.train = true; a.prec = n.prec;
+  if ((rc = run_batch(n.dt, n.dn, given, w.p, a, w.st))) return rc;
+  return ck(cudaStreamSynchronize(w.st), "grad_point batch");
+}
+
+int flush_for_grad(int gid) {
+  int rc = RC_OK;
+  for (int t = 1; t <= MAXH; ++t)
+    if (g_twk[t].used && g_twk[t].qn && g_twk[t].qgid == gid) {
+      int r = flush_queue(t);
+      if (r && !rc) rc = r;
+    }
+  return rc;
+}
+
+int flush_for_net(int nid) {
+  int rc = RC_OK;
+  for (int t = 1; t <= MAXH; ++t)
+    if (g_twk[t].used && g_twk[t].qn && g_twk[t].nid == nid) {
+      int r = flush_queue(t);
+      if (r && !rc) rc = r;
+    }
+  return rc;
+}
+
+void free_work(WorkH &w) {
+  w.p.release();
+  if (w.st) cudaStreamDestroy(w.st);
+  if (w.dX) cudaFree(w.dX);
+  w = WorkH();
+}
+
+bool table_args_ok(int d0, int k, int nseed, const int *seeds) {
+  if (d0 < 1 || k < 1 || k > 15 || nseed < 0) return false;
+  if (seeds)
+    for (int i = 0; i < d0 * nseed; ++i)
+      if (seeds[i] < 0 || seeds[i] > k) return false;
+  return true;
+}
+
+// ---- nn_weight.dat (lib/net_module.f90:146-243) ----
+struct Reader {
+  std::vector<std::string> lines;
+  size_t ln = 0;
+  bool ok = true;
+  // list-directed read of n values starting at a fresh record; the rest of
+  // the last record is discarded
+  std::vector<std::string> read(size_t n) {
+    std::vector<std::string> out;
+    while (out.size() < n) {
+      if (ln >= lines.size()) { ok = false; return out; }
+      std::istringstream is(lines[ln++]);
+      std::string tok;
+      while (out.size() < n && is >> tok) {
+        if (tok[0] == '/' || tok[0] == '!') break;
+        out.push_back(tok);
+      }
+    }
+    return out;
+  }
+  void skip() {
+    if (ln < lines.size()) ln++;
+    else ok = false;
+  }
+};
+
+double to_d(const std::string &s, bool &ok) {
+  std::string t = s;
+  for (char &c : t)
+    if (c == 'd' || c == 'D') c = 'e';
+  char *end = nullptr;
+  double v = std::strtod(t.c_str(), &end);
+  if (end == t.c_str()) ok = false;
+  return v;
+}
+
+int load_net(const char *fname, const TableSet &ts, int &out) {
+  std::ifstream f(fname);
+  if (!f) return RC_BAD_FILE;
+  Reader r;
+  std::string line;
+  while (std::getline(f, line)) r.lines.push_back(line);
+  r.skip();  // epoch
+  auto h = r.read(2);
+  bool ok = r.ok;
+  if (!ok || h.size() < 2) return RC_BAD_FILE;
+  int ifunc = (int)to_d(h[1], ok);
+  if (!ok || ifunc < 0 || ifunc > 4) return RC_BAD_FILE;
+  auto ao = r.read(2);
+  if (!r.ok || ao.size() < 2 || (int)to_d(ao[1], ok) != 0) {
+    set_error("the weight file has a nonlinear output layer");
+    return RC_BAD_FILE;
+  }
+  auto nl = r.read(1);
+  if (!r.ok) return RC_BAD_FILE;
+  int nlayer = (int)to_d(nl[0], ok);
+  if (!ok || nlayer < 2 || nlayer > 64) return RC_BAD_FILE;
+  std::vector<int> dims(nlayer);
+  for (int i = 0; i < nlayer; ++i) {
+    auto v = r.read(1);
+    if (!r.ok) return RC_BAD_FILE;
+    dims[i] = (int)to_d(v[0], ok);
+  }
+  if (!ok) return RC_BAD_FILE;
+  if (ts.iact != ifunc) {
+    set_error("the weight file names another activation than the table set");
+    return RC_BAD_FILE;
+  }
+  int id = free_slot(g_net);
+  if (id < 0) return RC_BAD_ARG;
+  NetH tmp;
+  int rc = init_net(tmp, ts, nlayer, dims.data());
+  if (rc) return rc;
+  size_t p = 0;
+  for (int l = 2; l <= nlayer; ++l) {
+    r.skip();  // "#l=" header
+    for (int j = 0; j < dims[l - 1]; ++j) {
+      auto v = r.read(dims[l - 2] + 1);
+      if (!r.ok) return RC_BAD_FILE;
+      for (auto &s : v) tmp.w[p++] = to_d(s, ok);
+    }
+  }
+  if (!ok) return RC_BAD_FILE;
+  g_net[id] = std::move(tmp);
+  out = id;
+  return RC_OK;
+}
+
+int run_eval(int nid, WorkH &w, int npts, const double *x, double *tm,
+             bool host) {
+  NetH &n = g_net[nid];
+  int rc;
+  if ((rc = work_stream(w))) return rc;
+  if ((rc = net_device(n, w.st))) return rc;
+  const int na = n.ts.na, d0 = n.ts.d0, nout = n.dims[n.nlayer - 1];
+  if ((rc = work_planes(w, n, npts, false))) return rc;
+  DevRule none;
+  const int cap = w.p.cap_pts;
+  // host batches are staged through the plane buffers chunk by chunk
+  for (int c0 = 0; c0 < npts; c0 += (host ? cap : npts)) {
+    int np = host ? std::min(cap, npts - c0) : npts;
+    BatchArgs a;
+    a.npts = np;
+    a.prec = n.prec;
+    if (host) {
+      if ((rc = ck(cudaMemcpyAsync(w.p.X, x + (size_t)c0 * d0, sizeof(double) * np * d0,
+                                   cudaMemcpyHostToDevice, w.st), "H2D")))
+        return rc;
+      a.X = w.p.X;
+      a.out = w.p.out;
+    } else {
+      a.X = x;
+      a.out = tm;
+    }
+    if ((rc = run_batch(n.dt, n.dn, none, w.p, a, w.st))) return rc;
+    if (host) {
+      if ((rc = ck(cudaMemcpyAsync(tm + (size_t)c0 * na * nout, w.p.out,
+                                   sizeof(double) * np * na * nout,
+                                   cudaMemcpyDeviceToHost, w.st), "D2H")))
+        return rc;
+    }
+  }
+  if (host) return ck(cudaStreamSynchronize(w.st), "eval");
+  return RC_OK;
+}
+
+// checks shared by the training entries: net, work space, accumulator
+int check_train(int nid, int tid, int gid, bool need_gid) {
+  if (bad_net(nid)) return RC_BAD_ARG;
+  if (tid < 1 || tid > MAXH || !g_twk[tid].used) return RC_BAD_ARG;
+  if (g_twk[tid].nid != nid || g_twk[tid].gen != g_gen[nid]) return RC_BAD_ARG;
+  if (need_gid) {
+    if (gid < 1 || gid > MAXH || !g_grd[gid].used) return RC_BAD_ARG;
+    if (g_grd[gid].nid != nid || g_grd[gid].gen != g_gen[nid]) return RC_BAD_ARG;
+  }
+  return RC_OK;
+}
+
+// [npts][na][nout] -> [npts][nout][na] / output 1 only
+void relayout(const double *src, double *dst, int npts, int na, int nout,
+              bool first_only) {
+  for (int p = 0; p < npts; ++p)
+    for (int ia = 0; ia < na; ++ia) {
+      const double *s = src + ((size_t)p * na + ia) * nout;
+      if (first_only) dst[(size_t)p * na + ia] = s[0];
+      else
+        for (int o = 0; o < nout; ++o) dst[((size_t)p * nout + o) * na + ia] = s[o];
+    }
+}
+
+// one training batch from host buffers (grad_batch, grad_rule_batch,
+// jrow_batch).  kind SEED_GIVEN uses seed[npts][na] (output 1).
+int host_train(int nid, int tid, int npts, const double *x, int kind,
+               RuleH *rule, const double *seed, double *grad_dev, double *rows,
+               double *loss, double *t, double *resid) {
+  NetH &n = g_net[nid];
+  WorkH &w = g_twk[tid];
+  int rc;
+  if ((rc = flush_queue(tid))) return rc;
+  if ((rc = work_stream(w))) return rc;
+  if ((rc = net_device(n, w.st))) return rc;
+  if (rule && (rc = rule_device(*rule, n.ts))) return rc;
+  if ((rc = work_planes(w, n, npts, false))) return rc;
+  const int na = n.ts.na, d0 = n.ts.d0, nout = n.dims[n.nlayer - 1];
+  const int cap = w.p.cap_pts;
+  const int nw = (int)n.w.size();
+  double *dseed = nullptr, *drows = nullptr, *dloss = nullptr;
+  if (kind == SEED_GIVEN) {
+    if ((rc = ck(cudaMalloc(&dseed, sizeof(double) * (size_t)cap * nout * na), "cudaMalloc"))) return rc;
+  }
+  if (rows) {
+    if ((rc = ck(cudaMalloc(&drows, sizeof(double) * (size_t)cap * nw), "cudaMalloc"))) {
+      if (dseed) cudaFree(dseed);
+      return rc;
+    }
+  }
+  if ((rc = ck(cudaMalloc(&dloss, sizeof(double)), "cudaMalloc"))) {
+    if (dseed) cudaFree(dseed);
+    if (drows) cudaFree(drows);
+    return rc;
+  }
+  cudaMemsetAsync(dloss, 0, sizeof(double), w.st);
+  std::vector<double> sm, tbuf;
+  for (int c0 = 0; c0 < npts && !rc; c0 += cap) {
+    const int np = std::min(cap, npts - c0);
+    rc = ck(cudaMemcpyAsync(w.p.X, x + (size_t)c0 * d0, sizeof(double) * np * d0,
+                            cudaMemcpyHostToDevice, w.st), "H2D");
+    if (rc) break;
+    DevRule given;
+    given.kind = SEED_GIVEN;
+    if (kind == SEED_GIVEN) {
+      sm.assign((size_t)np * nout * na, 0.0);
+      for (int p = 0; p < np; ++p)
+        std::memcpy(&sm[(size_t)p * nout * na], seed + (size_t)(c0 + p) * na, sizeof(double) * na);
+      rc = ck(cudaMemcpyAsync(dseed, sm.data(), sizeof(double) * sm.size(),
+                              cudaMemcpyHostToDevice, w.st), "H2D");
+      if (rc) break;
+    }
+    BatchArgs a;
+    a.npts = np; a.X = w.p.X; a.out = (t || resid) ? w.p.out : nullptr;
+    a.seeds = dseed; a.grad = rows ? nullptr : grad_dev; a.rows = drows;
+    a.loss = dloss; a.train = true; a.prec = n.prec;
+    rc = run_batch(n.dt, n.dn, rule ? rule->d : given, w.p, a, w.st);
+    if (rc) break;
+    if (rows) {
+      rc = ck(cudaMemcpyAsync(rows + (size_t)c0 * nw, drows, sizeof(double) * (size_t)np * nw,
+                              cudaMemcpyDeviceToHost, w.st), "D2H");
+      if (rc) break;
+    }
+    if (t || resid) {
+      tbuf.resize((size_t)np * na * nout);
+      rc = ck(cudaMemcpyAsync(tbuf.data(), w.p.out, sizeof(double) * tbuf.size(),
+                              cudaMemcpyDeviceToHost, w.st), "D2H");
+      if (!rc) rc = ck(cudaStreamSynchronize(w.st), "sync");
+      if (rc) break;
+      std::vector<double> t1((size_t)np * na);
+      relayout(tbuf.data(), t1.data(), np, na, nout, true);
+      if (t) std::memcpy(t + (size_t)c0 * na, t1.data(), sizeof(double) * t1.size());
+      if (resid && rule) {
+        const SeedRuleHost &r = rule->r;
+        for (int p = 0; p < np; ++p) {
+          const double *tp = &t1[(size_t)p * na];
+          double R = 0.0;
+          for (size_t k = 0; k < r.coeff.size(); ++k)
+            R = r.nonlin[k] ? R + r.coeff[k] * tp[0] * tp[r.ind[k]] : R + r.coeff[k] * tp[r.ind[k]];
+          resid[c0 + p] = R;
+        }
+      }
+    }
+  }
+  double lv = 0.0;
+  if (!rc) rc = ck(cudaMemcpyAsync(&lv, dloss, sizeof(double), cudaMemcpyDeviceToHost, w.st), "D2H");
+  if (!rc) rc = ck(cudaStreamSynchronize(w.st), "train batch");
+  if (loss) *loss = lv;
+  if (dseed) cudaFree(dseed);
+  if (drows) cudaFree(drows);
+  cudaFree(dloss);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ------------------------------------------------------------- tables
+int dnnf90_tables_init_dense(int d0, int k) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!table_args_ok(d0, k, 0, nullptr)) return RC_BAD_ARG;
+  TableSet ts;
+  if (!build_tables(d0, k, 0, nullptr, ts).empty()) return RC_BAD_ARG;
+  g_cur = std::move(ts);
+  g_cur_ready = true;
+  return RC_OK;
+}
+
+int dnnf90_tables_init_closure(int d0, int k, int nseed, const int *seeds) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!table_args_ok(d0, k, nseed, seeds)) return RC_BAD_ARG;
+  TableSet ts;
+  std::string e = build_tables(d0, k, nseed, seeds, ts);
+  if (!e.empty()) {
+    set_error(e);
+    return RC_BAD_ARG;
+  }
+  g_cur = std::move(ts);
+  g_cur_ready = true;
+  return RC_OK;
+}
+
+int dnnf90_nderiv(void) { return g_cur_ready ? g_cur.na : 0; }
+
+int dnnf90_alpha(int ia, int *a) {
+  if (!g_cur_ready || ia < 1 || ia > g_cur.na) return RC_BAD_ARG;
+  for (int i = 0; i < g_cur.d0; ++i) a[i] = g_cur.alpha[(size_t)(ia - 1) * g_cur.d0 + i];
+  return RC_OK;
+}
+
+int dnnf90_tabset_dense(int d0, int k) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!table_args_ok(d0, k, 0, nullptr)) return RC_BAD_ARG;
+  int id = free_slot(g_tab);
+  if (id < 0) return RC_BAD_ARG;
+  TableSet ts;
+  if (!build_tables(d0, k, 0, nullptr, ts).empty()) return RC_BAD_ARG;
+  g_cur = ts;  // the reference leaves the module tables holding the last set
+  g_cur_ready = true;
+  g_tab[id].ts = std::move(ts);
+  g_tab[id].used = true;
+  return id;
+}
+
+int dnnf90_tabset_closure(int d0, int k, int nseed, const int *seeds) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!table_args_ok(d0, k, nseed, seeds)) return RC_BAD_ARG;
+  int id = free_slot(g_tab);
+  if (id < 0) return RC_BAD_ARG;
+  TableSet ts;
+  std::string e = build_tables(d0, k, nseed, seeds, ts);
+  if (!e.empty()) {
+    set_error(e);
+    return RC_BAD_ARG;
+  }
+  g_cur = ts;
+  g_cur_ready = true;
+  g_tab[id].ts = std::move(ts);
+  g_tab[id].used = true;
+  return id;
+}
+
+int dnnf90_tabset_nderiv(int tid) {
+  if (tid < 1 || tid > MAXH || !g_tab[tid].used) return RC_BAD_ARG;
+  return g_tab[tid].ts.na;
+}
+
+int dnnf90_tabset_activation(int tid, int iact) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (tid < 1 || tid > MAXH || !g_tab[tid].used) return RC_BAD_ARG;
+  if (iact < 0 || iact > 4) return RC_BAD_FILE;
+  g_tab[tid].ts.iact = iact;
+  return RC_OK;
+}
+
+// ------------------------------------------------------------- networks
+int dnnf90_net_create(int nlayer, const int *dims) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!g_cur_ready || nlayer < 2 || !dims) return RC_BAD_ARG;
+  int id = free_slot(g_net);
+  if (id < 0) return RC_BAD_ARG;
+  TableSet ts = g_cur;
+  ts.iact = 0;
+  NetH n;
+  int rc = init_net(n, ts, nlayer, dims);
+  if (rc) return rc;
+  g_net[id] = std::move(n);
+  return id;
+}
+
+int dnnf90_net_create_ts(int tid, int nlayer, const int *dims) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (nlayer < 2 || !dims) return RC_BAD_ARG;
+  for (int l = 0; l < nlayer; ++l)
+    if (dims[l] < 1) return RC_BAD_ARG;
+  if (tid < 1 || tid > MAXH || !g_tab[tid].used) return RC_BAD_ARG;
+  int id = free_slot(g_net);
+  if (id < 0) return RC_BAD_ARG;
+  NetH n;
+  int rc = init_net(n, g_tab[tid].ts, nlayer, dims);
+  if (rc) return rc;
+  g_net[id] = std::move(n);
+  return id;
+}
+
+int dnnf90_net_load(const char *filename) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!filename) return RC_BAD_ARG;
+  std::ifstream f(filename);
+  if (!f) return RC_BAD_FILE;
+  if (!g_cur_ready) return RC_BAD_ARG;
+  if (free_slot(g_net) < 0) return RC_BAD_ARG;
+  TableSet ts = g_cur;
+  ts.iact = 0;
+  int id = 0;
+  int rc = load_net(filename, ts, id);
+  return rc ? rc : id;
+}
+
+int dnnf90_net_load_ts(int tid, const char *filename) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (tid < 1 || tid > MAXH || !g_tab[tid].used || !filename) return RC_BAD_ARG;
+  std::ifstream f(filename);
+  if (!f) return RC_BAD_FILE;
+  if (free_slot(g_net) < 0) return RC_BAD_ARG;
+  int id = 0;
+  int rc = load_net(filename, g_tab[tid].ts, id);
+  return rc ? rc : id;
+}
+
+int dnnf90_net_set_layer(int nid, int l, const double *wrow) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid) || l < 2 || l > g_net[nid].nlayer || !wrow) return RC_BAD_ARG;
+  NetH &n = g_net[nid];
+  flush_for_net(nid);  // queued points were added under the old weights
+  size_t o = layer_off(n, l);
+  std::memcpy(&n.w[o], wrow, sizeof(double) * n.dims[l - 1] * (n.dims[l - 2] + 1));
+  n.wver++;
+  return RC_OK;
+}
+
+int dnnf90_net_free(int nid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid)) return RC_BAD_ARG;
+  NetH &n = g_net[nid];
+  n.dt.release();
+  n.dn.release();
+  n = NetH();
+  g_gen[nid]++;
+  return RC_OK;
+}
+
+// ------------------------------------------------------------- evaluation
+int dnnf90_work_create(int nid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid)) return RC_BAD_ARG;
+  int id = free_slot(g_wrk);
+  if (id < 0) return RC_BAD_ARG;
+  g_wrk[id] = WorkH();
+  g_wrk[id].used = true;
+  g_wrk[id].nid = nid;
+  g_wrk[id].gen = g_gen[nid];
+  return id;
+}
+
+int dnnf90_work_free(int wid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (wid < 1 || wid > MAXH || !g_wrk[wid].used) return RC_BAD_ARG;
+  free_work(g_wrk[wid]);
+  return RC_OK;
+}
+
+static int check_eval(int nid, int wid) {
+  if (bad_net(nid) || wid < 1 || wid > MAXH || !g_wrk[wid].used) return RC_BAD_ARG;
+  if (g_wrk[wid].nid != nid || g_wrk[wid].gen != g_gen[nid]) return RC_BAD_ARG;
+  return RC_OK;
+}
+
+int dnnf90_eval(int nid, int wid, const double *x, double *t) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_eval(nid, wid);
+  if (rc) return rc;
+  NetH &n = g_net[nid];
+  const int na = n.ts.na, nout = n.dims[n.nlayer - 1];
+  std::vector<double> tm((size_t)na * nout);
+  if ((rc = run_eval(nid, g_wrk[wid], 1, x, tm.data(), true))) return rc;
+  for (int ia = 0; ia < na; ++ia) t[ia] = tm[(size_t)ia * nout];
+  return RC_OK;
+}
+
+int dnnf90_eval_batch(int nid, int wid, int npts, const double *x, double *t) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_eval(nid, wid);
+  if (rc) return rc;
+  if (npts < 0 || (npts > 0 && (!x || !t))) return RC_BAD_ARG;
+  if (npts == 0) return RC_OK;
+  NetH &n = g_net[nid];
+  const int na = n.ts.na, nout = n.dims[n.nlayer - 1];
+  std::vector<double> tm((size_t)npts * na * nout);
+  if ((rc = run_eval(nid, g_wrk[wid], npts, x, tm.data(), true))) return rc;
+  relayout(tm.data(), t, npts, na, nout, true);
+  return RC_OK;
+}
+
+int dnnf90_eval_batch_multi(int nid, int wid, int npts, const double *x, double *tmo) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_eval(nid, wid);
+  if (rc) return rc;
+  if (npts < 0 || (npts > 0 && (!x || !tmo))) return RC_BAD_ARG;
+  if (npts == 0) return RC_OK;
+  NetH &n = g_net[nid];
+  const int na = n.ts.na, nout = n.dims[n.nlayer - 1];
+  std::vector<double> tm((size_t)npts * na * nout);
+  if ((rc = run_eval(nid, g_wrk[wid], npts, x, tm.data(), true))) return rc;
+  relayout(tm.data(), tmo, npts, na, nout, false);
+  return RC_OK;
+}
+
+// ------------------------------------------------------------- training
+int dnnf90_twork_create(int nid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid)) return RC_BAD_ARG;
+  int id = free_slot(g_twk);
+  if (id < 0) return RC_BAD_ARG;
+  g_twk[id] = WorkH();
+  g_twk[id].used = true;
+  g_twk[id].nid = nid;
+  g_twk[id].gen = g_gen[nid];
+  return id;
+}
+
+int dnnf90_twork_free(int tid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (tid < 1 || tid > MAXH || !g_twk[tid].used) return RC_BAD_ARG;
+  flush_queue(tid);
+  free_work(g_twk[tid]);
+  return RC_OK;
+}
+
+int dnnf90_twork_set_chunk(int tid, int npts) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (tid < 1 || tid > MAXH || !g_twk[tid].used || npts < 0) return RC_BAD_ARG;
+  g_twk[tid].chunk = npts;
+  return RC_OK;
+}
+
+int dnnf90_grad_create(int nid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid)) return RC_BAD_ARG;
+  int id = free_slot(g_grd);
+  if (id < 0) return RC_BAD_ARG;
+  g_grd[id] = GradH();
+  g_grd[id].used = true;
+  g_grd[id].nid = nid;
+  g_grd[id].gen = g_gen[nid];
+  g_grd[id].nw = (int)g_net[nid].w.size();
+  return id;
+}
+
+int dnnf90_grad_free(int gid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (gid < 1 || gid > MAXH || !g_grd[gid].used) return RC_BAD_ARG;
+  for (int t = 1; t <= MAXH; ++t)  // queued points of this accumulator die with it
+    if (g_twk[t].used && g_twk[t].qgid == gid) g_twk[t].qn = 0;
+  GradH &g = g_grd[gid];
+  if (g.d) cudaFree(g.d);
+  if (g.m) cudaFree(g.m);
+  if (g.v) cudaFree(g.v);
+  g = GradH();
+  return RC_OK;
+}
+
+int dnnf90_grad_zero(int gid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (gid < 1 || gid > MAXH || !g_grd[gid].used) return RC_BAD_ARG;
+  for (int t = 1; t <= MAXH; ++t)  // zeroing discards what was queued
+    if (g_twk[t].used && g_twk[t].qgid == gid) g_twk[t].qn = 0;
+  GradH &g = g_grd[gid];
+  if (g.d) return ck(cudaMemset(g.d, 0, sizeof(double) * std::max(1, g.nw)), "grad_zero");
+  return RC_OK;
+}
+
+int dnnf90_grad_point(int nid, int tid, const double *x, const double *seed, int gid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, gid, true);
+  if (rc) return rc;
+  if (!x || !seed) return RC_BAD_ARG;
+  if ((rc = device_ready())) return rc;
+  WorkH &w = g_twk[tid];
+  NetH &n = g_net[nid];
+  if (w.qn && w.qgid != gid)
+    if ((rc = flush_queue(tid))) return rc;
+  const int na = n.ts.na, d0 = n.ts.d0;
+  if (w.qn == 0) {
+    w.qx.resize((size_t)QCAP * d0);
+    w.qs.resize((size_t)QCAP * na);
+  }
+  w.qgid = gid;
+  std::memcpy(&w.qx[(size_t)w.qn * d0], x, sizeof(double) * d0);
+  std::memcpy(&w.qs[(size_t)w.qn * na], seed, sizeof(double) * na);
+  w.qn++;
+  if (w.qn == QCAP) return flush_queue(tid);
+  return RC_OK;
+}
+
+int dnnf90_adam_step(int nid, int gid, double eta, double beta1, double beta2,
+                     double eps, int nbatch, int istep) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid) || gid < 1 || gid > MAXH || !g_grd[gid].used) return RC_BAD_ARG;
+  if (g_grd[gid].nid != nid || g_grd[gid].gen != g_gen[nid]) return RC_BAD_ARG;
+  int rc = flush_for_grad(gid);
+  if (rc) return rc;
+  NetH &n = g_net[nid];
+  GradH &g = g_grd[gid];
+  if ((rc = net_device(n, nullptr))) return rc;
+  if ((rc = grad_alloc(g))) return rc;
+  if (!g.m) {
+    if ((rc = ck(cudaMalloc(&g.m, sizeof(double) * g.nw), "cudaMalloc"))) return rc;
+    if ((rc = ck(cudaMalloc(&g.v, sizeof(double) * g.nw), "cudaMalloc"))) return rc;
+    cudaMemset(g.m, 0, sizeof(double) * g.nw);
+    cudaMemset(g.v, 0, sizeof(double) * g.nw);
+  }
+  if ((rc = adam_device(n.dn.w64, g.d, g.m, g.v, g.nw, eta, beta1, beta2, eps, nbatch,
+                        istep, nullptr)))
+    return rc;
+  if ((rc = ck(cudaMemcpy(n.w.data(), n.dn.w64, sizeof(double) * n.w.size(),
+                          cudaMemcpyDeviceToHost), "weights D2H")))
+    return rc;
+  n.wver++;  // the device FP32 / split copies follow on the next use
+  return RC_OK;
+}
+
+// ------------------------------------------------------------- extensions
+int dnnf90_net_set_precision(int nid, int prec) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid) || (prec != PREC_F64 && prec != PREC_SPLIT)) return RC_BAD_ARG;
+  flush_for_net(nid);
+  g_net[nid].prec = prec;
+  return RC_OK;
+}
+
+int dnnf90_nweights(int nid) {
+  if (bad_net(nid)) return RC_BAD_ARG;
+  return (int)g_net[nid].w.size();
+}
+
+int dnnf90_net_get_layer(int nid, int l, double *wrow) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid) || l < 2 || l > g_net[nid].nlayer || !wrow) return RC_BAD_ARG;
+  NetH &n = g_net[nid];
+  std::memcpy(wrow, &n.w[layer_off(n, l)], sizeof(double) * n.dims[l - 1] * (n.dims[l - 2] + 1));
+  return RC_OK;
+}
+
+int dnnf90_net_save(int nid, const char *filename) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid) || !filename) return RC_BAD_ARG;
+  NetH &n = g_net[nid];
+  FILE *f = std::fopen(filename, "w");
+  if (!f) return RC_BAD_FILE;
+  std::fprintf(f, "0\nfunc %d\nActivation_out 0\n%d\n", n.ts.iact, n.nlayer);
+  for (int l = 0; l < n.nlayer; ++l) std::fprintf(f, "%d\n", n.dims[l]);
+  size_t p = 0;
+  for (int l = 2; l <= n.nlayer; ++l) {
+    std::fprintf(f, " #l= %d\n", l);
+    for (int j = 0; j < n.dims[l - 1]; ++j) {
+      for (int i = 0; i <= n.dims[l - 2]; ++i) std::fprintf(f, "%25.16E", n.w[p++]);
+      std::fprintf(f, "\n");
+    }
+  }
+  std::fclose(f);
+  return RC_OK;
+}
+
+int dnnf90_grad_batch(int nid, int tid, int npts, const double *x, const double *seed,
+                      int gid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, gid, true);
+  if (rc) return rc;
+  if (npts < 0 || (npts > 0 && (!x || !seed))) return RC_BAD_ARG;
+  if (npts == 0) return RC_OK;
+  if ((rc = device_ready()) || (rc = grad_alloc(g_grd[gid]))) return rc;
+  return host_train(nid, tid, npts, x, SEED_GIVEN, nullptr, seed, g_grd[gid].d, nullptr,
+                    nullptr, nullptr, nullptr);
+}
+
+int dnnf90_seed_rule_create(int kind, int nterm, const double *coeff, const int *slot,
+                            const int *nonlin, double fac) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (kind < SEED_HALFSQ || kind > SEED_JROW || nterm < 0) return RC_BAD_ARG;
+  if (kind != SEED_HALFSQ && (nterm < 1 || !coeff || !slot)) return RC_BAD_ARG;
+  int id = free_slot(g_rule);
+  if (id < 0) return RC_BAD_ARG;
+  RuleH r;
+  r.used = true;
+  r.r.kind = kind;
+  r.r.fac = fac;
+  for (int k = 0; k < nterm && kind != SEED_HALFSQ; ++k) {
+    if (slot[k] < 1) return RC_BAD_ARG;
+    r.r.coeff.push_back(coeff[k]);
+    r.r.ind.push_back(slot[k] - 1);
+    r.r.nonlin.push_back(nonlin ? (nonlin[k] ? 1 : 0) : 0);
+  }
+  g_rule[id] = std::move(r);
+  return id;
+}
+
+int dnnf90_seed_rule_free(int rid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (rid < 1 || rid > MAXH || !g_rule[rid].used) return RC_BAD_ARG;
+  g_rule[rid].d.release();
+  g_rule[rid] = RuleH();
+  return RC_OK;
+}
+
+static bool bad_rule(int rid) { return rid < 1 || rid > MAXH || !g_rule[rid].used; }
+
+int dnnf90_grad_rule_batch(int nid, int tid, int npts, const double *x, int rid, int gid,
+                           double *loss, double *t) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, gid, true);
+  if (rc) return rc;
+  if (bad_rule(rid) || g_rule[rid].r.kind == SEED_JROW) return RC_BAD_ARG;
+  if (npts < 0 || (npts > 0 && !x)) return RC_BAD_ARG;
+  if (loss) *loss = 0.0;
+  if (npts == 0) return RC_OK;
+  if ((rc = device_ready()) || (rc = grad_alloc(g_grd[gid]))) return rc;
+  return host_train(nid, tid, npts, x, g_rule[rid].r.kind, &g_rule[rid], nullptr,
+                    g_grd[gid].d, nullptr, loss, t, nullptr);
+}
+
+int dnnf90_jrow_batch(int nid, int tid, int npts, const double *x, int rid, double *rows,
+                      double *resid, double *t) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, 0, false);
+  if (rc) return rc;
+  if (bad_rule(rid) || g_rule[rid].r.kind != SEED_JROW) return RC_BAD_ARG;
+  if (npts < 0 || (npts > 0 && (!x || !rows))) return RC_BAD_ARG;
+  if (npts == 0) return RC_OK;
+  if ((rc = device_ready())) return rc;
+  return host_train(nid, tid, npts, x, SEED_JROW, &g_rule[rid], nullptr, nullptr, rows,
+                    nullptr, t, resid);
+}
+
+int dnnf90_grad_read(int gid, double *g) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (gid < 1 || gid > MAXH || !g_grd[gid].used || !g) return RC_BAD_ARG;
+  int rc = flush_for_grad(gid);
+  if (rc) return rc;
+  GradH &gr = g_grd[gid];
+  if (!gr.d) {
+    std::memset(g, 0, sizeof(double) * gr.nw);
+    return RC_OK;
+  }
+  return ck(cudaMemcpy(g, gr.d, sizeof(double) * gr.nw, cudaMemcpyDeviceToHost), "D2H");
+}
+
+int dnnf90_ngd_step(int nid, int nrow, const double *rows, const double *b, int nb,
+                    double mu, int prec, double *u) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid) || nrow < 1 || nb < 1 || !rows || !b || !u) return RC_BAD_ARG;
+  if (prec != PREC_F64 && prec != PREC_SPLIT) return RC_BAD_ARG;
+  int rc = device_ready();
+  if (rc) return rc;
+  const int nw = (int)g_net[nid].w.size();
+  double *dr = nullptr, *db = nullptr, *du = nullptr;
+  if ((rc = ck(cudaMalloc(&dr, sizeof(double) * (size_t)nrow * nw), "cudaMalloc"))) return rc;
+  if ((rc = ck(cudaMalloc(&db, sizeof(double) * nw * 2), "cudaMalloc"))) {
+    cudaFree(dr);
+    return rc;
+  }
+  du = db + nw;
+  rc = ck(cudaMemcpy(dr, rows, sizeof(double) * (size_t)nrow * nw, cudaMemcpyHostToDevice), "H2D");
+  if (!rc) rc = ck(cudaMemcpy(db, b, sizeof(double) * nw, cudaMemcpyHostToDevice), "H2D");
+  if (!rc) rc = ngd_device(dr, nrow, nw, db, nb, mu, du, prec, nullptr);
+  if (!rc) rc = ck(cudaMemcpy(u, du, sizeof(double) * nw, cudaMemcpyDeviceToHost), "D2H");
+  cudaFree(dr);
+  cudaFree(db);
+  return rc;
+}
+
+// ------------------------------------------------------------- device pointers
+int dnnf90_set_weights_dev(int nid, const double *w_dev, void *stream) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid) || !w_dev) return RC_BAD_ARG;
+  int rc = device_ready();
+  if (rc) return rc;
+  NetH &n = g_net[nid];
+  flush_for_net(nid);
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = ck(cudaMemcpyAsync(n.w.data(), w_dev, sizeof(double) * n.w.size(),
+                               cudaMemcpyDeviceToHost, st), "weights D2H")))
+    return rc;
+  if ((rc = ck(cudaStreamSynchronize(st), "sync"))) return rc;
+  n.wver++;
+  return net_device(n, st);
+}
+
+int dnnf90_forward_dev(int nid, int tid, int npts, const double *x_dev, double *tm_dev,
+                       int keep, void *stream) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, 0, false);
+  if (rc) return rc;
+  if (npts < 0 || (npts > 0 && !x_dev)) return RC_BAD_ARG;
+  if (npts == 0) return RC_OK;
+  NetH &n = g_net[nid];
+  WorkH &w = g_twk[tid];
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = net_device(n, st))) return rc;
+  if ((rc = work_planes(w, n, npts, keep != 0))) return rc;
+  if (keep) {
+    if ((rc = forward_keep(n.dt, n.dn, w.p, n.prec, npts, x_dev, tm_dev, st))) return rc;
+    w.kept = true;
+    w.kept_x = x_dev;
+    w.kept_n = npts;
+    w.kept_ver = n.wver;
+    return RC_OK;
+  }
+  w.kept = false;
+  DevRule none;
+  BatchArgs a;
+  a.npts = npts; a.X = x_dev; a.out = tm_dev; a.prec = n.prec;
+  return run_batch(n.dt, n.dn, none, w.p, a, st);
+}
+
+int dnnf90_backward_dev(int nid, int tid, int npts, const double *x_dev,
+                        const double *seedm_dev, double *grad_dev, void *stream) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, 0, false);
+  if (rc) return rc;
+  if (npts < 0 || (npts > 0 && (!x_dev || !seedm_dev || !grad_dev))) return RC_BAD_ARG;
+  if (npts == 0) return RC_OK;
+  NetH &n = g_net[nid];
+  WorkH &w = g_twk[tid];
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = net_device(n, st))) return rc;
+  if (w.kept && w.kept_x == x_dev && w.kept_n == npts && w.kept_ver == n.wver &&
+      w.p.prec == n.prec)
+    return adjoint_kept(n.dt, n.dn, w.p, n.prec, npts, x_dev, seedm_dev, grad_dev, st);
+  // recompute mode: the forward runs again inside the adjoint
+  if ((rc = work_planes(w, n, npts, false))) return rc;
+  w.kept = false;
+  DevRule given;
+  given.kind = SEED_GIVEN;
+  BatchArgs a;
+  a.npts = npts; a.X = x_dev; a.seeds = seedm_dev; a.grad = grad_dev;
+  a.train = true; a.prec = n.prec;
+  return run_batch(n.dt, n.dn, given, w.p, a, st);
+}
+
+int dnnf90_grad_rule_dev(int nid, int tid, int npts, const double *x_dev, int rid,
+                         double *grad_dev, double *loss_dev, double *tm_dev, void *stream) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, 0, false);
+  if (rc) return rc;
+  if (bad_rule(rid) || g_rule[rid].r.kind == SEED_JROW) return RC_BAD_ARG;
+  if (npts < 0 || (npts > 0 && (!x_dev || !grad_dev))) return RC_BAD_ARG;
+  if (npts == 0) return RC_OK;
+  NetH &n = g_net[nid];
+  WorkH &w = g_twk[tid];
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = net_device(n, st))) return rc;
+  if ((rc = rule_device(g_rule[rid], n.ts))) return rc;
+  if ((rc = work_planes(w, n, npts, false))) return rc;
+  w.kept = false;
+  BatchArgs a;
+  a.npts = npts; a.X = x_dev; a.out = tm_dev; a.grad = grad_dev; a.loss = loss_dev;
+  a.train = true; a.prec = n.prec;
+  return run_batch(n.dt, n.dn, g_rule[rid].d, w.p, a, st);
+}
+
+int dnnf90_jrow_dev(int nid, int tid, int npts, const double *x_dev, int rid,
+                    double *rows_dev, double *tm_dev, void *stream) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, 0, false);
+  if (rc) return rc;
+  if (bad_rule(rid) || g_rule[rid].r.kind != SEED_JROW) return RC_BAD_ARG;
+  if (npts < 0 || (npts > 0 && (!x_dev || !rows_dev))) return RC_BAD_ARG;
+  if (npts == 0) return RC_OK;
+  NetH &n = g_net[nid];
+  WorkH &w = g_twk[tid];
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = net_device(n, st))) return rc;
+  if ((rc = rule_device(g_rule[rid], n.ts))) return rc;
+  if ((rc = work_planes(w, n, npts, false))) return rc;
+  w.kept = false;
+  BatchArgs a;
+  a.npts = npts; a.X = x_dev; a.out = tm_dev; a.rows = rows_dev;
+  a.train = true; a.prec = n.prec;
+  return run_batch(n.dt, n.dn, g_rule[rid].d, w.p, a, st);
+}
+
+const char *dnnf90_last_error(void) { return last_error(); }
+
+long long dnnf90_launch_count(void) { return launch_count(); }
+
+int dnnf90_profile_enable(int on) {
+  profile_enable(on != 0);
+  return RC_OK;
+}
+
+int dnnf90_profile_read(char *buf, int len) {
+  std::string s = profile_read();
+  if (!buf || len <= 0) return (int)s.size() + 1;
+  std::snprintf(buf, (size_t)len, "%s", s.c_str());
+  return (int)s.size() + 1;
+}
+
+int dnnf90_device_available(void) { return device_ready() == RC_OK ? 1 : 0; }
+
+}  // extern "C"

@@ -1,0 +1,195 @@
+// engine.hpp - the device side of the derivative-carrying evaluation and its
+// adjoint: device copies of table sets and weights, per-work-space plane
+// buffers, and the batched forward / seed / adjoint driver.
+//
+// Layout in HBM (one chunk of P points at a time):
+//   T_l, h_l  [P][na][n_l]   carried derivatives and the h cache of hidden
+//                            layer l (neuron index fastest, so a warp reads
+//                            one 128-byte line per multi-index)
+//   S, Sb, Tb [P][na][nmax]  one layer at a time
+//   out       [P][na][nout]  output derivatives (identity read-out)
+//   seed      [P][nout][na]  dL/dT at the output
+// The reference keeps the same per-point planes with the point axis absent
+// (twork_t, lib/train_module.f90:74-90).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "tables.hpp"
+
+namespace dnnf90 {
+
+enum Precision : int {
+  PREC_F64 = 0,    // plain path: FP64 everywhere
+  PREC_SPLIT = 1,  // FP32 planes and Bell arithmetic, sigma^(q) in FP64,
+                   // layer GEMMs as 3-term split-BF16 products with FP32
+                   // accumulation, FP64 gradient reductions
+};
+
+// error codes at the C boundary (the reference's are 0, -1, -2)
+enum : int {
+  RC_OK = 0,
+  RC_BAD_ARG = -1,
+  RC_BAD_FILE = -2,
+  RC_DEVICE = -3,      // CUDA error or no usable GPU
+  RC_NOMEM = -4,       // device allocation failed
+  RC_UNSUPPORTED = -5  // valid for the reference, outside this device path
+};
+
+// seed rules evaluated on the device at the output layer
+enum SeedKind : int {
+  SEED_GIVEN = 0,   // caller supplied dL/dT per point
+  SEED_HALFSQ = 1,  // L = sum_a T_a^2 / 2, seed = T
+  SEED_PINN = 2,    // L = fac R^2 / 2 with R a linear / u*T_a term list
+  SEED_JROW = 3     // seed = dR/dT, per-point gradient rows
+};
+
+struct SeedRuleHost {
+  int kind = SEED_HALFSQ;
+  std::vector<double> coeff;
+  std::vector<int> ind;     // 0-based slots
+  std::vector<int> nonlin;  // 1: term is coeff * T_0 * T_ind
+  double fac = 1.0;
+};
+
+// device copy of one table set
+struct DevTables {
+  int d0 = 0, k = 0, na = 0, nslot = 0, nfq = 0, npair = 0;
+  int *deg = nullptr;        // [na]
+  int *alpha = nullptr;      // [na][d0]
+  int *ind_e1 = nullptr;     // [d0]
+  int *seg = nullptr;        // [na][k+1][3] = {start, num, store slot}
+  uint32_t *fq_pk = nullptr; // ib | operand << 16 (operand: S slot if q==2
+                             // else state slot of B_{id,q-1})
+  double *fq_c64 = nullptr;
+  float *fq_c32 = nullptr;
+  int *pseg = nullptr;       // [na][2] = {start, num}
+  uint32_t *pair_pk = nullptr;  // ia | id << 16
+  double *pair_c64 = nullptr;
+  float *pair_c32 = nullptr;
+  double *tpc = nullptr;     // [(k+2)][(k+3)]
+  int iact = 0;
+  void release();
+};
+
+int upload_tables(const TableSet &t, DevTables &d);
+
+// device copy of a network's weights
+struct DevNet {
+  int nlayer = 0, nw = 0;
+  std::vector<int> dims;
+  std::vector<size_t> woff;  // offset of layer l (index l-1) in the flat array
+  double *w64 = nullptr;     // flat [layer][j][0..m]
+  float *w32 = nullptr;      // FP32 copy for the split path
+  uint64_t uploaded = 0;     // host weight version on the device
+  void release();
+};
+
+// per work-space device buffers, sized for a chunk of points
+struct Planes {
+  int cap_pts = 0;           // points per chunk
+  int prec = -1;
+  size_t bytes = 0;
+  void *base = nullptr;      // one allocation, carved below
+  std::vector<void *> T, h;  // per layer (index l-1), hidden layers only
+  void *S = nullptr, *Sb = nullptr, *Tb = nullptr, *seed = nullptr;
+  void *scratch = nullptr;   // Bell state spill when it does not fit smem
+  size_t scratch_bytes = 0;
+  double *X = nullptr;       // [P][d0] staged inputs
+  double *out = nullptr;     // [P][na][nout]
+  double *loss = nullptr;    // [1]
+  void release();
+};
+
+struct Stream {
+  cudaStream_t s = nullptr;
+};
+
+// Batched driver over npts points already resident on the device.
+//   X      [npts][d0]
+//   out    [npts][na][nout] (may be null)
+//   seeds  [npts][nout][na] for SEED_GIVEN
+//   grad   flat FP64 weight layout, accumulated into (may be null: eval)
+//   rows   [npts][nw] for SEED_JROW
+//   loss   one double, accumulated into (may be null)
+struct BatchArgs {
+  int npts = 0;
+  const double *X = nullptr;
+  double *out = nullptr;
+  const double *seeds = nullptr;
+  double *grad = nullptr;
+  double *rows = nullptr;
+  double *loss = nullptr;
+  bool train = false;
+  int prec = PREC_F64;
+};
+
+// device-side seed rule
+struct DevRule {
+  int kind = SEED_HALFSQ;
+  int nterm = 0;
+  double fac = 1.0;
+  double *coeff = nullptr;
+  int *ind = nullptr;
+  int *nonlin = nullptr;
+  void release();
+};
+int upload_rule(const SeedRuleHost &r, DevRule &d);
+
+int ensure_planes(const DevTables &t, const DevNet &n, int prec, int cap_pts,
+                  Planes &p);
+int run_batch(const DevTables &t, const DevNet &n, const DevRule &rule,
+              Planes &p, const BatchArgs &a, cudaStream_t st);
+
+// Forward of npts <= p.cap_pts points that keeps every plane, and the
+// adjoint from a caller seed [npts][nout][na] on those planes (the
+// store-and-reuse mode of the autograd backward).
+int forward_keep(const DevTables &t, const DevNet &n, Planes &p, int prec,
+                 int npts, const double *X, double *out, cudaStream_t st);
+int adjoint_kept(const DevTables &t, const DevNet &n, Planes &p, int prec,
+                 int npts, const double *X, const double *seed, double *grad,
+                 cudaStream_t st);
+
+// Adam update on the device (opt_adam_step, lib/train_module.f90:656-683);
+// m and v are allocated by the caller and zero on the first call
+int adam_device(double *w, const double *g, double *m, double *v, int nw,
+                double eta, double b1, double b2, double eps, int nbatch,
+                int istep, cudaStream_t st);
+
+// Damped Gauss-Newton step of app/optimizer_module.f90:221-469 (ABS
+// damping): u = (J^T J / nb + mu I)^{-1} (b / nb), J = rows[nrow][nw].
+// The metric is formed on the tensor cores (split-precision) or in FP64
+// (prec), then Cholesky-factored and solved in FP64.
+int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
+               double mu, double *u, int prec, cudaStream_t st);
+
+// count of kernel launches issued by this library (process-wide)
+void note_launch();
+long long launch_count();
+
+// Per-kernel device timing: while enabled, every launch is bracketed by a
+// pair of CUDA events recorded on its own stream; profile_read sums the
+// elapsed times by kernel name.
+void profile_enable(bool on);
+int prof_begin(const char *name, cudaStream_t st);
+void prof_end(int idx, cudaStream_t st);
+std::string profile_read();
+
+#define LAUNCH(name, st, ...)                                 \
+  do {                                                        \
+    int pi_ = ::dnnf90::prof_begin(name, st);                 \
+    __VA_ARGS__;                                              \
+    ::dnnf90::prof_end(pi_, st);                              \
+    ::dnnf90::note_launch();                                  \
+  } while (0)
+
+// device selection and error text
+int device_ready();
+const char *last_error();
+void set_error(const std::string &msg);
+
+}  // namespace dnnf90

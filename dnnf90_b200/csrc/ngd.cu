@@ -1,0 +1,272 @@
+// ngd.cu - the damped Gauss-Newton step of app/optimizer_module.f90:221-469
+// (primal route, ABS damping) on the device:
+//   G = J^T J / nb + mu I,  u = G^{-1} (b / nb),
+// with the metric formed from the residual-Jacobian rows J[nrow][nw] and
+// solved by an FP64 Cholesky factorization (the reference eliminates with
+// partial pivoting, gauss_solve :472-522; G is symmetric positive definite
+// once damped, so the factorization is the natural device form).
+//
+// The metric build is a GEMM: in the split path J is carried as three bf16
+// terms and the six cross products are accumulated in FP32 per 64-row slab
+// (tensor cores), the slabs summed in FP64; in the plain path it is an FP64
+// CUDA-core GEMM.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+
+#include "engine.hpp"
+#include "gemm_tc.hpp"
+
+namespace dnnf90 {
+
+#define CKN(call)                                                      \
+  do {                                                                 \
+    cudaError_t e_ = (call);                                           \
+    if (e_ != cudaSuccess) {                                           \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));   \
+      return e_ == cudaErrorMemoryAllocation ? RC_NOMEM : RC_DEVICE;   \
+    }                                                                  \
+  } while (0)
+
+constexpr int NB = 64;
+
+// G[i][j] += sum_{r in slab} J[r][i] J[r][j] for the lower tiles (j <= i),
+// FP64 CUDA-core tiles of 64 x 64, split over rows with atomics.
+__global__ void __launch_bounds__(256) k_syrk_f64(const double *J, int nrow, int nw,
+                                                  double *G, int rchunk) {
+  const int ti = blockIdx.y, tj = blockIdx.x;
+  if (tj > ti) return;
+  __shared__ double As[16][65], Bs[16][65];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int i0 = ti * 64, j0 = tj * 64;
+  double acc[4][4] = {};
+  const int r0 = blockIdx.z * rchunk, r1 = min(nrow, r0 + rchunk);
+  for (int k0 = r0; k0 < r1; k0 += 16) {
+    for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+      int kk = e / 64, c = e - kk * 64;
+      int r = k0 + kk;
+      As[kk][c] = (r < r1 && i0 + c < nw) ? J[(size_t)r * nw + i0 + c] : 0.0;
+      Bs[kk][c] = (r < r1 && j0 + c < nw) ? J[(size_t)r * nw + j0 + c] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { a[u] = As[kk][ty + 16 * u]; b[u] = Bs[kk][tx + 16 * u]; }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * b[v];
+    }
+    __syncthreads();
+  }
+  for (int u = 0; u < 4; ++u) {
+    int i = i0 + ty + 16 * u;
+    if (i >= nw) continue;
+    for (int v = 0; v < 4; ++v) {
+      int j = j0 + tx + 16 * v;
+      if (j < nw && j <= i) atomicAdd(G + (size_t)i * nw + j, acc[u][v]);
+    }
+  }
+}
+
+// G = G / nb + mu I on the lower triangle; rhs = b / nb
+__global__ void k_scale_damp(double *G, int nw, double inv_nb, double mu,
+                             const double *b, double *rhs) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)nw * nw;
+       e += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(e / nw), j = (int)(e - (size_t)i * nw);
+    if (j > i) continue;
+    double v = G[e] * inv_nb;
+    if (i == j) v += mu;
+    G[e] = v;
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += gridDim.x * blockDim.x)
+    rhs[i] = b[i] * inv_nb;
+}
+
+// unblocked Cholesky of the diagonal block [k0, k0+nb) in shared memory;
+// info[0] receives the first non-positive pivot (1-based) if any
+__global__ void k_potrf_diag(double *G, int nw, int k0, int nb, int *info) {
+  __shared__ double A[NB][NB + 1];
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    int i = e / nb, j = e - i * nb;
+    A[i][j] = j <= i ? G[(size_t)(k0 + i) * nw + k0 + j] : 0.0;
+  }
+  __syncthreads();
+  for (int k = 0; k < nb; ++k) {
+    if (threadIdx.x == 0) {
+      double d = A[k][k];
+      if (!(d > 0.0)) {
+        if (info[0] == 0) info[0] = k0 + k + 1;
+        d = 1.0;
+      }
+      A[k][k] = sqrt(d);
+    }
+    __syncthreads();
+    for (int i = k + 1 + threadIdx.x; i < nb; i += blockDim.x) A[i][k] /= A[k][k];
+    __syncthreads();
+    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+      int i = e / nb, j = e - i * nb;
+      if (i > k && j > k && j <= i) A[i][j] -= A[i][k] * A[j][k];
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    int i = e / nb, j = e - i * nb;
+    if (j <= i) G[(size_t)(k0 + i) * nw + k0 + j] = A[i][j];
+  }
+}
+
+// L21 = A21 L11^{-T}: every row below the block solved independently
+__global__ void k_trsm_panel(double *G, int nw, int k0, int nb) {
+  __shared__ double L[NB][NB + 1];
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    int i = e / nb, j = e - i * nb;
+    L[i][j] = j <= i ? G[(size_t)(k0 + i) * nw + k0 + j] : 0.0;
+  }
+  __syncthreads();
+  for (int r = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x; r < nw;
+       r += gridDim.x * blockDim.x) {
+    double *row = G + (size_t)r * nw + k0;
+    double x[NB];
+    for (int j = 0; j < nb; ++j) {
+      double s = row[j];
+      for (int t = 0; t < j; ++t) s -= x[t] * L[j][t];
+      x[j] = s / L[j][j];
+    }
+    for (int j = 0; j < nb; ++j) row[j] = x[j];
+  }
+}
+
+// trailing update A22 -= L21 L21^T on the lower tiles
+__global__ void __launch_bounds__(256) k_syrk_trail(double *G, int nw, int k0, int nb) {
+  const int base = k0 + nb;
+  const int ti = blockIdx.y, tj = blockIdx.x;
+  if (tj > ti) return;
+  const int i0 = base + ti * 64, j0 = base + tj * 64;
+  __shared__ double As[16][65], Bs[16][65];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4] = {};
+  for (int k = 0; k < nb; k += 16) {
+    for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+      int c = e / 16, kk = e - c * 16;
+      int kx = k0 + k + kk;
+      As[kk][c] = (i0 + c < nw && k + kk < nb) ? G[(size_t)(i0 + c) * nw + kx] : 0.0;
+      Bs[kk][c] = (j0 + c < nw && k + kk < nb) ? G[(size_t)(j0 + c) * nw + kx] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { a[u] = As[kk][ty + 16 * u]; b[u] = Bs[kk][tx + 16 * u]; }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * b[v];
+    }
+    __syncthreads();
+  }
+  for (int u = 0; u < 4; ++u) {
+    int i = i0 + ty + 16 * u;
+    if (i >= nw) continue;
+    for (int v = 0; v < 4; ++v) {
+      int j = j0 + tx + 16 * v;
+      if (j < nw && j <= i) G[(size_t)i * nw + j] -= acc[u][v];
+    }
+  }
+}
+
+// L y = r then L^T u = y, one block; rows are visited in order with a
+// block-wide dot product per row
+__global__ void __launch_bounds__(1024) k_chol_solve(const double *G, int nw, double *x) {
+  __shared__ double red[32];
+  __shared__ double val;
+  for (int i = 0; i < nw; ++i) {  // forward
+    double s = 0.0;
+    for (int j = threadIdx.x; j < i; j += blockDim.x) s += G[(size_t)i * nw + j] * x[j];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+      for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (threadIdx.x == 0) {
+        val = (x[i] - v) / G[(size_t)i * nw + i];
+        x[i] = val;
+      }
+    }
+    __syncthreads();
+  }
+  for (int i = nw - 1; i >= 0; --i) {  // backward with L^T: column i of L
+    double s = 0.0;
+    for (int j = i + 1 + threadIdx.x; j < nw; j += blockDim.x) s += G[(size_t)j * nw + i] * x[j];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+      for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (threadIdx.x == 0) x[i] = (x[i] - v) / G[(size_t)i * nw + i];
+    }
+    __syncthreads();
+  }
+}
+
+int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
+               double mu, double *u, int prec, cudaStream_t st) {
+  double *G = nullptr;
+  int *info = nullptr;
+  CKN(cudaMalloc(&G, sizeof(double) * (size_t)nw * nw));
+  CKN(cudaMalloc(&info, sizeof(int)));
+  CKN(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)nw * nw, st));
+  CKN(cudaMemsetAsync(info, 0, sizeof(int), st));
+  const int tiles = (nw + 63) / 64;
+  int rc = RC_OK;
+  if (prec == PREC_SPLIT && gemm_tc_available()) {
+    rc = gemm_tc_syrk(rows, nrow, nw, G, st);
+  } else {
+    int rchunk = std::max(64, (nrow + 7) / 8);
+    rchunk = (rchunk + 15) / 16 * 16;
+    dim3 grid(tiles, tiles, (nrow + rchunk - 1) / rchunk);
+    LAUNCH("k_syrk_f64", st, k_syrk_f64<<<grid, 256, 0, st>>>(rows, nrow, nw, G, rchunk));
+    CKN(cudaGetLastError());
+  }
+  if (rc) {
+    cudaFree(G);
+    cudaFree(info);
+    return rc;
+  }
+  LAUNCH("k_scale_damp", st, k_scale_damp<<<1024, 256, 0, st>>>(G, nw, 1.0 / (double)nb, mu, b, u));
+  CKN(cudaGetLastError());
+  for (int k0 = 0; k0 < nw; k0 += NB) {
+    const int nbk = std::min(NB, nw - k0);
+    LAUNCH("k_potrf_diag", st, k_potrf_diag<<<1, 256, 0, st>>>(G, nw, k0, nbk, info));
+    CKN(cudaGetLastError());
+    if (k0 + nbk < nw) {
+      const int rem = nw - k0 - nbk;
+      LAUNCH("k_trsm_panel", st, k_trsm_panel<<<std::max(1, std::min(256, (rem + 127) / 128)), 128, 0, st>>>(G, nw, k0, nbk));
+      CKN(cudaGetLastError());
+      const int tt = (rem + 63) / 64;
+      LAUNCH("k_syrk_trail", st, k_syrk_trail<<<dim3(tt, tt), 256, 0, st>>>(G, nw, k0, nbk));
+      CKN(cudaGetLastError());
+    }
+  }
+  LAUNCH("k_chol_solve", st, k_chol_solve<<<1, 1024, 0, st>>>(G, nw, u));
+  CKN(cudaGetLastError());
+  int hinfo = 0;
+  CKN(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKN(cudaStreamSynchronize(st));
+  cudaFree(G);
+  cudaFree(info);
+  if (hinfo) {
+    set_error("the damped metric is not positive definite at column " + std::to_string(hinfo));
+    return RC_BAD_ARG;
+  }
+  return RC_OK;
+}
+
+}  // namespace dnnf90

@@ -1,0 +1,110 @@
+/* dnnf90_b200.h - entry points of the B200 device path beyond the 24 of
+ * dnnf90.h.  The reference evaluates one point per call
+ * (lib/train_module.f90:198-209); these take whole batches, either in host
+ * memory (copies to and from the device inside the call) or already on the
+ * device with a caller stream (the torch.autograd.Function path).
+ *
+ * Layouts: x[npts][d0]; t[npts][na] (output 1, slot order of dnnf90_alpha);
+ * tm[npts][nout][na]; seed[npts][na] (output 1) or seedm[npts][nout][na];
+ * weights and gradients in the flat layer layout: layers 2..nlayer
+ * concatenated, each dims[l-1] rows of dims[l-2]+1 doubles, bias first
+ * (the dnnf90_net_set_layer row layout, lib/c_api_module.f90:185-205).
+ * Return codes as in dnnf90.h.
+ */
+#ifndef DNNF90_B200_H
+#define DNNF90_B200_H
+#include "dnnf90.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* precision of a network's device path.  0 = plain FP64 (every kernel in
+ * FP64; agrees with the reference to rounding).  1 = split: FP32 planes and
+ * Bell arithmetic, sigma^(q) in FP64, layer GEMMs as 3-term split-BF16
+ * products with FP32 accumulation on the tensor cores, FP64 gradient
+ * reductions.  New; the reference is FP64 only. */
+int dnnf90_net_set_precision(int nid, int prec);
+/* number of weights of a network (flat layout); new */
+int dnnf90_nweights(int nid);
+/* read layer l back in the dnnf90_net_set_layer row layout; new */
+int dnnf90_net_get_layer(int nid, int l, double *wrow);
+/* write a network in nn_weight.dat format; counterpart of net_save,
+ * lib/net_module.f90:219-243 */
+int dnnf90_net_save(int nid, const char *filename);
+
+/* net_eval_hod over a batch (lib/net_module.f90:295-375 per point) */
+int dnnf90_eval_batch(int nid, int wid, int npts, const double *x, double *t);
+/* net_eval_hod_multi over a batch (lib/net_module.f90:389-408) */
+int dnnf90_eval_batch_multi(int nid, int wid, int npts, const double *x,
+                            double *tm);
+/* net_grad_point over a batch with caller seeds (lib/train_module.f90:
+ * 478-489 per point), added to accumulator gid */
+int dnnf90_grad_batch(int nid, int tid, int npts, const double *x,
+                      const double *seed, int gid);
+
+/* A seed rule: the loss seed formed on the device from each point's output
+ * derivatives (app/pinn_module.f90:32-65).  kind 1: L = sum_a T_a^2/2,
+ * seed = T.  kind 2: R = sum_k coeff_k T_{slot_k} (times T_1 when
+ * nonlin_k), L = fac R^2/2, seed = fac R dR/dT (set_pinn_seed).  kind 3:
+ * seed = dR/dT, one Jacobian row per point (app/lib_net_module.f90:
+ * 314-330).  slot is 1-based.  Returns a rule handle. */
+int dnnf90_seed_rule_create(int kind, int nterm, const double *coeff,
+                            const int *slot, const int *nonlin, double fac);
+int dnnf90_seed_rule_free(int rid);
+/* forward -> device seed -> adjoint over a batch, added to gid; loss (sum
+ * over points) and t (output 1) may be NULL */
+int dnnf90_grad_rule_batch(int nid, int tid, int npts, const double *x,
+                           int rid, int gid, double *loss, double *t);
+/* Jacobian rows of a rule's residual, rows[npts][nweights]; resid[npts]
+ * (the residual R per point) and t may be NULL */
+int dnnf90_jrow_batch(int nid, int tid, int npts, const double *x, int rid,
+                      double *rows, double *resid, double *t);
+/* flush the points queued for gid and copy the accumulator out */
+int dnnf90_grad_read(int gid, double *g);
+/* damped Gauss-Newton step of app/optimizer_module.f90:221-469 with the ABS
+ * damping: u = (J^T J / nb + mu I)^{-1} (b / nb), rows[nrow][nw], b[nw].
+ * prec 1 forms the metric as split-precision tensor-core products, prec 0
+ * in FP64; the solve is an FP64 Cholesky factorization. */
+int dnnf90_ngd_step(int nid, int nrow, const double *rows, const double *b,
+                    int nb, double mu, int prec, double *u);
+
+/* ---- device-pointer entry points (pointers to device memory; stream is
+ * a cudaStream_t, NULL for the legacy default stream) ---- */
+/* weights from a device array in the flat layout */
+int dnnf90_set_weights_dev(int nid, const double *w_dev, void *stream);
+/* forward of npts points: tm_dev[npts][na][nout] (may be NULL).  keep = 1
+ * keeps every plane on work space tid for dnnf90_backward_dev. */
+int dnnf90_forward_dev(int nid, int tid, int npts, const double *x_dev,
+                       double *tm_dev, int keep, void *stream);
+/* adjoint from seedm_dev[npts][nout][na], added to grad_dev[nweights].  Uses
+ * the planes kept by the last keep=1 forward of the same points and
+ * weights on tid; otherwise recomputes the forward first. */
+int dnnf90_backward_dev(int nid, int tid, int npts, const double *x_dev,
+                        const double *seedm_dev, double *grad_dev,
+                        void *stream);
+/* forward -> rule seed -> adjoint, grad_dev += dL/dw, loss_dev[0] += L;
+ * tm_dev (may be NULL) receives the output derivatives [npts][na][nout] */
+int dnnf90_grad_rule_dev(int nid, int tid, int npts, const double *x_dev,
+                         int rid, double *grad_dev, double *loss_dev,
+                         double *tm_dev, void *stream);
+/* Jacobian rows rows_dev[npts][nweights] of a rule's residual */
+int dnnf90_jrow_dev(int nid, int tid, int npts, const double *x_dev, int rid,
+                    double *rows_dev, double *tm_dev, void *stream);
+/* points per device chunk of a training work space (0 = automatic) */
+int dnnf90_twork_set_chunk(int tid, int npts);
+
+/* text of the last error on this thread; 1 if a CUDA device is usable */
+const char *dnnf90_last_error(void);
+int dnnf90_device_available(void);
+/* number of kernels this library has launched in the process */
+long long dnnf90_launch_count(void);
+/* per-kernel device timing: while enabled every launch is bracketed by CUDA
+ * events on its stream; read writes "name launches total_ms" lines into buf
+ * (returns the length needed) and clears the record */
+int dnnf90_profile_enable(int on);
+int dnnf90_profile_read(char *buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
