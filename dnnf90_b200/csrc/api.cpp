@@ -1151,10 +1151,20 @@ int dnnf90_profile_enable(int on) {
 }
 
 int dnnf90_profile_read(char *buf, int len) {
-  std::string s = profile_read();
-  if (!buf || len <= 0) return (int)s.size() + 1;
-  std::snprintf(buf, (size_t)len, "%s", s.c_str());
-  return (int)s.size() + 1;
+  // a call without a buffer collects the records and reports the length;
+  // the next call with a buffer hands the same text out
+  static std::string pending;
+  static bool have = false;
+  if (!have) {
+    pending = profile_read();
+    have = true;
+  }
+  const int need = (int)pending.size() + 1;
+  if (!buf || len <= 0) return need;
+  std::snprintf(buf, (size_t)len, "%s", pending.c_str());
+  pending.clear();
+  have = false;
+  return need;
 }
 
 int dnnf90_device_available(void) { return device_ready() == RC_OK ? 1 : 0; }

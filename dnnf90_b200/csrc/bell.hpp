@@ -1,0 +1,35 @@
+// bell.hpp - warp-cooperative Bell kernels (see bell.cu, bell_plan.hpp).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "bell_plan.hpp"
+
+namespace dnnf90 {
+
+struct DevTables;
+
+constexpr int BELL_WORKERS = 16;  // warps per block sharing one point's state
+
+struct DevBellPlan {
+  bool ready = false;
+  int workers = 0, k = 0, na = 0, nslot = 0;
+  int *fw_list = nullptr, *fw_arec = nullptr, *fw_grec = nullptr;
+  double *fw_gc64 = nullptr;
+  float *fw_gc32 = nullptr;
+  int *aj_list = nullptr, *aj_orec = nullptr, *aj_pair = nullptr;
+  double *aj_c64 = nullptr;
+  float *aj_c32 = nullptr;
+  void release();
+};
+
+int upload_bell_plan(const TableSet &t, DevBellPlan &d);
+
+// RC_UNSUPPORTED when the set does not fit (K > 8 or the per-point state
+// exceeds shared memory): the caller then uses the generic kernels.
+int bell_fwd2(const DevBellPlan &bp, const DevTables &t, int n, int npts, const void *S,
+              void *T, void *h, bool train, int prec, cudaStream_t st);
+int bell_adj2(const DevBellPlan &bp, const DevTables &t, int n, int npts, const void *Tb,
+              const void *h, void *Sb, double *gbias, int gstride, int prec,
+              cudaStream_t st);
+
+}  // namespace dnnf90

@@ -1,0 +1,39 @@
+// bell_plan.hpp - work lists of the warp-cooperative Bell kernels.
+//
+// The forward recurrence of lib/train_module.f90:303-325,
+//   B_{a,q} = sum_{b in fq(a,q)} C(a,b)/q S_b B_{a-b,q-1},
+//   T_a = sum_q sigma^(q) B_{a,q},  h_a = sum_q sigma^(q+1) B_{a,q},
+// is regrouped by b: for one output a the same sub-multi-index b serves
+// every level q <= p - |b| + 1, so one "group" {b, g = a - b, C(a,b),
+// qmax} feeds up to K-1 register accumulators.  Multi-indices of one
+// degree are independent of each other, so each degree is a phase whose
+// outputs are spread over the workers (warps) of a block, balanced by work.
+//
+// The adjoint (:381-403) has no recurrence: every Sb_b is one sum over
+// a >= b of C(a,b) Tb_a h_{a-b}; Sb_0 is the sum of Tb_a h_a.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "tables.hpp"
+
+namespace dnnf90 {
+
+struct BellPlan {
+  int workers = 0, k = 0, na = 0, nslot = 0;
+  // forward
+  std::vector<int> fw_list;   // [(k+1) * workers][2]: start, count into fw_arec
+  std::vector<int> fw_arec;   // [*][4]: ia | p << 16, gstart, gcount, bbase
+  std::vector<int> fw_grec;   // [*][4]: ib, g, gbase (state slot of B_{g,2}), qmax
+  std::vector<double> fw_gc;  // C(a,b) per group
+  std::vector<int> bbase;     // [na]: state slot of B_{a,2} (or -1)
+  // adjoint
+  std::vector<int> aj_list;   // [workers][2]
+  std::vector<int> aj_orec;   // [*][4]: ib, pstart, pcount, 0
+  std::vector<int> aj_pair;   // [*]: ia | id << 16
+  std::vector<double> aj_c;
+};
+
+BellPlan build_bell_plan(const TableSet &t, int workers);
+
+}  // namespace dnnf90

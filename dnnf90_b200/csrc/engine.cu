@@ -164,6 +164,7 @@ void DevTables::release() {
                 pair_c64, pair_c32, tpc};
   for (void *p : ps)
     if (p) cudaFree(p);
+  bp.release();
   *this = DevTables();
 }
 
@@ -232,6 +233,7 @@ int upload_tables(const TableSet &t, DevTables &d) {
   if ((rc = dput(&d.pair_c64, t.pair_binom.data(), t.pair_binom.size()))) return rc;
   if ((rc = dput(&d.pair_c32, pair32.data(), pair32.size()))) return rc;
   if ((rc = dput(&d.tpc, t.tpc.data(), t.tpc.size()))) return rc;
+  if ((rc = upload_bell_plan(t, d.bp))) return rc;
   return RC_OK;
 }
 
@@ -641,7 +643,7 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
   __shared__ R As[BK][BM + 1];
   __shared__ R Bs[BK][BN + 1];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;  // M tiles on x (no 65535 cap)
   const R *A = (const R *)g.A;
   const R *B = (const R *)g.B;
   R acc[4][4];
@@ -842,6 +844,11 @@ template <typename R>
 static int launch_bell_fwd(const DevTables &t, int n, int npts, const void *S,
                            void *T, void *h, bool train, Planes &p,
                            cudaStream_t st) {
+  {
+    int rc2 = bell_fwd2(t.bp, t, n, npts, S, T, h, train,
+                        sizeof(R) == 8 ? PREC_F64 : PREC_SPLIT, st);
+    if (rc2 != RC_UNSUPPORTED) return rc2;
+  }
   int nthr;
   size_t smem;
   bell_shape(t.nslot, sizeof(R), n, &nthr, &smem);
@@ -880,10 +887,10 @@ static int launch_gemm_cc(int mode, int M, int N, int K, int na, const void *A,
   g.M = M; g.N = N; g.K = K; g.na = na; g.A = A; g.B = B; g.lda = lda;
   g.ldb = ldb; g.C = C; g.ldc = ldc; g.G = G; g.gld = gld; g.kchunk = 0;
   if (mode == G_FWD) {
-    dim3 grid((N + 63) / 64, (M + 63) / 64);
+    dim3 grid((M + 63) / 64, (N + 63) / 64);
     LAUNCH("k_gemm", st, k_gemm<R, G_FWD><<<grid, 256, 0, st>>>(g));
   } else if (mode == G_DT) {
-    dim3 grid((N + 63) / 64, (M + 63) / 64);
+    dim3 grid((M + 63) / 64, (N + 63) / 64);
     LAUNCH("k_gemm", st, k_gemm<R, G_DT><<<grid, 256, 0, st>>>(g));
   } else {
     int tiles = ((N + 63) / 64) * ((M + 63) / 64);
@@ -892,7 +899,7 @@ static int launch_gemm_cc(int mode, int M, int N, int K, int na, const void *A,
     // FP32 partial sums stay short: the reduction across blocks is FP64
     if (sizeof(R) == 4) g.kchunk = std::min(g.kchunk, 4096);
     splits = (K + g.kchunk - 1) / g.kchunk;
-    dim3 grid((N + 63) / 64, (M + 63) / 64, splits);
+    dim3 grid((M + 63) / 64, (N + 63) / 64, splits);
     LAUNCH("k_gemm", st, k_gemm<R, G_DW><<<grid, 256, 0, st>>>(g));
   }
   CK(cudaGetLastError());
@@ -997,9 +1004,15 @@ static int adj_chunk(Chunk<R> &c, const double *X, const double *seed,
     aj.Tb = p.Tb; aj.h = p.h[l - 1]; aj.Sb = p.Sb;
     aj.gbias = rows || !grad ? nullptr : grad + net.woff[l - 1];
     aj.gstride = m + 1;
-    dim3 grid(std::min(np, smc * 8), (n + 127) / 128);
-    LAUNCH("k_bell_adj", c.st, k_bell_adj<R><<<grid, 128, 0, c.st>>>(aj));
-    CK(cudaGetLastError());
+    rc = bell_adj2(t.bp, t, n, np, p.Tb, p.h[l - 1], p.Sb, aj.gbias, aj.gstride,
+                   split ? PREC_SPLIT : PREC_F64, c.st);
+    if (rc == RC_UNSUPPORTED) {
+      dim3 grid(std::min(np, smc * 8), (n + 127) / 128);
+      LAUNCH("k_bell_adj", c.st, k_bell_adj<R><<<grid, 128, 0, c.st>>>(aj));
+      CK(cudaGetLastError());
+    } else if (rc) {
+      return rc;
+    }
     const int M = np * na;
     if (rows) {
       LAUNCH("k_dw_rows", c.st, k_dw_rows<R><<<std::min(np, smc * 8), 256, 0, c.st>>>(n, m, na, np, p.Sb, p.T[l - 2],

@@ -19,6 +19,7 @@
 #include <string>
 #include <vector>
 
+#include "bell.hpp"
 #include "tables.hpp"
 
 namespace dnnf90 {
@@ -73,6 +74,7 @@ struct DevTables {
   float *pair_c32 = nullptr;
   double *tpc = nullptr;     // [(k+2)][(k+3)]
   int iact = 0;
+  DevBellPlan bp;            // work lists of the warp-cooperative kernels
   void release();
 };
 
