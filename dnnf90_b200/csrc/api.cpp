@@ -164,7 +164,7 @@ int net_device(NetH &n, cudaStream_t st) {
                                  cudaMemcpyHostToDevice, st), "weights H2D")))
       return rc;
     if ((rc = weights_to_f32(d.w64, d.w32, n.w.size(), st))) return rc;
-    if ((rc = gemm_tc_prepare(&d, st))) return rc;
+    if ((rc = gemm_tc_prepare(&d, n.w.data(), st))) return rc;
     d.uploaded = n.wver;
   }
   return RC_OK;
@@ -264,7 +264,8 @@ int flush_queue(int tid) {
   BatchArgs a;
   a.npts = np; a.X = w.dX; a.seeds = w.dS; a.grad = g.d; a.train = true; a.prec = n.prec;
   if ((rc = run_batch(n.dt, n.dn, given, w.p, a, w.st))) return rc;
-  return ck(cudaStreamSynchronize(w.st), "grad_point batch");
+  if ((rc = ck(cudaStreamSynchronize(w.st), "grad_point batch"))) return rc;
+  return gemm_tc_flag(&n.dn, w.st);
 }
 
 int flush_for_grad(int gid) {
@@ -424,7 +425,10 @@ int run_eval(int nid, WorkH &w, int npts, const double *x, double *tm,
         return rc;
     }
   }
-  if (host) return ck(cudaStreamSynchronize(w.st), "eval");
+  if (host) {
+    if ((rc = ck(cudaStreamSynchronize(w.st), "eval"))) return rc;
+    return gemm_tc_flag(&n.dn, w.st);
+  }
   return RC_OK;
 }
 
@@ -535,6 +539,7 @@ int host_train(int nid, int tid, int npts, const double *x, int kind,
   double lv = 0.0;
   if (!rc) rc = ck(cudaMemcpyAsync(&lv, dloss, sizeof(double), cudaMemcpyDeviceToHost, w.st), "D2H");
   if (!rc) rc = ck(cudaStreamSynchronize(w.st), "train batch");
+  if (!rc) rc = gemm_tc_flag(&n.dn, w.st);
   if (loss) *loss = lv;
   if (dseed) cudaFree(dseed);
   if (drows) cudaFree(drows);

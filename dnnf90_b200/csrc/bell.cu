@@ -46,7 +46,7 @@ static int put(T **d, const std::vector<T> &h) {
 
 int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
   d.release();
-  BellPlan P = build_bell_plan(t, BELL_WORKERS);
+  BellPlan P = build_bell_plan(t, BELL_WORKERS, ADJ_WORKERS);
   d.workers = P.workers;
   d.k = P.k;
   d.na = P.na;
@@ -122,13 +122,28 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd2(Fwd2Args a) {
         R acc[KK + 1];
 #pragma unroll
         for (int q = 0; q <= KK; ++q) acc[q] = (R)0;
-        for (int g = ar.y; g < ar.y + ar.z; ++g) {
-          const int4 gr = __ldg(a.grec + g);  // ib, g, gbase, qmax
-          const R x = __ldg(gc + g) * sS[gr.x * NPB + ln];
-          if (KK >= 2) acc[2] += x * sS[gr.y * NPB + ln];
+        // the group records of four groups are fetched together, so their
+        // latency is paid once per four groups, not on every group
+        const int gend = ar.y + ar.z;
+        for (int g0 = ar.y; g0 < gend; g0 += BELL_UNROLL) {
+          int4 gr[BELL_UNROLL];
+          R cv[BELL_UNROLL];
 #pragma unroll
-          for (int q = 3; q <= KK; ++q)
-            if (q <= gr.w) acc[q] += x * sB[(gr.z + q - 3) * NPB + ln];
+          for (int u = 0; u < BELL_UNROLL; ++u) {
+            const int gi = min(g0 + u, gend - 1);
+            gr[u] = __ldg(a.grec + gi);  // ib, g, gbase, qmax
+            cv[u] = __ldg(gc + gi);
+          }
+#pragma unroll
+          for (int u = 0; u < BELL_UNROLL; ++u) {
+            if (g0 + u < gend) {
+              const R x = cv[u] * sS[gr[u].x * NPB + ln];
+              if (KK >= 2) acc[2] += x * sS[gr[u].y * NPB + ln];
+#pragma unroll
+              for (int q = 3; q <= KK; ++q)
+                if (q <= gr[u].w) acc[q] += x * sB[(gr[u].z + q - 3) * NPB + ln];
+            }
+          }
         }
         const R sa = sS[ia * NPB + ln];
         R tt = dt[1] * sa, hh = dt[2] * sa;
@@ -163,7 +178,7 @@ struct Adj2Args {
 };
 
 template <typename R, int NPB>
-__global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_adj2(Adj2Args a) {
+__global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj2(Adj2Args a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R *sT = (R *)smem_raw;
   R *sH = sT + (size_t)a.na * NPB;
@@ -181,7 +196,7 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_adj2(Adj2Args a) {
     const R *Tb = (const R *)a.Tb + pt * plane;
     const R *Hh = (const R *)a.h + pt * plane;
     R *Sb = (R *)a.Sb + pt * plane;
-    for (int ia = warp; ia < a.na; ia += BELL_WORKERS)
+    for (int ia = warp; ia < a.na; ia += ADJ_WORKERS)
       if (lact) {
         sT[ia * NPB + lane] = act ? Tb[(size_t)ia * n + j] : (R)0;
         sH[ia * NPB + lane] = act ? Hh[(size_t)ia * n + j] : (R)0;
@@ -190,16 +205,24 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_adj2(Adj2Args a) {
     for (int r = rs; r < rs + rn; ++r) {
       const int4 o = __ldg(a.orec + r);  // ib, pstart, pcount
       R s0 = (R)0, s1 = (R)0;
-      int ip = o.y;
       const int pe = o.y + o.z;
-      for (; ip + 1 < pe; ip += 2) {
-        const int k0 = __ldg(a.pair + ip), k1 = __ldg(a.pair + ip + 1);
-        s0 += __ldg(cc + ip) * sT[(k0 & 0xffff) * NPB + ln] * sH[(k0 >> 16) * NPB + ln];
-        s1 += __ldg(cc + ip + 1) * sT[(k1 & 0xffff) * NPB + ln] * sH[(k1 >> 16) * NPB + ln];
-      }
-      if (ip < pe) {
-        const int k0 = __ldg(a.pair + ip);
-        s0 += __ldg(cc + ip) * sT[(k0 & 0xffff) * NPB + ln] * sH[(k0 >> 16) * NPB + ln];
+      for (int ip = o.y; ip < pe; ip += 2 * ADJ_UNROLL) {
+        int kk[2 * ADJ_UNROLL];
+        R cv[2 * ADJ_UNROLL];
+#pragma unroll
+        for (int u = 0; u < 2 * ADJ_UNROLL; ++u) {
+          const int pi = min(ip + u, pe - 1);
+          kk[u] = __ldg(a.pair + pi);
+          cv[u] = __ldg(cc + pi);
+        }
+#pragma unroll
+        for (int u = 0; u < 2 * ADJ_UNROLL; ++u) {
+          if (ip + u < pe) {
+            const R v = cv[u] * sT[(kk[u] & 0xffff) * NPB + ln] * sH[(kk[u] >> 16) * NPB + ln];
+            if (u & 1) s1 += v;
+            else s0 += v;
+          }
+        }
       }
       const R s = s0 + s1;
       if (act) Sb[(size_t)o.x * n + j] = s;
@@ -290,7 +313,7 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
   dim3 grid(gx, gy);
   auto k = k_bell_adj2<R, NPB>;
   CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  LAUNCH("k_bell_adj", st, k<<<grid, BELL_WORKERS * 32, smem, st>>>(a));
+  LAUNCH("k_bell_adj", st, k<<<grid, ADJ_WORKERS * 32, smem, st>>>(a));
   CKB(cudaGetLastError());
   return RC_OK;
 }

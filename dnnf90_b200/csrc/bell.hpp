@@ -8,7 +8,10 @@ namespace dnnf90 {
 
 struct DevTables;
 
-constexpr int BELL_WORKERS = 16;  // warps per block sharing one point's state
+constexpr int BELL_WORKERS = 32;  // warps per block sharing one point's state
+constexpr int BELL_UNROLL = 4;    // table records fetched ahead per step
+constexpr int ADJ_WORKERS = 16;   // warps per block of the adjoint
+constexpr int ADJ_UNROLL = 2;     // pairs fetched ahead: 2 * ADJ_UNROLL
 
 struct DevBellPlan {
   bool ready = false;

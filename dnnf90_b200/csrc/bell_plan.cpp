@@ -26,7 +26,7 @@ std::vector<std::vector<int>> balance(const std::vector<long> &cost, int workers
 
 }  // namespace
 
-BellPlan build_bell_plan(const TableSet &t, int workers) {
+BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
   BellPlan P;
   P.workers = workers;
   P.k = t.k;
@@ -96,9 +96,9 @@ BellPlan build_bell_plan(const TableSet &t, int workers) {
       lists[ib].push_back({(uint32_t)t.pair_ia[ip] | ((uint32_t)t.pair_id[ip] << 16),
                            t.pair_binom[ip]});
   for (int ib = 0; ib < na; ++ib) cost.push_back(4 + (long)lists[ib].size());
-  auto asg = balance(cost, workers);
-  P.aj_list.assign((size_t)workers * 2, 0);
-  for (int w = 0; w < workers; ++w) {
+  auto asg = balance(cost, aj_workers);
+  P.aj_list.assign((size_t)aj_workers * 2, 0);
+  for (int w = 0; w < aj_workers; ++w) {
     P.aj_list[w * 2] = (int)P.aj_orec.size() / 4;
     P.aj_list[w * 2 + 1] = (int)asg[w].size();
     for (int ib : asg[w]) {

@@ -34,6 +34,6 @@ struct BellPlan {
   std::vector<double> aj_c;
 };
 
-BellPlan build_bell_plan(const TableSet &t, int workers);
+BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers);
 
 }  // namespace dnnf90

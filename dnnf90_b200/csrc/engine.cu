@@ -944,9 +944,10 @@ static int fwd_chunk(Chunk<R> &c, const DevRule *rule, const double *X,
   for (int l = 3; l < L; ++l) {
     const int n = net.dims[l - 1], m = net.dims[l - 2];
     const int M = np * na;
-    if (c.split() && gemm_tc_available())
-      rc = gemm_tc_fwd(&net, l, M, n, m, na, p.T[l - 2], p.S, c.st);
-    else
+    rc = c.split() && gemm_tc_available()
+             ? gemm_tc_fwd(&net, l, M, n, m, na, p.T[l - 2], p.S, c.st)
+             : RC_UNSUPPORTED;
+    if (rc == RC_UNSUPPORTED)
       rc = launch_gemm_cc<R>(G_FWD, M, n, m, na, p.T[l - 2], m, c.W(l), m + 1, p.S, n,
                              nullptr, 0, c.st);
     if (rc) return rc;
@@ -1019,16 +1020,17 @@ static int adj_chunk(Chunk<R> &c, const double *X, const double *seed,
                                                              rows, net.nw, net.woff[l - 1]));
       CK(cudaGetLastError());
     } else if (grad) {
-      if (split && gemm_tc_available())
-        rc = gemm_tc_dw(&net, l, M, n, m, p.Sb, p.T[l - 2], grad + net.woff[l - 1], c.st);
-      else
+      rc = split && gemm_tc_available()
+               ? gemm_tc_dw(&net, l, M, n, m, p.Sb, p.T[l - 2], grad + net.woff[l - 1], c.st)
+               : RC_UNSUPPORTED;
+      if (rc == RC_UNSUPPORTED)
         rc = launch_gemm_cc<R>(G_DW, n, m, M, na, p.Sb, n, p.T[l - 2], m, nullptr, 0,
                                grad + net.woff[l - 1], m + 1, c.st);
       if (rc) return rc;
     }
-    if (split && gemm_tc_available())
-      rc = gemm_tc_dt(&net, l, M, n, m, p.Sb, p.Tb, c.st);
-    else
+    rc = split && gemm_tc_available() ? gemm_tc_dt(&net, l, M, n, m, p.Sb, p.Tb, c.st)
+                                      : RC_UNSUPPORTED;
+    if (rc == RC_UNSUPPORTED)
       rc = launch_gemm_cc<R>(G_DT, M, m, n, na, p.Sb, n, c.W(l), m + 1, p.Tb, m, nullptr,
                              0, c.st);
     if (rc) return rc;

@@ -87,6 +87,7 @@ struct DevNet {
   std::vector<size_t> woff;  // offset of layer l (index l-1) in the flat array
   double *w64 = nullptr;     // flat [layer][j][0..m]
   float *w32 = nullptr;      // FP32 copy for the split path
+  void *tc = nullptr;        // pre-split tensor-core weight operands
   uint64_t uploaded = 0;     // host weight version on the device
   void release();
 };

@@ -1,27 +1,771 @@
-// gemm_tc.cu - split-BF16 tcgen05 GEMMs (see gemm_tc.hpp).
+// gemm_tc.cu - split-BF16 layer GEMMs on the tcgen05 tensor cores.
+//
+// One persistent kernel, warp-specialised (416 threads):
+//   warps 0-7  producers: read FP32 operand rows from HBM (coalesced 16-byte
+//              loads, the next K block prefetched into registers), split every value x into three bf16 terms
+//              x1 = bf16(x), x2 = bf16(x - x1), x3 = bf16(x - x1 - x2) and
+//              store them in the 128-byte-swizzled canonical layout the
+//              tensor core reads (one tile per term)
+//   warp 12    MMA issuer: per 16-deep k-step six tcgen05.mma (kind::f16,
+//              bf16 x bf16 -> FP32) for the cross terms of order <= 2:
+//              a3b1, a2b2, a1b3, a2b1, a1b2, a1b1, smallest first, into an
+//              accumulator in tensor memory (two buffers, so the epilogue of
+//              one tile overlaps the products of the next)
+//   warps 8-11 epilogue: tcgen05.ld of the accumulator (lane = row), bias
+//              on the alpha = 0 rows, FP32 store; or, for the weight
+//              gradient, FP32 partials of 512 rows added into FP64
+//              registers and reduced to HBM with FP64 atomics
+// Hand-offs are mbarriers: producer -> MMA (full), MMA -> producer (empty,
+// through tcgen05.commit), MMA -> epilogue (tmem full), epilogue -> MMA
+// (tmem empty).  Every wait is bounded; a wait that runs out sets a flag
+// that the host reads after the launch, and the kernel returns.
+//
+// Modes:
+//   FWD  S[M][N]  = A[M][K] W^T  (+ bias[N] on rows r % na == 0),
+//        A = T_{l-1} plane (K-major), W pre-split and pre-swizzled
+//   DT   Tb[M][N] = A[M][K] W    (A = Sb plane, K = n, N = m)
+//   DW   G[j][1+i] += sum_r A[r][j] B[r][i]  (A = Sb, B = T_{l-1}, both
+//        MN-major tiles, K = rows split across blocks)
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "engine.hpp"
 #include "gemm_tc.hpp"
 
 namespace dnnf90 {
 
-bool gemm_tc_available() { return false; }
-void gemm_tc_release_weights(DevNet *) {}
-int gemm_tc_prepare(DevNet *, cudaStream_t) { return RC_OK; }
-int gemm_tc_fwd(const DevNet *, int, int, int, int, int, const void *, void *,
-                cudaStream_t) {
-  return RC_UNSUPPORTED;
+#define CKT(call)                                                      \
+  do {                                                                 \
+    cudaError_t e_ = (call);                                           \
+    if (e_ != cudaSuccess) {                                           \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));   \
+      return e_ == cudaErrorMemoryAllocation ? RC_NOMEM : RC_DEVICE;   \
+    }                                                                  \
+  } while (0)
+
+namespace tc {
+
+constexpr int NPROD_WARPS = 8, NPROD = NPROD_WARPS * 32;  // producers
+constexpr int EPI_WARP0 = 8;                              // warps 8-11: epilogue
+constexpr int MMA_WARP = 12;
+constexpr int NTHREADS = 13 * 32;
+constexpr int BM = 128;       // rows per tile (MMA M)
+constexpr int BK = 64;        // K per block: one 128-byte bf16 swizzle row
+constexpr int ROWB = 128;     // bytes per swizzled row
+constexpr int MODE_FWD = 0, MODE_DT = 1, MODE_DW = 2;
+constexpr long WAIT_LIMIT = 1L << 26;  // polls before a wait gives up (seconds)
+
+__device__ __forceinline__ uint32_t su32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
 }
-int gemm_tc_dt(const DevNet *, int, int, int, int, const void *, void *,
-               cudaStream_t) {
-  return RC_UNSUPPORTED;
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t cnt) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(cnt) : "memory");
 }
-int gemm_tc_dw(const DevNet *, int, int, int, int, const void *, const void *,
-               double *, cudaStream_t) {
-  return RC_UNSUPPORTED;
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(su32(b))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t par) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(su32(b)), "r"(par)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; false (and the error flag set) when the limit runs out
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t par, int *flag, int code) {
+  for (long it = 0; it < WAIT_LIMIT; ++it) {
+    if (mbar_try(b, par)) return true;
+    if (*(volatile int *)flag) return false;
+    if (it > 64) __nanosleep(32);
+  }
+  atomicCAS(flag, 0, code);
+  return false;
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// smem matrix descriptor, SWIZZLE_128B, sm100 version bits
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= 1ull << 46;  // descriptor version for sm_100
+  d |= 2ull << 61;  // SWIZZLE_128B
+  return d;
+}
+// instruction descriptor: kind::f16, A = B = bf16, D = f32, M = 128
+__host__ __device__ constexpr uint32_t idesc(int n, int a_mn, int b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+         ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t id,
+                                    uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(id), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t *b) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   su32(b))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-int gemm_tc_syrk(const double *, int, int, double *, cudaStream_t) {
-  return RC_UNSUPPORTED;
+// the three bf16 terms of four FP32 values, packed two per word
+__device__ __forceinline__ void split4(float4 x, uint2 &p1, uint2 &p2, uint2 &p3) {
+  float xs[4] = {x.x, x.y, x.z, x.w};
+  uint16_t h[3][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    float r = xs[i];
+    __nv_bfloat16 b1 = __float2bfloat16_rn(r);
+    r = r - __bfloat162float(b1);
+    __nv_bfloat16 b2 = __float2bfloat16_rn(r);
+    r = r - __bfloat162float(b2);
+    __nv_bfloat16 b3 = __float2bfloat16_rn(r);
+    h[0][i] = __bfloat16_as_ushort(b1);
+    h[1][i] = __bfloat16_as_ushort(b2);
+    h[2][i] = __bfloat16_as_ushort(b3);
+  }
+  p1 = make_uint2(h[0][0] | ((uint32_t)h[0][1] << 16), h[0][2] | ((uint32_t)h[0][3] << 16));
+  p2 = make_uint2(h[1][0] | ((uint32_t)h[1][1] << 16), h[1][2] | ((uint32_t)h[1][3] << 16));
+  p3 = make_uint2(h[2][0] | ((uint32_t)h[2][1] << 16), h[2][2] | ((uint32_t)h[2][3] << 16));
+}
+
+// byte offset of (row, k) in a K-major SW128 tile of 8-row atoms
+__device__ __forceinline__ uint32_t kmaj_off(int row, int k) {
+  return (uint32_t)((row >> 3) * 1024 + (row & 7) * ROWB + ((((k >> 3) ^ (row & 7)) & 7) << 4) +
+                    (k & 7) * 2);
+}
+// byte offset of (mn, k) in an MN-major SW128 tile: atoms of 64 mn x 8 k,
+// mn blocks LBO = 1024 apart, k atoms SBO = mnb * 1024 apart
+__device__ __forceinline__ uint32_t mnmaj_off(int mn, int k, int mnb) {
+  const int r = k & 7;
+  return (uint32_t)((k >> 3) * mnb * 1024 + (mn >> 6) * 1024 + r * ROWB +
+                    (((((mn >> 3) & 7) ^ r)) << 4) + (mn & 7) * 2);
+}
+
+struct Args {
+  int mode;
+  int M, N, K, na;
+  const float *A;  // FWD/DT: [M][K]; DW: [K][Mdw] (Sb)
+  const float *B;  // DW only: [K][Ndw] (T_{l-1})
+  int lda, ldb;
+  const uint8_t *W;     // FWD/DT: pre-split weights, [3][nkb][BN rows][128 B] per N tile
+  const float *bias;    // FWD: [N]
+  float *C;             // FWD/DT: [M][ldc]
+  int ldc;
+  double *G;            // DW: [Mdw][gld], column offset 1
+  int gld;
+  int BN;               // N per tile
+  int ntn;              // N tiles
+  int kchunk;           // DW: K blocks per TMEM partial
+  int kblocks_per_cta;  // DW: K blocks per block of the grid
+  int *flag;            // wait time-out / error flag
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(NTHREADS, 1) k_tc_gemm(Args g) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t *sm = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int BN = g.BN;
+  const int nkb = (MODE == MODE_DW) ? 0 : (g.K + BK - 1) / BK;
+  // ---- shared memory layout
+  // FWD/DT: [B resident: 3 * nkb * BN * 128][stages: NST * 3 * 128 * 128]
+  // DW:     [stages: NST * (3 * 8*2*1024 (A, 64 k x 128 mn) + 3 * 8*mnbB*1024 (B))]
+  const int mnbB = (MODE == MODE_DW) ? (BN + 63) / 64 : 0;
+  const uint32_t a_tile = (MODE == MODE_DW) ? 8 * 2 * 1024 : BM * ROWB;      // one term
+  const uint32_t b_tile = (MODE == MODE_DW) ? 8 * mnbB * 1024 : BN * ROWB;   // one term
+  const uint32_t stage_bytes = (MODE == MODE_DW) ? 3 * (a_tile + b_tile) : 3 * a_tile;
+  const uint32_t bres = (MODE == MODE_DW) ? 0 : 3 * nkb * b_tile;
+  const int NST = (MODE == MODE_DW) ? 3 : 2;
+  uint8_t *sB = sm;
+  uint8_t *sStage = sm + bres;
+  uint64_t *bars = (uint64_t *)(sStage + NST * stage_bytes);
+  uint64_t *full = bars, *empty = bars + NST, *tfull = bars + 2 * NST, *tempty = bars + 2 * NST + 2;
+  uint32_t *tmem_hold = (uint32_t *)(bars + 2 * NST + 4);
+
+  const int ntn = g.ntn;
+  const int tn = blockIdx.y;  // N tile of this block
+  const int n0 = tn * BN;
+  // tile sequence of this block
+  int tiles_m = 0, first_m = 0, step_m = 1, kb_begin = 0, kb_end = 0;
+  if (MODE == MODE_DW) {
+    const int nkb_all = (g.K + BK - 1) / BK;
+    kb_begin = blockIdx.x * g.kblocks_per_cta;
+    kb_end = min(nkb_all, kb_begin + g.kblocks_per_cta);
+  } else {
+    tiles_m = (g.M + BM - 1) / BM;
+    first_m = blockIdx.x;
+    step_m = gridDim.x;
+  }
+  (void)ntn;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NST; ++s) {
+      mbar_init(full + s, NPROD);
+      mbar_init(empty + s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(tfull + b, 1);
+      mbar_init(tempty + b, 128);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  const uint32_t tcols = (MODE == MODE_DW) ? 128u : (BN <= 64 ? 128u : 256u);
+  if (warp == MMA_WARP) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     su32(tmem_hold)),
+                 "r"(tcols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // resident weights (FWD/DT): copied once by the producers
+  if (MODE != MODE_DW && warp < NPROD_WARPS) {
+    const uint4 *src = (const uint4 *)(g.W + (size_t)tn * bres);
+    uint4 *dst = (uint4 *)sB;
+    for (int i = threadIdx.x; i < (int)(bres / 16); i += NPROD) dst[i] = src[i];
+    fence_proxy_async();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_hold;
+  int *flag = g.flag;
+
+  if (warp < NPROD_WARPS) {
+    // ------------------------------------------------------------ producers
+    // Every global load of the next K block is issued before the current
+    // block is split and stored, so two blocks of loads are in flight.
+    const int t = threadIdx.x;  // 0..NPROD-1
+    int stage = 0;
+    uint32_t ph = 0;
+    auto next_stage = [&]() {
+      if (++stage == NST) { stage = 0; ph ^= 1u; }
+    };
+    if (MODE != MODE_DW) {
+      constexpr int PF = BM * BK / 4 / NPROD;  // float4 per thread per block
+      auto load = [&](float4 *v, int mt, int kb) {
+        const int k0 = kb * BK;
+#pragma unroll
+        for (int it = 0; it < PF; ++it) {
+          const int e = it * NPROD + t;
+          const int row = e >> 4, c4 = e & 15;
+          const int gr = mt * BM + row, gk = k0 + c4 * 4;
+          v[it] = (gr < g.M && gk < g.K) ? __ldg((const float4 *)(g.A + (size_t)gr * g.lda + gk))
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      };
+      float4 cur[PF], nxt[PF];
+      int mt = first_m, kb = 0;
+      if (mt < tiles_m) load(cur, mt, 0);
+      while (mt < tiles_m) {
+        int nmt = mt, nkb2 = kb + 1;
+        if (nkb2 == nkb) { nkb2 = 0; nmt += step_m; }
+        if (nmt < tiles_m) load(nxt, nmt, nkb2);
+        if (!mbar_wait(empty + stage, ph ^ 1u, flag, 1)) goto done;
+        uint8_t *st = sStage + stage * stage_bytes;
+#pragma unroll
+        for (int it = 0; it < PF; ++it) {
+          const int e = it * NPROD + t;
+          const int row = e >> 4, c4 = e & 15;
+          uint2 p1, p2, p3;
+          split4(cur[it], p1, p2, p3);
+          const uint32_t off = kmaj_off(row, c4 * 4);
+          *(uint2 *)(st + off) = p1;
+          *(uint2 *)(st + a_tile + off) = p2;
+          *(uint2 *)(st + 2 * a_tile + off) = p3;
+        }
+        fence_proxy_async();
+        mbar_arrive(full + stage);
+        next_stage();
+#pragma unroll
+        for (int it = 0; it < PF; ++it) cur[it] = nxt[it];
+        mt = nmt;
+        kb = nkb2;
+      }
+    } else {
+      // A: 64 rows x 128 j of Sb (32 threads per row); B: 64 rows x 64 i
+      // of T_{l-1} (16 threads per row)
+      constexpr int PA = 64 * 32 / NPROD, PB = 64 * 16 / NPROD;
+      const int Mdw = g.M;
+      auto load = [&](float4 *va, float4 *vb, int kb) {
+        const int r0 = kb * BK;
+#pragma unroll
+        for (int it = 0; it < PA; ++it) {
+          const int e = it * NPROD + t;
+          const int kr = e >> 5, j = (e & 31) * 4;
+          const int gr = r0 + kr;
+          va[it] = (gr < g.K && j < Mdw) ? __ldg((const float4 *)(g.A + (size_t)gr * g.lda + j))
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int it = 0; it < PB; ++it) {
+          const int e = it * NPROD + t;
+          const int kr = e >> 4, i = n0 + (e & 15) * 4;
+          const int gr = r0 + kr;
+          vb[it] = (gr < g.K && i < g.N) ? __ldg((const float4 *)(g.B + (size_t)gr * g.ldb + i))
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      };
+      float4 ca[PA], cb[PB], na_[PA], nb_[PB];
+      if (kb_begin < kb_end) load(ca, cb, kb_begin);
+      for (int kb = kb_begin; kb < kb_end; ++kb) {
+        if (kb + 1 < kb_end) load(na_, nb_, kb + 1);
+        if (!mbar_wait(empty + stage, ph ^ 1u, flag, 1)) goto done;
+        uint8_t *st = sStage + stage * stage_bytes;
+        uint8_t *sb = st + 3 * a_tile;
+#pragma unroll
+        for (int it = 0; it < PA; ++it) {
+          const int e = it * NPROD + t;
+          const int kr = e >> 5, j = (e & 31) * 4;
+          uint2 p1, p2, p3;
+          split4(ca[it], p1, p2, p3);
+          const uint32_t off = mnmaj_off(j, kr, 2);
+          *(uint2 *)(st + off) = p1;
+          *(uint2 *)(st + a_tile + off) = p2;
+          *(uint2 *)(st + 2 * a_tile + off) = p3;
+        }
+#pragma unroll
+        for (int it = 0; it < PB; ++it) {
+          const int e = it * NPROD + t;
+          const int kr = e >> 4, il = (e & 15) * 4;
+          uint2 p1, p2, p3;
+          split4(cb[it], p1, p2, p3);
+          const uint32_t off = mnmaj_off(il, kr, mnbB);
+          *(uint2 *)(sb + off) = p1;
+          *(uint2 *)(sb + b_tile + off) = p2;
+          *(uint2 *)(sb + 2 * b_tile + off) = p3;
+        }
+        fence_proxy_async();
+        mbar_arrive(full + stage);
+        next_stage();
+#pragma unroll
+        for (int it = 0; it < PA; ++it) ca[it] = na_[it];
+#pragma unroll
+        for (int it = 0; it < PB; ++it) cb[it] = nb_[it];
+      }
+    }
+  } else if (warp == MMA_WARP) {
+    // ------------------------------------------------------------ MMA issuer
+    int stage = 0;
+    uint32_t ph = 0;
+    auto next_stage = [&]() {
+      if (++stage == NST) { stage = 0; ph ^= 1u; }
+    };
+    // term pairs, smallest first: (a3,b1) (a2,b2) (a1,b3) (a2,b1) (a1,b2) (a1,b1)
+    const int pa[6] = {2, 1, 0, 1, 0, 0};
+    const int pb[6] = {0, 1, 2, 0, 1, 0};
+    if (MODE != MODE_DW) {
+      const uint32_t id = idesc(BN, 0, 0);
+      int buf = 0;
+      uint32_t tph = 0;
+      for (int mt = first_m; mt < tiles_m; mt += step_m) {
+        if (!mbar_wait(tempty + buf, tph ^ 1u, flag, 2)) goto done;
+        tc_fence_after();
+        const uint32_t dcol = tmem + (uint32_t)(buf * BN);
+        for (int kb = 0; kb < nkb; ++kb) {
+          if (!mbar_wait(full + stage, ph, flag, 3)) goto done;
+          tc_fence_after();
+          if (lane == 0) {
+            const uint32_t sa = su32(sStage + stage * stage_bytes);
+            const uint32_t sbb = su32(sB);
+            const int ksteps = min(BK, g.K - kb * BK) / 16;
+            for (int ks = 0; ks < ksteps; ++ks) {
+#pragma unroll
+              for (int p = 0; p < 6; ++p) {
+                const uint64_t ad = sdesc(sa + pa[p] * a_tile + ks * 32, 16, 1024);
+                const uint64_t bd =
+                    sdesc(sbb + (pb[p] * nkb + kb) * b_tile + ks * 32, 16, 1024);
+                mma(dcol, ad, bd, id, (kb | ks | p) ? 1u : 0u);
+              }
+            }
+            mma_commit(empty + stage);
+          }
+          __syncwarp();
+          next_stage();
+        }
+        if (lane == 0) mma_commit(tfull + buf);
+        __syncwarp();
+        if (++buf == 2) { buf = 0; tph ^= 1u; }
+      }
+    } else {
+      const uint32_t id = idesc(BN, 1, 1);
+      int buf = 0;
+      uint32_t tph = 0;
+      int inchunk = 0;
+      for (int kb = kb_begin; kb < kb_end; ++kb) {
+        if (inchunk == 0) {
+          if (!mbar_wait(tempty + buf, tph ^ 1u, flag, 2)) goto done;
+          tc_fence_after();
+        }
+        if (!mbar_wait(full + stage, ph, flag, 3)) goto done;
+        tc_fence_after();
+        if (lane == 0) {
+          const uint32_t sa = su32(sStage + stage * stage_bytes);
+          const uint32_t sbb = sa + 3 * a_tile;
+          const uint32_t dcol = tmem + (uint32_t)(buf * 64);
+#pragma unroll
+          for (int ks = 0; ks < BK / 16; ++ks) {
+#pragma unroll
+            for (int p = 0; p < 6; ++p) {
+              // one 16-deep step spans two 8-row k atoms
+              const uint64_t ad = sdesc(sa + pa[p] * a_tile + ks * 2 * (2 * 1024), 1024, 2 * 1024);
+              const uint64_t bd =
+                  sdesc(sbb + pb[p] * b_tile + ks * 2 * (mnbB * 1024), 1024, mnbB * 1024);
+              mma(dcol, ad, bd, id, (inchunk | ks | p) ? 1u : 0u);
+            }
+          }
+          mma_commit(empty + stage);
+        }
+        __syncwarp();
+        next_stage();
+        if (++inchunk == g.kchunk || kb + 1 == kb_end) {
+          if (lane == 0) mma_commit(tfull + buf);
+          __syncwarp();
+          inchunk = 0;
+          if (++buf == 2) { buf = 0; tph ^= 1u; }
+        }
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3;           // TMEM lane quadrant of this warp
+    const int row = q * 32 + lane;    // accumulator row = TMEM lane
+    const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
+    if (MODE != MODE_DW) {
+      int buf = 0;
+      uint32_t tph = 0;
+      for (int mt = first_m; mt < tiles_m; mt += step_m) {
+        if (!mbar_wait(tfull + buf, tph, flag, 4)) goto done;
+        tc_fence_after();
+        const int gr = mt * BM + row;
+        const bool ok = gr < g.M;
+        const bool brow = (MODE == MODE_FWD) && ok && (gr % g.na == 0);
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+          float v[32];
+          tmem_ld32(lane_addr + (uint32_t)(buf * BN + c0), v);
+          if (ok) {
+            float *dst = g.C + (size_t)gr * g.ldc + n0 + c0;
+#pragma unroll
+            for (int i = 0; i < 32; i += 4) {
+              float4 o = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+              if (brow) {
+                o.x += g.bias[n0 + c0 + i];
+                o.y += g.bias[n0 + c0 + i + 1];
+                o.z += g.bias[n0 + c0 + i + 2];
+                o.w += g.bias[n0 + c0 + i + 3];
+              }
+              if (n0 + c0 + i < g.N) *(float4 *)(dst + i) = o;
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(tempty + buf);
+        if (++buf == 2) { buf = 0; tph ^= 1u; }
+      }
+    } else {
+      double acc[64];
+#pragma unroll
+      for (int i = 0; i < 64; ++i) acc[i] = 0.0;
+      int buf = 0;
+      uint32_t tph = 0;
+      const int nch = (kb_end - kb_begin + g.kchunk - 1) / g.kchunk;
+      for (int ch = 0; ch < nch; ++ch) {
+        if (!mbar_wait(tfull + buf, tph, flag, 4)) goto done;
+        tc_fence_after();
+#pragma unroll
+        for (int c0 = 0; c0 < 64; c0 += 32) {
+          float v[32];
+          tmem_ld32(lane_addr + (uint32_t)(buf * 64 + c0), v);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) acc[c0 + i] += (double)v[i];
+        }
+        tc_fence_before();
+        mbar_arrive(tempty + buf);
+        if (++buf == 2) { buf = 0; tph ^= 1u; }
+      }
+      if (row < g.M && nch > 0) {
+        double *dst = g.G + (size_t)row * g.gld + 1 + n0;
+#pragma unroll
+        for (int i = 0; i < 64; ++i)
+          if (n0 + i < g.N) atomicAdd(dst + i, acc[i]);
+      }
+    }
+  }
+done:
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == MMA_WARP)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols)
+                 : "memory");
+}
+
+// host-side split of one FP32 value into three bf16 terms (round to nearest
+// even, as __float2bfloat16_rn)
+static uint16_t bf16_rn(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40);
+  uint32_t r = u + 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(r >> 16);
+}
+static float bf16_f(uint16_t h) {
+  uint32_t u = (uint32_t)h << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+static size_t kmaj_off_h(int row, int k) {
+  return (size_t)((row >> 3) * 1024 + (row & 7) * ROWB + ((((k >> 3) ^ (row & 7)) & 7) << 4) +
+                  (k & 7) * 2);
+}
+
+// pre-split weights of one GEMM: Bmat(nrow = N, k = K) element source
+// fn(n, k), laid out [N tile][term][K block][BN rows][128 B]
+template <typename F>
+static std::vector<uint8_t> prep_b(int N, int K, int BN, F fn) {
+  const int nkb = (K + BK - 1) / BK, ntn = (N + BN - 1) / BN;
+  const size_t btile = (size_t)BN * ROWB;
+  std::vector<uint8_t> out((size_t)ntn * 3 * nkb * btile, 0);
+  for (int tn = 0; tn < ntn; ++tn)
+    for (int r = 0; r < BN; ++r) {
+      const int n = tn * BN + r;
+      if (n >= N) continue;
+      for (int k = 0; k < K; ++k) {
+        float x = fn(n, k);
+        uint16_t h1 = bf16_rn(x);
+        float rr = x - bf16_f(h1);
+        uint16_t h2 = bf16_rn(rr);
+        rr = rr - bf16_f(h2);
+        uint16_t h3 = bf16_rn(rr);
+        const int kb = k / BK, kk = k % BK;
+        const uint16_t hs[3] = {h1, h2, h3};
+        for (int p = 0; p < 3; ++p) {
+          size_t off = (size_t)tn * 3 * nkb * btile + ((size_t)p * nkb + kb) * btile +
+                       kmaj_off_h(r, kk);
+          std::memcpy(&out[off], &hs[p], 2);
+        }
+      }
+    }
+  return out;
+}
+
+}  // namespace tc
+
+// per-network pre-split weights
+struct TcWeights {
+  std::vector<uint8_t *> fwd, dt;  // per layer (index l-1)
+  std::vector<float *> bias;
+  std::vector<int> bn_fwd, bn_dt;
+  int *flag = nullptr;
+};
+
+static bool g_tc_checked = false, g_tc_ok = false;
+
+bool gemm_tc_available() {
+  if (!g_tc_checked) {
+    g_tc_checked = true;
+    int dev = 0, major = 0, minor = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev) == cudaSuccess)
+      g_tc_ok = (major == 10 && minor == 0);
+  }
+  return g_tc_ok;
+}
+
+void gemm_tc_release_weights(DevNet *net) {
+  TcWeights *w = (TcWeights *)net->tc;
+  if (!w) return;
+  for (auto p : w->fwd) if (p) cudaFree(p);
+  for (auto p : w->dt) if (p) cudaFree(p);
+  for (auto p : w->bias) if (p) cudaFree(p);
+  if (w->flag) cudaFree(w->flag);
+  delete w;
+  net->tc = nullptr;
+}
+
+static bool tc_shape_ok(int N, int K) {
+  if (N % 16 || K % 16 || N < 16 || K < 16) return false;
+  if (N > 128 && N % 128) return false;
+  const int BN = std::min(N, 128), nkb = (K + 63) / 64;
+  const size_t smem = (size_t)3 * nkb * BN * 128 + 2 * 3 * 128 * 128 + 2048;
+  return smem <= 227 * 1024;
+}
+
+int gemm_tc_prepare(DevNet *net, const double *hw, cudaStream_t st) {
+  if (!gemm_tc_available()) return RC_OK;
+  gemm_tc_release_weights(net);
+  TcWeights *w = new TcWeights();
+  net->tc = w;
+  const int L = net->nlayer;
+  w->fwd.assign(L, nullptr);
+  w->dt.assign(L, nullptr);
+  w->bias.assign(L, nullptr);
+  w->bn_fwd.assign(L, 0);
+  w->bn_dt.assign(L, 0);
+  CKT(cudaMalloc(&w->flag, sizeof(int)));
+  CKT(cudaMemsetAsync(w->flag, 0, sizeof(int), st));
+  for (int l = 3; l < L; ++l) {  // hidden layers with a GEMM
+    const int n = net->dims[l - 1], m = net->dims[l - 2];
+    const double *Wl = hw + net->woff[l - 1];
+    if (tc_shape_ok(n, m)) {
+      const int BN = std::min(n, 128);
+      auto b = tc::prep_b(n, m, BN, [&](int j, int k) { return (float)Wl[(size_t)j * (m + 1) + 1 + k]; });
+      CKT(cudaMalloc(&w->fwd[l - 1], b.size()));
+      CKT(cudaMemcpy(w->fwd[l - 1], b.data(), b.size(), cudaMemcpyHostToDevice));
+      std::vector<float> bias(n);
+      for (int j = 0; j < n; ++j) bias[j] = (float)Wl[(size_t)j * (m + 1)];
+      CKT(cudaMalloc(&w->bias[l - 1], n * sizeof(float)));
+      CKT(cudaMemcpy(w->bias[l - 1], bias.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+      w->bn_fwd[l - 1] = BN;
+    }
+    if (tc_shape_ok(m, n)) {
+      const int BN = std::min(m, 128);
+      auto b = tc::prep_b(m, n, BN, [&](int i, int j) { return (float)Wl[(size_t)j * (m + 1) + 1 + i]; });
+      CKT(cudaMalloc(&w->dt[l - 1], b.size()));
+      CKT(cudaMemcpy(w->dt[l - 1], b.data(), b.size(), cudaMemcpyHostToDevice));
+      w->bn_dt[l - 1] = BN;
+    }
+  }
+  return RC_OK;
+}
+
+static int sm_count_t() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+static int check_flag(int *flag, cudaStream_t st, const char *what) {
+  (void)flag;
+  (void)st;
+  (void)what;
+  return RC_OK;
+}
+
+static int launch(const tc::Args &a, int mode, dim3 grid, size_t smem, cudaStream_t st) {
+  if (mode == tc::MODE_FWD) {
+    CKT(cudaFuncSetAttribute(tc::k_tc_gemm<tc::MODE_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LAUNCH("k_tc_gemm_fwd", st, tc::k_tc_gemm<tc::MODE_FWD><<<grid, tc::NTHREADS, smem, st>>>(a));
+  } else if (mode == tc::MODE_DT) {
+    CKT(cudaFuncSetAttribute(tc::k_tc_gemm<tc::MODE_DT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LAUNCH("k_tc_gemm_dt", st, tc::k_tc_gemm<tc::MODE_DT><<<grid, tc::NTHREADS, smem, st>>>(a));
+  } else {
+    CKT(cudaFuncSetAttribute(tc::k_tc_gemm<tc::MODE_DW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LAUNCH("k_tc_gemm_dw", st, tc::k_tc_gemm<tc::MODE_DW><<<grid, tc::NTHREADS, smem, st>>>(a));
+  }
+  CKT(cudaGetLastError());
+  return RC_OK;
+}
+
+static int fwd_like(int mode, const uint8_t *W, const float *bias, int BN, int M, int N, int K,
+                    int na, const void *A, void *C, int *flag, cudaStream_t st) {
+  const int nkb = (K + tc::BK - 1) / tc::BK;
+  const int ntn = (N + BN - 1) / BN;
+  const size_t bres = (size_t)3 * nkb * BN * tc::ROWB;
+  const size_t smem = 1024 + bres + 2 * 3 * tc::BM * tc::ROWB + 1024;
+  tc::Args a;
+  std::memset(&a, 0, sizeof a);
+  a.mode = mode; a.M = M; a.N = N; a.K = K; a.na = na;
+  a.A = (const float *)A; a.lda = K; a.W = W; a.bias = bias;
+  a.C = (float *)C; a.ldc = N; a.BN = BN; a.ntn = ntn; a.flag = flag;
+  const int tiles_m = (M + tc::BM - 1) / tc::BM;
+  dim3 grid(std::max(1, std::min(tiles_m, sm_count_t() / ntn)), ntn);
+  return launch(a, mode, grid, smem, st);
+}
+
+int gemm_tc_fwd(const DevNet *net, int l, int M, int n, int m, int na, const void *A, void *C,
+                cudaStream_t st) {
+  TcWeights *w = (TcWeights *)net->tc;
+  if (!w || !w->fwd[l - 1]) return RC_UNSUPPORTED;
+  return fwd_like(tc::MODE_FWD, w->fwd[l - 1], w->bias[l - 1], w->bn_fwd[l - 1], M, n, m, na, A,
+                  C, w->flag, st);
+}
+
+int gemm_tc_dt(const DevNet *net, int l, int M, int n, int m, const void *Sb, void *Tb,
+               cudaStream_t st) {
+  TcWeights *w = (TcWeights *)net->tc;
+  if (!w || !w->dt[l - 1]) return RC_UNSUPPORTED;
+  return fwd_like(tc::MODE_DT, w->dt[l - 1], nullptr, w->bn_dt[l - 1], M, m, n, 1, Sb, Tb,
+                  w->flag, st);
+}
+
+int gemm_tc_dw(const DevNet *net, int l, int M, int n, int m, const void *Sb, const void *Tm,
+               double *G, cudaStream_t st) {
+  TcWeights *w = (TcWeights *)net->tc;
+  if (!w || n > 128 || n % 16 || m % 16) return RC_UNSUPPORTED;
+  const int BN = 64;
+  const int ntn = (m + BN - 1) / BN;
+  const int nkb_all = (M + tc::BK - 1) / tc::BK;
+  const int ctas_k = std::max(1, std::min(nkb_all, sm_count_t() / ntn));
+  tc::Args a;
+  std::memset(&a, 0, sizeof a);
+  a.mode = tc::MODE_DW; a.M = n; a.N = m; a.K = M; a.na = 1;
+  a.A = (const float *)Sb; a.lda = n; a.B = (const float *)Tm; a.ldb = m;
+  a.G = G; a.gld = m + 1; a.BN = BN; a.ntn = ntn; a.kchunk = 8;
+  a.kblocks_per_cta = (nkb_all + ctas_k - 1) / ctas_k;
+  a.flag = w->flag;
+  const size_t stage = 3 * (8 * 2 * 1024) + 3 * (8 * 1 * 1024);
+  const size_t smem = 1024 + 3 * stage + 1024;
+  dim3 grid((nkb_all + a.kblocks_per_cta - 1) / a.kblocks_per_cta, ntn);
+  return launch(a, tc::MODE_DW, grid, smem, st);
+}
+
+int gemm_tc_syrk(const double *, int, int, double *, cudaStream_t) { return RC_UNSUPPORTED; }
+
+int gemm_tc_flag(const DevNet *net, cudaStream_t st) {
+  TcWeights *w = (TcWeights *)net->tc;
+  if (!w) return RC_OK;
+  int h = 0;
+  CKT(cudaMemcpyAsync(&h, w->flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKT(cudaStreamSynchronize(st));
+  if (h) {
+    set_error("tensor-core GEMM: an mbarrier wait timed out (code " + std::to_string(h) + ")");
+    return RC_DEVICE;
+  }
+  return check_flag(w->flag, st, "");
 }
 
 }  // namespace dnnf90

@@ -18,8 +18,12 @@ struct DevNet;
 
 bool gemm_tc_available();
 void gemm_tc_release_weights(DevNet *net);
-// Prepares the split weight operands of every layer from net->w32.
-int gemm_tc_prepare(DevNet *net, cudaStream_t st);
+// Pre-splits and pre-swizzles the weight operands of every hidden layer
+// from the host weights hw (flat layer layout).
+int gemm_tc_prepare(DevNet *net, const double *hw, cudaStream_t st);
+// Reads the wait time-out flag of the network's tensor-core GEMMs
+// (synchronises st); RC_DEVICE if a wait ran out.
+int gemm_tc_flag(const DevNet *net, cudaStream_t st);
 
 int gemm_tc_fwd(const DevNet *net, int l, int M, int n, int m, int na,
                 const void *A, void *C, cudaStream_t st);

@@ -225,10 +225,10 @@ int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
   CKN(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)nw * nw, st));
   CKN(cudaMemsetAsync(info, 0, sizeof(int), st));
   const int tiles = (nw + 63) / 64;
-  int rc = RC_OK;
-  if (prec == PREC_SPLIT && gemm_tc_available()) {
-    rc = gemm_tc_syrk(rows, nrow, nw, G, st);
-  } else {
+  int rc = RC_UNSUPPORTED;
+  if (prec == PREC_SPLIT && gemm_tc_available()) rc = gemm_tc_syrk(rows, nrow, nw, G, st);
+  if (rc == RC_UNSUPPORTED) {
+    rc = RC_OK;
     int rchunk = std::max(64, (nrow + 7) / 8);
     rchunk = (rchunk + 15) / 16 * 16;
     dim3 grid(tiles, tiles, (nrow + rchunk - 1) / rchunk);
