@@ -30,7 +30,8 @@ namespace dnnf90 {
 
 void DevBellPlan::release() {
   void *ps[] = {fw_list, fw_arec, fw_grec, fw_gc64, fw_gc32, aj_list, aj_orec, aj_pair,
-                aj_c64, aj_c32};
+                aj_c64, aj_c32, f3_list, f3_arec, f3_grec, f3_gc64, f3_gc32, a3_orec,
+                a3_pair, sc64, sc32, f4_grec, a4_pair};
   for (void *p : ps)
     if (p) cudaFree(p);
   *this = DevBellPlan();
@@ -64,6 +65,31 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
   if ((rc = put(&d.aj_pair, P.aj_pair))) return rc;
   if ((rc = put(&d.aj_c64, P.aj_c))) return rc;
   if ((rc = put(&d.aj_c32, ac32))) return rc;
+  std::vector<float> g3(P.f3_gc.begin(), P.f3_gc.end());
+  if ((rc = put(&d.f3_list, P.f3_list))) return rc;
+  if ((rc = put(&d.f3_arec, P.f3_arec))) return rc;
+  if ((rc = put(&d.f3_grec, P.f3_grec))) return rc;
+  if ((rc = put(&d.f3_gc64, P.f3_gc))) return rc;
+  if ((rc = put(&d.f3_gc32, g3))) return rc;
+  if ((rc = put(&d.a3_orec, P.a3_orec))) return rc;
+  if ((rc = put(&d.a3_pair, P.a3_pair))) return rc;
+  if ((rc = put(&d.f4_grec, P.f4_grec))) return rc;
+  std::vector<uint32_t> a4(P.a4_pair);
+  for (int i = 0; i < 4; ++i) a4.push_back(0);
+  if ((rc = put(&d.a4_pair, a4))) return rc;
+  d.nuv = P.nuv;
+  std::vector<double> sc(3 * (size_t)P.na);
+  for (int i = 0; i < P.na; ++i) {
+    sc[i] = P.fact[i];
+    sc[P.na + i] = 1.0 / P.fact[i];
+    sc[2 * P.na + i] = 1.0 / P.fact[i];
+  }
+  std::vector<float> sc32(sc.begin(), sc.end());
+  if ((rc = put(&d.sc64, sc))) return rc;
+  if ((rc = put(&d.sc32, sc32))) return rc;
+  d.f3_ok = P.f3_ok;
+  d.nrows = P.nrows;
+  d.dt_off = P.dt_off;
   d.ready = true;
   return RC_OK;
 }
@@ -233,6 +259,278 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj2(Adj2Args a) {
   if (a.gbias && act && gb != 0.0) atomicAdd(a.gbias + (size_t)j * a.gstride, gb);
 }
 
+
+// ---------------------------------------------------------------- v3
+struct Fwd3Args {
+  int n, na, npts, iact, dt_off, nrows, nuv;
+  const double *tpc;
+  const int *list;
+  const int4 *arec;
+  const uint32_t *grec;
+  const void *sc;  // [0, na): a!, [na, 2na): 1/a!
+  const void *S;
+  void *T, *h;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+// 16-byte asynchronous copy global -> shared; src_bytes < 16 zero-fills
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Rows [0, nr) of a [na][n] plane slice (neurons j0..j0+NPB-1, 128 bytes a
+// row) copied into shared rows dst[r * 128]; columns at or beyond n fill
+// with zeros.  n is a multiple of 4, so every 16-byte piece is either
+// wholly inside the row or wholly outside it.
+template <int NPB, typename R>
+__device__ __forceinline__ void stage_rows(unsigned char *dst, const R *src, int nr, int n,
+                                           int j0, int nthreads) {
+  constexpr int PER = 16 / sizeof(R);  // values per 16-byte piece
+  for (int c = threadIdx.x; c < nr * 8; c += nthreads) {
+    const int r = c >> 3, piece = c & 7;
+    const int col = j0 + piece * PER;
+    const int ok = col < n ? 16 : 0;
+    const R *g = src + (size_t)r * n + (ok ? col : 0);
+    cp_async16(dst + r * 128 + piece * 16, g, ok);
+  }
+}
+
+// One state row is 128 bytes: NPB lanes x sizeof(R).  Row r of this lane
+// is at  base + r * 128,  base = smem + lane * sizeof(R).  The S rows of
+// the point being computed sit at rows [0, na) or, for the other buffer,
+// [nrows, nrows + na): the next point's S streams into one buffer while
+// the other is read.
+template <typename R, int KK, int NPB, bool TRAIN>
+__global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool lact = lane < NPB;
+  const int ln = lact ? lane : 0;
+  const int j0 = blockIdx.y * NPB;
+  const int j = j0 + ln;
+  const bool act = lact && j < a.n;
+  const int n = a.n;
+  const size_t plane = (size_t)a.na * n;
+  unsigned char *base = smem_raw + ln * sizeof(R);
+#define ROWV(off) (*(R *)(base + (off)))
+#define ROWS(off) (*(R *)(sbase + (off)))
+  const R *sc = (const R *)a.sc;
+  const int sbuf1 = a.nrows * 128;
+  int buf = 0;
+  if (blockIdx.x < a.npts)
+    stage_rows<NPB, R>(smem_raw, (const R *)a.S + blockIdx.x * plane, a.na, n, j0, BELL_WORKERS * 32);
+  cp_async_commit();
+  for (int pt = blockIdx.x; pt < a.npts; pt += gridDim.x) {
+    const int nxt = pt + gridDim.x;
+    if (nxt < a.npts)
+      stage_rows<NPB, R>(smem_raw + (buf ? 0 : sbuf1), (const R *)a.S + nxt * plane, a.na, n, j0,
+                         BELL_WORKERS * 32);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    unsigned char *sbase = base + (buf ? sbuf1 : 0);
+    // normalise: row b of S becomes S_b / b!  (row 0 keeps S_0)
+    for (int ia = warp; ia < a.na; ia += BELL_WORKERS)
+      if (lact) ROWS(ia * 128) *= __ldg(sc + a.na + ia);
+    __syncthreads();
+    R *T = (R *)a.T + pt * plane;
+    R *H = TRAIN ? (R *)a.h + pt * plane : nullptr;
+    if (warp == 0 && lact) {
+      double d[KK + 2];
+      sigma_derivs(a.iact, a.tpc, KK, (double)ROWS(0), d);
+#pragma unroll
+      for (int q = 0; q <= KK + 1; ++q) ROWV(a.dt_off + q * 128) = (R)d[q];
+      if (act) {
+        T[j] = (R)d[0];
+        if (TRAIN) H[j] = (R)d[1];
+      }
+    }
+    __syncthreads();
+    R dt[KK + 2];
+#pragma unroll
+    for (int q = 0; q <= KK + 1; ++q) dt[q] = ROWV(a.dt_off + q * 128);
+    R uc[KK + 1], vc[KK + 1];
+#pragma unroll
+    for (int q = 1; q < KK; ++q) {
+      uc[q] = dt[q + 1] * (R)(1.0 / (q + 1));
+      vc[q] = dt[q + 2] * (R)(1.0 / (q + 1));
+    }
+    for (int p = 1; p <= KK; ++p) {
+      const int rs = __ldg(a.list + (p * BELL_WORKERS + warp) * 2);
+      const int rn = __ldg(a.list + (p * BELL_WORKERS + warp) * 2 + 1);
+      for (int r = rs; r < rs + rn; ++r) {
+        const int4 A0 = __ldg(a.arec + 2 * r), A1 = __ldg(a.arec + 2 * r + 1);
+        const int ia = A0.x & 0xffff;
+        const R sa = ROWS(ia * 128);
+        const R fa = __ldg(sc + ia);
+        const int gs = A0.y, ge = A0.y + A0.z;
+        if (p == KK) {
+          // top degree: T_a / a! = s' S~_a + sum_b S~_b U~_{a-b}, likewise h with V~
+          R tt = dt[1] * sa, hh = dt[2] * sa;
+          const int voff = a.nuv * 128;
+          for (int g0 = gs; g0 < ge; g0 += BELL_UNROLL) {
+            uint32_t gr[BELL_UNROLL];
+#pragma unroll
+            for (int u = 0; u < BELL_UNROLL; ++u) gr[u] = __ldg(a.grec + min(g0 + u, ge - 1));
+#pragma unroll
+            for (int u = 0; u < BELL_UNROLL; ++u)
+              if (g0 + u < ge) {
+                const R x = ROWS((gr[u] & 0x3ffu) << 7);
+                const int uo = (int)(gr[u] >> 10) << 7;
+                tt += x * ROWV(uo);
+                hh += x * ROWV(uo + voff);
+              }
+          }
+          if (act) {
+            T[(size_t)ia * n + j] = fa * tt;
+            if (TRAIN) H[(size_t)ia * n + j] = fa * hh;
+          }
+          continue;
+        }
+        R acc[KK + 1];
+#pragma unroll
+        for (int q = 0; q <= KK; ++q) acc[q] = (R)0;
+        const uint64_t bands = ((uint64_t)(uint32_t)A0.w << 32) | (uint32_t)A1.w;
+        int g = gs;
+        // the next record is fetched while the current one is applied
+        uint32_t nr = __ldg(a.grec + min(g, max(ge - 1, 0)));
+#pragma unroll
+        for (int d = KK - 1; d >= 1; --d) {
+          if (d < p) {
+            const int cnt = (int)((bands >> (8 * (d - 1))) & 0xffu);
+            for (int e = 0; e < cnt; ++e, ++g) {
+              const uint32_t gr = nr;
+              nr = __ldg(a.grec + min(g + 1, ge - 1));
+              const R x = ROWS((gr & 0x3ffu) << 7);
+              acc[2] += x * ROWS(((gr >> 10) & 0x3ffu) << 7);
+              const int zo = (int)(gr >> 20) << 7;
+#pragma unroll
+              for (int q = 3; q <= d + 1; ++q) acc[q] += x * ROWV(zo + (q - 3) * 128);
+            }
+          }
+        }
+        R tt = dt[1] * sa, hh = dt[2] * sa, uu = uc[1] * sa, vv = vc[1] * sa;
+#pragma unroll
+        for (int q = 2; q < KK; ++q) {
+          if (q <= p) {
+            const R b = acc[q] * (R)(1.0 / q);
+            if (A1.x >= 0 && lact) ROWV(A1.x + (q - 2) * 128) = b;
+            tt += dt[q] * b;
+            hh += dt[q + 1] * b;
+            uu += uc[q] * b;
+            vv += vc[q] * b;
+          }
+        }
+        if (A1.y >= 0 && lact) {
+          ROWV(A1.y) = uu;
+          ROWV(A1.z) = vv;
+        }
+        if (act) {
+          T[(size_t)ia * n + j] = fa * tt;
+          if (TRAIN) H[(size_t)ia * n + j] = fa * hh;
+        }
+      }
+      __syncthreads();
+    }
+    buf ^= 1;
+  }
+  cp_async_wait<0>();
+#undef ROWS
+#undef ROWV
+}
+
+struct Adj3Args {
+  int n, na, npts, gstride;
+  const int *list;
+  const int4 *orec;
+  const uint32_t *pair;  // Tb row | h row << 16
+  const void *sc;  // [3][na]
+  const void *Tb, *h;
+  void *Sb;
+  double *gbias;
+};
+
+// Bell adjoint as a correlation: Sb_b b! = sum_{a >= b} (a! Tb_a)(h_{a-b}/(a-b)!).
+// Shared memory holds two buffers of [Tb rows | h rows]; the next point's
+// rows stream into one while the other is scaled and read.
+template <typename R, int NPB>
+__global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj3(Adj3Args a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool lact = lane < NPB;
+  const int ln = lact ? lane : 0;
+  const int j0 = blockIdx.y * NPB;
+  const int j = j0 + ln;
+  const bool act = lact && j < a.n;
+  const int n = a.n, na = a.na;
+  const size_t plane = (size_t)na * n;
+  const int bufb = 2 * na * 128;  // bytes per buffer
+  const R *sc = (const R *)a.sc;
+  const int rs = __ldg(a.list + warp * 2), rn = __ldg(a.list + warp * 2 + 1);
+  double gb = 0.0;
+  int buf = 0;
+  if (blockIdx.x < a.npts) {
+    stage_rows<NPB, R>(smem_raw, (const R *)a.Tb + blockIdx.x * plane, na, n, j0, ADJ_WORKERS * 32);
+    stage_rows<NPB, R>(smem_raw + na * 128, (const R *)a.h + blockIdx.x * plane, na, n, j0,
+                       ADJ_WORKERS * 32);
+  }
+  cp_async_commit();
+  for (int pt = blockIdx.x; pt < a.npts; pt += gridDim.x) {
+    const int nxt = pt + gridDim.x;
+    unsigned char *cur = smem_raw + buf * bufb;
+    if (nxt < a.npts) {
+      unsigned char *oth = smem_raw + (buf ^ 1) * bufb;
+      stage_rows<NPB, R>(oth, (const R *)a.Tb + nxt * plane, na, n, j0, ADJ_WORKERS * 32);
+      stage_rows<NPB, R>(oth + na * 128, (const R *)a.h + nxt * plane, na, n, j0, ADJ_WORKERS * 32);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    // scale: row a of Tb by a!, row g of h by 1/g!
+    for (int r = warp; r < 2 * na; r += ADJ_WORKERS)
+      if (lact) *(R *)(cur + r * 128 + lane * sizeof(R)) *= __ldg(sc + r);
+    __syncthreads();
+    unsigned char *base = cur + ln * sizeof(R);
+    R *Sb = (R *)a.Sb + pt * plane;
+    for (int r = rs; r < rs + rn; ++r) {
+      const int4 o = __ldg(a.orec + r);  // ib, pstart, pcount
+      R s0 = (R)0, s1 = (R)0;
+      const int pe = o.y + o.z;
+      for (int ip = o.y; ip < pe; ip += 4) {
+        uint32_t pk[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) pk[u] = __ldg(a.pair + min(ip + u, pe - 1));
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (ip + u < pe) {
+            const R v = *(const R *)(base + ((pk[u] & 0xffffu) << 7)) *
+                        *(const R *)(base + ((pk[u] >> 16) << 7));
+            if (u & 1) s1 += v;
+            else s0 += v;
+          }
+      }
+      const R s = (s0 + s1) * __ldg(sc + 2 * na + o.x);
+      if (act) Sb[(size_t)o.x * n + j] = s;
+      if (o.x == 0) gb += (double)s;
+    }
+    __syncthreads();
+    buf ^= 1;
+  }
+  cp_async_wait<0>();
+  if (a.gbias && act && gb != 0.0) atomicAdd(a.gbias + (size_t)j * a.gstride, gb);
+}
+
 static int sm_count_b() {
   static int n = 0;
   if (!n) {
@@ -245,8 +543,43 @@ static int sm_count_b() {
 }
 
 template <typename R, int KK>
+static int fwd3_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int npts,
+                         const void *S, void *T, void *h, bool train, cudaStream_t st) {
+  constexpr int NPB = sizeof(R) == 8 ? 16 : 32;
+  static_assert(NPB * sizeof(R) == 128, "one state row is 128 bytes");
+  const size_t smem = ((size_t)bp.nrows + t.na) * 128;
+  if (!bp.f3_ok || smem > 227 * 1024 || n % (16 / (int)sizeof(R))) return RC_UNSUPPORTED;
+  Fwd3Args a;
+  a.n = n; a.na = t.na; a.npts = npts; a.iact = t.iact; a.dt_off = bp.dt_off;
+  a.nrows = bp.nrows;
+  a.tpc = t.tpc; a.list = bp.f3_list; a.arec = (const int4 *)bp.f3_arec;
+  a.grec = bp.f4_grec; a.nuv = bp.nuv;
+  a.sc = sizeof(R) == 8 ? (const void *)bp.sc64 : (const void *)bp.sc32;
+  a.S = S; a.T = T; a.h = h;
+  const int gy = (n + NPB - 1) / NPB;
+  const int per_sm = std::max(1, (int)((228 * 1024) / (smem + 1024)));
+  const int gx = std::max(1, std::min(npts, sm_count_b() * per_sm / gy + 1));
+  dim3 grid(gx, gy);
+  if (train) {
+    auto k = k_bell_fwd3<R, KK, NPB, true>;
+    CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LAUNCH("k_bell_fwd", st, k<<<grid, BELL_WORKERS * 32, smem, st>>>(a));
+  } else {
+    auto k = k_bell_fwd3<R, KK, NPB, false>;
+    CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LAUNCH("k_bell_fwd", st, k<<<grid, BELL_WORKERS * 32, smem, st>>>(a));
+  }
+  CKB(cudaGetLastError());
+  return RC_OK;
+}
+
+template <typename R, int KK>
 static int fwd2_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int npts,
                          const void *S, void *T, void *h, bool train, cudaStream_t st) {
+  {
+    int rc3 = fwd3_dispatch<R, KK>(bp, t, n, npts, S, T, h, train, st);
+    if (rc3 != RC_UNSUPPORTED) return rc3;
+  }
   constexpr int NPB = sizeof(R) == 8 ? 16 : 32;
   const size_t smem = ((size_t)t.na + bp.nslot + KK + 2) * NPB * sizeof(R);
   if (smem > 227 * 1024) return RC_UNSUPPORTED;
@@ -302,6 +635,22 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
   constexpr int NPB = sizeof(R) == 8 ? 16 : 32;
   const size_t smem = (size_t)2 * t.na * NPB * sizeof(R);
   if (smem > 227 * 1024) return RC_UNSUPPORTED;
+  if (bp.a3_orec && (size_t)4 * t.na * 128 <= 227 * 1024 && n % (16 / (int)sizeof(R)) == 0) {
+    const size_t smem3 = (size_t)4 * t.na * 128;
+    Adj3Args b;
+    b.n = n; b.na = t.na; b.npts = npts; b.gstride = gstride; b.list = bp.aj_list;
+    b.orec = (const int4 *)bp.a3_orec; b.pair = bp.a4_pair;
+    b.sc = sizeof(R) == 8 ? (const void *)bp.sc64 : (const void *)bp.sc32;
+    b.Tb = Tb; b.h = h; b.Sb = Sb; b.gbias = gbias;
+    const int gy = (n + NPB - 1) / NPB;
+    const int per_sm = std::max(1, (int)((228 * 1024) / (smem3 + 1024)));
+    const int gx = std::max(1, std::min(npts, sm_count_b() * per_sm / gy + 1));
+    auto k = k_bell_adj3<R, NPB>;
+    CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
+    LAUNCH("k_bell_adj", st, k<<<dim3(gx, gy), ADJ_WORKERS * 32, smem3, st>>>(b));
+    CKB(cudaGetLastError());
+    return RC_OK;
+  }
   Adj2Args a;
   a.n = n; a.na = t.na; a.npts = npts; a.gstride = gstride; a.list = bp.aj_list;
   a.orec = (const int4 *)bp.aj_orec; a.pair = bp.aj_pair;

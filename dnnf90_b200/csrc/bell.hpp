@@ -10,7 +10,7 @@ struct DevTables;
 
 constexpr int BELL_WORKERS = 32;  // warps per block sharing one point's state
 constexpr int BELL_UNROLL = 4;    // table records fetched ahead per step
-constexpr int ADJ_WORKERS = 16;   // warps per block of the adjoint
+constexpr int ADJ_WORKERS = 32;   // warps per block of the adjoint
 constexpr int ADJ_UNROLL = 2;     // pairs fetched ahead: 2 * ADJ_UNROLL
 
 struct DevBellPlan {
@@ -22,6 +22,17 @@ struct DevBellPlan {
   int *aj_list = nullptr, *aj_orec = nullptr, *aj_pair = nullptr;
   double *aj_c64 = nullptr;
   float *aj_c32 = nullptr;
+  // v3
+  bool f3_ok = false;
+  int nrows = 0, dt_off = 0;
+  int *f3_list = nullptr, *f3_arec = nullptr, *f3_grec = nullptr;
+  double *f3_gc64 = nullptr;
+  float *f3_gc32 = nullptr;
+  int *a3_orec = nullptr, *a3_pair = nullptr;
+  uint32_t *f4_grec = nullptr, *a4_pair = nullptr;
+  int nuv = 0;
+  double *sc64 = nullptr;  // [3][na]: a!, 1/a!, 1/a! (Tb, h, Sb scales)
+  float *sc32 = nullptr;
   void release();
 };
 

@@ -87,6 +87,114 @@ BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
     }
   }
 
+  // ---- forward v3.  T_a = sum_q s^(q) B_{a,q} regrouped by b (0 < b < a):
+  //   T_a = s' S_a + sum_b C(a,b) S_b U_{a-b},  h_a = s'' S_a + sum_b C(a,b) S_b V_{a-b},
+  //   U_g = sum_{q=1}^{|g|} s^(q+1)/(q+1) B_{g,q},  V_g = sum s^(q+2)/(q+1) B_{g,q}
+  // (the q >= 2 terms of lib/train_module.f90:308-322 with the level index
+  // shifted).  The top degree uses it directly, so no Bell value of degree
+  // K-1 is kept; lower degrees run the recurrence, whose group of b reads
+  // every level of g = a - b (qmax = |g| + 1), so groups are banded by |g|.
+  {
+    const int ROW = 128;  // bytes per state row (NPB lanes x sizeof(R))
+    std::vector<int> b_off(na, -1), u_off(na, -1), v_off(na, -1);
+    int row = na;  // rows 0..na-1: S
+    for (int ia = 1; ia < na; ++ia)
+      if (t.deg[ia] >= 2 && t.deg[ia] <= k - 2) {
+        b_off[ia] = row * ROW;
+        row += t.deg[ia] - 1;
+      }
+    for (int ia = 1; ia < na; ++ia)
+      if (t.deg[ia] <= k - 1) u_off[ia] = (row++) * ROW;
+    P.nuv = 0;
+    for (int ia = 1; ia < na; ++ia)
+      if (t.deg[ia] <= k - 1) {
+        v_off[ia] = (row++) * ROW;
+        P.nuv++;
+      }
+    P.dt_off = row * ROW;
+    P.nrows = row + k + 2;
+    P.f3_list.assign((size_t)(k + 1) * workers * 2, 0);
+    for (int p = 1; p <= k; ++p) {
+      std::vector<int> items;
+      std::vector<long> cost;
+      for (int ia = 1; ia < na; ++ia)
+        if (t.deg[ia] == p) {
+          items.push_back(ia);
+          long c = 6;
+          const int st = p >= 2 ? t.fq_at(ia, 2) : 0, nn = p >= 2 ? t.fq_len(ia, 2) : 0;
+          for (int i = st; i < st + nn; ++i) c += p == k ? 3 : 2 + (p - t.deg[t.fq_ib[i]]);
+          cost.push_back(c);
+        }
+      auto asg = balance(cost, workers);
+      for (int w = 0; w < workers; ++w) {
+        P.f3_list[((size_t)p * workers + w) * 2] = (int)P.f3_arec.size() / 8;
+        P.f3_list[((size_t)p * workers + w) * 2 + 1] = (int)asg[w].size();
+        for (int it : asg[w]) {
+          const int ia = items[it];
+          const int gstart = (int)P.f3_grec.size() / 4;
+          uint64_t bands = 0;
+          if (p >= 2) {
+            const int st = t.fq_at(ia, 2), nn = t.fq_len(ia, 2);
+            std::vector<int> idx;
+            for (int i = st; i < st + nn; ++i) idx.push_back(i);
+            if (p < k)  // bands of |g| = d, longest first, slot order inside
+              std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+                return t.deg[t.fq_id[a]] > t.deg[t.fq_id[b]];
+              });
+            for (int i : idx) {
+              const int ib = t.fq_ib[i], g = t.fq_id[i];
+              P.f3_grec.push_back(ib * ROW);
+              P.f3_grec.push_back(g * ROW);
+              P.f3_grec.push_back(p == k ? u_off[g] : b_off[g]);
+              P.f3_grec.push_back(p == k ? v_off[g] : 0);
+              if (p == k)
+                P.f4_grec.push_back((uint32_t)ib | ((uint32_t)(u_off[g] / ROW) << 10));
+              else
+                P.f4_grec.push_back((uint32_t)ib | ((uint32_t)g << 10) |
+                                    ((uint32_t)(b_off[g] > 0 ? b_off[g] / ROW : 0) << 20));
+              P.f3_gc.push_back(t.fq_c[i] * 2.0);  // C(a,b)
+              if (p < k) bands += 1ull << (8 * (t.deg[g] - 1));
+            }
+          }
+          P.f3_arec.push_back(ia | (p << 16));
+          P.f3_arec.push_back(gstart);
+          P.f3_arec.push_back((int)P.f3_grec.size() / 4 - gstart);
+          P.f3_arec.push_back((int)(bands >> 32));
+          P.f3_arec.push_back(b_off[ia]);
+          P.f3_arec.push_back(u_off[ia]);
+          P.f3_arec.push_back(v_off[ia]);
+          P.f3_arec.push_back((int)(bands & 0xffffffffu));
+        }
+      }
+    }
+    P.f3_ok = k <= 8 && na <= 1023 && P.nrows <= 4095;
+    for (size_t r = 0; r < P.f3_arec.size(); r += 8) {
+      const int p = P.f3_arec[r] >> 16;
+      if (p < k && P.f3_arec[r + 2] > 0) {
+        // a band count above 255 would have carried into the next field
+        int total = 0;
+        const uint64_t b = ((uint64_t)(uint32_t)P.f3_arec[r + 3] << 32) | (uint32_t)P.f3_arec[r + 7];
+        for (int d = 1; d < p; ++d) total += (int)((b >> (8 * (d - 1))) & 0xff);
+        if (total != P.f3_arec[r + 2]) P.f3_ok = false;
+      }
+    }
+  }
+
+  // padding: the kernels prefetch the record after the last one of a list
+  for (int i = 0; i < 4; ++i) {
+    for (int c = 0; c < 4; ++c) P.f3_grec.push_back(0);
+    P.f3_gc.push_back(0.0);
+    P.f4_grec.push_back(0);
+  }
+
+  // ---- factorial scales of the adjoint v3 (records built with the lists below)
+  {
+    P.fact.assign(na, 1.0);
+    for (int ia = 0; ia < na; ++ia)
+      for (int i = 0; i < t.d0; ++i)
+        for (int v = 2; v <= t.alpha[(size_t)ia * t.d0 + i]; ++v) P.fact[ia] *= v;
+  }
+
   // adjoint outputs: Sb_0 (pairs (a, a) for every a) and every Sb_b, b >= 1
   std::vector<long> cost;
   std::vector<std::vector<std::pair<uint32_t, double>>> lists(na);
@@ -106,9 +214,17 @@ BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
       P.aj_orec.push_back((int)P.aj_pair.size());
       P.aj_orec.push_back((int)lists[ib].size());
       P.aj_orec.push_back(0);
+      P.a3_orec.push_back(ib);
+      P.a3_orec.push_back((int)P.a3_pair.size() / 2);
+      P.a3_orec.push_back((int)lists[ib].size());
+      P.a3_orec.push_back(0);
       for (auto &pr : lists[ib]) {
         P.aj_pair.push_back((int)pr.first);
         P.aj_c.push_back(pr.second);
+        // rows 0..na-1 hold a! Tb_a, rows na..2na-1 hold h_g / g!
+        P.a3_pair.push_back((int)(pr.first & 0xffffu) * 128);
+        P.a3_pair.push_back((na + (int)(pr.first >> 16)) * 128);
+        P.a4_pair.push_back((pr.first & 0xffffu) | ((uint32_t)(na + (pr.first >> 16)) << 16));
       }
     }
   }

@@ -27,6 +27,29 @@ struct BellPlan {
   std::vector<int> fw_grec;   // [*][4]: ib, g, gbase (state slot of B_{g,2}), qmax
   std::vector<double> fw_gc;  // C(a,b) per group
   std::vector<int> bbase;     // [na]: state slot of B_{a,2} (or -1)
+  // forward, v3 (top degree by the U/V convolution, banded groups, byte
+  // offsets into the shared-memory state; one state row = 128 bytes)
+  int nrows = 0;              // state rows: S | B | U | V | sigma
+  std::vector<int> f3_list;   // [(k+1) * workers][2]
+  std::vector<int> f3_arec;   // [*][8]: ia | p << 16, gstart, gcount, band_hi,
+                              //         b_off, u_off, v_off, band_lo
+  std::vector<int> f3_grec;   // [*][4]: s_b off, s_g off, B_g (or U_g) off, V_g off
+  std::vector<double> f3_gc;  // C(a,b)
+  int dt_off = 0;             // byte offset of the sigma rows
+  bool f3_ok = false;         // every band fits its 8-bit count
+  // forward v4: the same work lists over factorial-normalised state
+  // (rows hold S_b/b!, B_{a,q}/a!, U_g/g!, V_g/g!), so no coefficient is
+  // needed; one 32-bit record per group:
+  //   p < K : ib | g << 10 | (first row of the B run of g) << 20
+  //   p = K : ib | (U row of g) << 10         (V row = U row + nuv)
+  std::vector<uint32_t> f4_grec;
+  int nuv = 0;
+  // adjoint, v3: Sb_b b! = sum_{a >= b} (a! Tb_a) (h_{a-b} / (a-b)!), the
+  // pair coefficient C(a,b) = a!/(b!(a-b)!) folded into per-row scales
+  std::vector<int> a3_orec;   // [*][4]: ib, pstart, pcount, 0
+  std::vector<int> a3_pair;   // [*][2]: byte offsets of the Tb and h rows
+  std::vector<uint32_t> a4_pair;  // [*]: Tb row | h row << 16
+  std::vector<double> fact;   // a! per slot
   // adjoint
   std::vector<int> aj_list;   // [workers][2]
   std::vector<int> aj_orec;   // [*][4]: ib, pstart, pcount, 0
