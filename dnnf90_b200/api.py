@@ -43,6 +43,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_backward_dev", "dnnf90_grad_rule_dev", "dnnf90_jrow_dev",
     "dnnf90_twork_set_chunk", "dnnf90_last_error", "dnnf90_device_available",
     "dnnf90_launch_count", "dnnf90_profile_enable", "dnnf90_profile_read",
+    "dnnf90_ngd_step_noalloc",
 ]
 
 _lib = None
@@ -119,6 +120,7 @@ def lib():
         "dnnf90_launch_count": [],
         "dnnf90_profile_enable": [i],
         "dnnf90_profile_read": [ctypes.c_char_p, i],
+        "dnnf90_ngd_step_noalloc": [i, i, p, p, i, d, p, p],
     }
     for name, args in sig.items():
         f = getattr(L, name)

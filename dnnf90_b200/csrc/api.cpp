@@ -1146,6 +1146,14 @@ int dnnf90_jrow_dev(int nid, int tid, int npts, const double *x_dev, int rid,
   return run_batch(n.dt, n.dn, g_rule[rid].d, w.p, a, st);
 }
 
+int dnnf90_ngd_step_noalloc(int nrow, int nw, const double *rows_dev, const double *b_dev,
+                            int nb, double mu, double *u_dev, void *stream) {
+  if (nrow < 1 || nw < 1 || nb < 1 || !rows_dev || !b_dev || !u_dev) return RC_BAD_ARG;
+  int rc = device_ready();
+  if (rc) return rc;
+  return ngd_device_noalloc(rows_dev, nrow, nw, b_dev, nb, mu, u_dev, (cudaStream_t)stream);
+}
+
 const char *dnnf90_last_error(void) { return last_error(); }
 
 long long dnnf90_launch_count(void) { return launch_count(); }

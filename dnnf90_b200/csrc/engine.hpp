@@ -170,6 +170,12 @@ int adam_device(double *w, const double *g, double *m, double *v, int nw,
 int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
                double mu, double *u, int prec, cudaStream_t st);
 
+// The same step on caller device buffers with the metric in a fixed
+// scratch area of the library (no device allocation); nw <= ngd_noalloc_maxw().
+int ngd_device_noalloc(const double *rows, int nrow, int nw, const double *b, int nb,
+                       double mu, double *u, cudaStream_t st);
+int ngd_noalloc_maxw();
+
 // count of kernel launches issued by this library (process-wide)
 void note_launch();
 long long launch_count();

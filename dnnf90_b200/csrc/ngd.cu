@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 
 #include "engine.hpp"
@@ -262,6 +263,85 @@ int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
   CKN(cudaStreamSynchronize(st));
   cudaFree(G);
   cudaFree(info);
+  if (hinfo) {
+    set_error("the damped metric is not positive definite at column " + std::to_string(hinfo));
+    return RC_BAD_ARG;
+  }
+  return RC_OK;
+}
+
+// ------------------------------------------------- no-allocation variant
+// dnnf90_ngd_step_noalloc runs the plain FP64 route above on caller
+// buffers without allocating device memory: the damped metric and the
+// pivot flag live in this fixed area instead.  The array belongs to every
+// GPU that loads the library, for the life of the process (8 MiB).
+constexpr int NGD_NOALLOC_MAXW = 1024;
+static __device__ __align__(256) double
+    g_ngd_scratch[(size_t)NGD_NOALLOC_MAXW * NGD_NOALLOC_MAXW + 32];
+
+int ngd_noalloc_maxw() { return NGD_NOALLOC_MAXW; }
+
+// Device address of the scratch on the current device, looked up once per
+// device (host code cannot use the array's name as a device address).
+static double *ngd_scratch_ptr() {
+  static std::mutex mu;
+  static double *ptr[256] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!ptr[dev]) {
+    double *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void **)&p, g_ngd_scratch);
+    if (e != cudaSuccess) {
+      set_error(std::string("cudaGetSymbolAddress(ngd scratch): ") + cudaGetErrorString(e));
+      return nullptr;
+    }
+    ptr[dev] = p;
+  }
+  return ptr[dev];
+}
+
+int ngd_device_noalloc(const double *rows, int nrow, int nw, const double *b, int nb,
+                       double mu, double *u, cudaStream_t st) {
+  if (nw > NGD_NOALLOC_MAXW) {
+    set_error("dnnf90_ngd_step_noalloc: nweights " + std::to_string(nw) +
+              " is above the fixed scratch limit of " + std::to_string(NGD_NOALLOC_MAXW));
+    return RC_BAD_ARG;
+  }
+  double *G = ngd_scratch_ptr();
+  if (!G) return RC_DEVICE;
+  int *info = (int *)(G + (size_t)NGD_NOALLOC_MAXW * NGD_NOALLOC_MAXW);
+  // the scratch keeps the previous call's contents: clear what accumulates
+  CKN(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)nw * nw, st));
+  CKN(cudaMemsetAsync(info, 0, sizeof(int), st));
+  const int tiles = (nw + 63) / 64;
+  {
+    int rchunk = std::max(64, (nrow + 7) / 8);
+    rchunk = (rchunk + 15) / 16 * 16;
+    dim3 grid(tiles, tiles, (nrow + rchunk - 1) / rchunk);
+    LAUNCH("k_syrk_f64", st, k_syrk_f64<<<grid, 256, 0, st>>>(rows, nrow, nw, G, rchunk));
+    CKN(cudaGetLastError());
+  }
+  LAUNCH("k_scale_damp", st, k_scale_damp<<<1024, 256, 0, st>>>(G, nw, 1.0 / (double)nb, mu, b, u));
+  CKN(cudaGetLastError());
+  for (int k0 = 0; k0 < nw; k0 += NB) {
+    const int nbk = std::min(NB, nw - k0);
+    LAUNCH("k_potrf_diag", st, k_potrf_diag<<<1, 256, 0, st>>>(G, nw, k0, nbk, info));
+    CKN(cudaGetLastError());
+    if (k0 + nbk < nw) {
+      const int rem = nw - k0 - nbk;
+      LAUNCH("k_trsm_panel", st, k_trsm_panel<<<std::max(1, std::min(256, (rem + 127) / 128)), 128, 0, st>>>(G, nw, k0, nbk));
+      CKN(cudaGetLastError());
+      const int tt = (rem + 63) / 64;
+      LAUNCH("k_syrk_trail", st, k_syrk_trail<<<dim3(tt, tt), 256, 0, st>>>(G, nw, k0, nbk));
+      CKN(cudaGetLastError());
+    }
+  }
+  LAUNCH("k_chol_solve", st, k_chol_solve<<<1, 1024, 0, st>>>(G, nw, u));
+  CKN(cudaGetLastError());
+  int hinfo = 0;
+  CKN(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKN(cudaStreamSynchronize(st));
   if (hinfo) {
     set_error("the damped metric is not positive definite at column " + std::to_string(hinfo));
     return RC_BAD_ARG;

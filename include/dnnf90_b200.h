@@ -93,6 +93,23 @@ int dnnf90_jrow_dev(int nid, int tid, int npts, const double *x_dev, int rid,
 /* points per device chunk of a training work space (0 = automatic) */
 int dnnf90_twork_set_chunk(int tid, int npts);
 
+/* dnnf90_ngd_step (plain FP64 route) on device buffers rows_dev[nrow][nw],
+ * b_dev[nw], u_dev[nw], for callers that cannot allocate device memory
+ * while they run: a host whose device memory is all handed out up front by
+ * its own allocator or pool, or a caller under a fixed device-memory
+ * budget.  No counterpart in the reference (its gauss_solve works on host
+ * arrays).  The call allocates nothing: the nw x nw metric sits in a fixed
+ * 8 MiB area inside the library that every GPU loading the library keeps
+ * until the process exits, so nw <= 1024; larger nw is refused (-1) with a
+ * message in dnnf90_last_error().  The first call on a device looks up the
+ * area's device address; make that first call before any stream capture.
+ * Every call shares the area: calls that overlap on the GPU (other
+ * threads, other streams) race and must be serialised by the caller.  The
+ * call synchronises stream (NULL: the legacy default stream). */
+int dnnf90_ngd_step_noalloc(int nrow, int nw, const double *rows_dev,
+                            const double *b_dev, int nb, double mu,
+                            double *u_dev, void *stream);
+
 /* text of the last error on this thread; 1 if a CUDA device is usable */
 const char *dnnf90_last_error(void);
 int dnnf90_device_available(void);
