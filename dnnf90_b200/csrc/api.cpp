@@ -1036,6 +1036,20 @@ int dnnf90_ngd_step(int nid, int nrow, const double *rows, const double *b, int 
 }
 
 // ------------------------------------------------------------- device pointers
+namespace {
+// End of a device-pointer call on the split path: wait for the work on st and
+// read the tensor-core GEMM's time-out flag, so that a GEMM that gave up is
+// an error code rather than silently wrong planes.  Skipped while st is being
+// captured into a graph (no synchronisation is allowed there).
+int dev_finish(NetH &n, cudaStream_t st, int rc) {
+  if (rc || n.prec != PREC_SPLIT) return rc;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return RC_OK;
+  return gemm_tc_flag(&n.dn, st);
+}
+}  // namespace
+
 int dnnf90_set_weights_dev(int nid, const double *w_dev, void *stream) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (bad_net(nid) || !w_dev) return RC_BAD_ARG;
@@ -1070,13 +1084,13 @@ int dnnf90_forward_dev(int nid, int tid, int npts, const double *x_dev, double *
     w.kept_x = x_dev;
     w.kept_n = npts;
     w.kept_ver = n.wver;
-    return RC_OK;
+    return dev_finish(n, st, RC_OK);
   }
   w.kept = false;
   DevRule none;
   BatchArgs a;
   a.npts = npts; a.X = x_dev; a.out = tm_dev; a.prec = n.prec;
-  return run_batch(n.dt, n.dn, none, w.p, a, st);
+  return dev_finish(n, st, run_batch(n.dt, n.dn, none, w.p, a, st));
 }
 
 int dnnf90_backward_dev(int nid, int tid, int npts, const double *x_dev,
@@ -1092,7 +1106,8 @@ int dnnf90_backward_dev(int nid, int tid, int npts, const double *x_dev,
   if ((rc = net_device(n, st))) return rc;
   if (w.kept && w.kept_x == x_dev && w.kept_n == npts && w.kept_ver == n.wver &&
       w.p.prec == n.prec)
-    return adjoint_kept(n.dt, n.dn, w.p, n.prec, npts, x_dev, seedm_dev, grad_dev, st);
+    return dev_finish(n, st,
+                      adjoint_kept(n.dt, n.dn, w.p, n.prec, npts, x_dev, seedm_dev, grad_dev, st));
   // recompute mode: the forward runs again inside the adjoint
   if ((rc = work_planes(w, n, npts, false))) return rc;
   w.kept = false;
@@ -1101,7 +1116,7 @@ int dnnf90_backward_dev(int nid, int tid, int npts, const double *x_dev,
   BatchArgs a;
   a.npts = npts; a.X = x_dev; a.seeds = seedm_dev; a.grad = grad_dev;
   a.train = true; a.prec = n.prec;
-  return run_batch(n.dt, n.dn, given, w.p, a, st);
+  return dev_finish(n, st, run_batch(n.dt, n.dn, given, w.p, a, st));
 }
 
 int dnnf90_grad_rule_dev(int nid, int tid, int npts, const double *x_dev, int rid,
@@ -1122,7 +1137,7 @@ int dnnf90_grad_rule_dev(int nid, int tid, int npts, const double *x_dev, int ri
   BatchArgs a;
   a.npts = npts; a.X = x_dev; a.out = tm_dev; a.grad = grad_dev; a.loss = loss_dev;
   a.train = true; a.prec = n.prec;
-  return run_batch(n.dt, n.dn, g_rule[rid].d, w.p, a, st);
+  return dev_finish(n, st, run_batch(n.dt, n.dn, g_rule[rid].d, w.p, a, st));
 }
 
 int dnnf90_jrow_dev(int nid, int tid, int npts, const double *x_dev, int rid,
@@ -1143,7 +1158,7 @@ int dnnf90_jrow_dev(int nid, int tid, int npts, const double *x_dev, int rid,
   BatchArgs a;
   a.npts = npts; a.X = x_dev; a.out = tm_dev; a.rows = rows_dev;
   a.train = true; a.prec = n.prec;
-  return run_batch(n.dt, n.dn, g_rule[rid].d, w.p, a, st);
+  return dev_finish(n, st, run_batch(n.dt, n.dn, g_rule[rid].d, w.p, a, st));
 }
 
 int dnnf90_ngd_step_noalloc(int nrow, int nw, const double *rows_dev, const double *b_dev,

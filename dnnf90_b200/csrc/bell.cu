@@ -106,7 +106,7 @@ struct Fwd2Args {
 
 template <typename R, int KK, int NPB, bool TRAIN>
 __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd2(Fwd2Args a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   R *sS = (R *)smem_raw;
   R *sB = sS + (size_t)a.na * NPB;
   R *sD = sB + (size_t)a.nslot * NPB;
@@ -205,7 +205,7 @@ struct Adj2Args {
 
 template <typename R, int NPB>
 __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj2(Adj2Args a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   R *sT = (R *)smem_raw;
   R *sH = sT + (size_t)a.na * NPB;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj2(Adj2Args a) {
 
 // ---------------------------------------------------------------- v3
 struct Fwd3Args {
-  int n, na, npts, iact, dt_off, nrows, nuv;
+  int n, na, npts, iact, dt_off, nrows, nuv, gy;
   const double *tpc;
   const int *list;
   const int4 *arec;
@@ -317,9 +317,6 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool lact = lane < NPB;
   const int ln = lact ? lane : 0;
-  const int j0 = blockIdx.y * NPB;
-  const int j = j0 + ln;
-  const bool act = lact && j < a.n;
   const int n = a.n;
   const size_t plane = (size_t)a.na * n;
   unsigned char *base = smem_raw + ln * sizeof(R);
@@ -328,14 +325,22 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
   const R *sc = (const R *)a.sc;
   const int sbuf1 = a.nrows * 128;
   int buf = 0;
-  if (blockIdx.x < a.npts)
-    stage_rows<NPB, R>(smem_raw, (const R *)a.S + blockIdx.x * plane, a.na, n, j0, BELL_WORKERS * 32);
+  // work items (neuron tile, point), tile-major; each block takes one
+  // contiguous run of them, so the grid is exactly the resident blocks
+  const long nitem = (long)a.npts * a.gy;
+  const long it0 = (long)blockIdx.x * nitem / gridDim.x;
+  const long it1 = (long)(blockIdx.x + 1) * nitem / gridDim.x;
+  if (it0 < it1)
+    stage_rows<NPB, R>(smem_raw, (const R *)a.S + (it0 % a.npts) * plane, a.na, n,
+                       (int)(it0 / a.npts) * NPB, BELL_WORKERS * 32);
   cp_async_commit();
-  for (int pt = blockIdx.x; pt < a.npts; pt += gridDim.x) {
-    const int nxt = pt + gridDim.x;
-    if (nxt < a.npts)
-      stage_rows<NPB, R>(smem_raw + (buf ? 0 : sbuf1), (const R *)a.S + nxt * plane, a.na, n, j0,
-                         BELL_WORKERS * 32);
+  for (long it = it0; it < it1; ++it) {
+    const int pt = (int)(it % a.npts);
+    const int j = (int)(it / a.npts) * NPB + ln;
+    const bool act = lact && j < n;
+    if (it + 1 < it1)
+      stage_rows<NPB, R>(smem_raw + (buf ? 0 : sbuf1), (const R *)a.S + ((it + 1) % a.npts) * plane,
+                         a.na, n, (int)((it + 1) / a.npts) * NPB, BELL_WORKERS * 32);
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
@@ -451,7 +456,7 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
 }
 
 struct Adj3Args {
-  int n, na, npts, gstride;
+  int n, na, npts, gstride, gy;
   const int *list;
   const int4 *orec;
   const uint32_t *pair;  // Tb row | h row << 16
@@ -470,29 +475,43 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj3(Adj3Args a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool lact = lane < NPB;
   const int ln = lact ? lane : 0;
-  const int j0 = blockIdx.y * NPB;
-  const int j = j0 + ln;
-  const bool act = lact && j < a.n;
   const int n = a.n, na = a.na;
   const size_t plane = (size_t)na * n;
   const int bufb = 2 * na * 128;  // bytes per buffer
   const R *sc = (const R *)a.sc;
   const int rs = __ldg(a.list + warp * 2), rn = __ldg(a.list + warp * 2 + 1);
+  // bias gradient of the neuron this lane holds, flushed when the tile changes
   double gb = 0.0;
+  int gj = -1;
   int buf = 0;
-  if (blockIdx.x < a.npts) {
-    stage_rows<NPB, R>(smem_raw, (const R *)a.Tb + blockIdx.x * plane, na, n, j0, ADJ_WORKERS * 32);
-    stage_rows<NPB, R>(smem_raw + na * 128, (const R *)a.h + blockIdx.x * plane, na, n, j0,
-                       ADJ_WORKERS * 32);
+  // work items (neuron tile, point), tile-major, one contiguous run per block
+  const long nitem = (long)a.npts * a.gy;
+  const long it0 = (long)blockIdx.x * nitem / gridDim.x;
+  const long it1 = (long)(blockIdx.x + 1) * nitem / gridDim.x;
+  if (it0 < it1) {
+    const size_t o = (it0 % a.npts) * plane;
+    const int j0 = (int)(it0 / a.npts) * NPB;
+    stage_rows<NPB, R>(smem_raw, (const R *)a.Tb + o, na, n, j0, ADJ_WORKERS * 32);
+    stage_rows<NPB, R>(smem_raw + na * 128, (const R *)a.h + o, na, n, j0, ADJ_WORKERS * 32);
   }
   cp_async_commit();
-  for (int pt = blockIdx.x; pt < a.npts; pt += gridDim.x) {
-    const int nxt = pt + gridDim.x;
+  for (long it = it0; it < it1; ++it) {
+    const int pt = (int)(it % a.npts);
+    const int j = (int)(it / a.npts) * NPB + ln;
+    const bool act = lact && j < n;
+    if (j != gj) {
+      if (a.gbias && gj >= 0 && gj < n && lact && gb != 0.0)
+        atomicAdd(a.gbias + (size_t)gj * a.gstride, gb);
+      gb = 0.0;
+      gj = j;
+    }
     unsigned char *cur = smem_raw + buf * bufb;
-    if (nxt < a.npts) {
+    if (it + 1 < it1) {
       unsigned char *oth = smem_raw + (buf ^ 1) * bufb;
-      stage_rows<NPB, R>(oth, (const R *)a.Tb + nxt * plane, na, n, j0, ADJ_WORKERS * 32);
-      stage_rows<NPB, R>(oth + na * 128, (const R *)a.h + nxt * plane, na, n, j0, ADJ_WORKERS * 32);
+      const size_t o = ((it + 1) % a.npts) * plane;
+      const int j0 = (int)((it + 1) / a.npts) * NPB;
+      stage_rows<NPB, R>(oth, (const R *)a.Tb + o, na, n, j0, ADJ_WORKERS * 32);
+      stage_rows<NPB, R>(oth + na * 128, (const R *)a.h + o, na, n, j0, ADJ_WORKERS * 32);
     }
     cp_async_commit();
     cp_async_wait<1>();
@@ -528,7 +547,8 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj3(Adj3Args a) {
     buf ^= 1;
   }
   cp_async_wait<0>();
-  if (a.gbias && act && gb != 0.0) atomicAdd(a.gbias + (size_t)j * a.gstride, gb);
+  if (a.gbias && gj >= 0 && gj < n && lact && gb != 0.0)
+    atomicAdd(a.gbias + (size_t)gj * a.gstride, gb);
 }
 
 static int sm_count_b() {
@@ -540,6 +560,18 @@ static int sm_count_b() {
     if (n <= 0) n = 148;
   }
   return n;
+}
+
+// blocks of a persistent launch: as many as are resident at once on the
+// device (occupancy of this kernel at this shared-memory size), at most one
+// per work item, so no block waits for a second wave
+static int persistent_grid(const void *k, int threads, size_t smem, long items) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const long g = (long)sm_count_b() * per_sm;
+  return (int)std::max(1L, std::min(g, items));
 }
 
 template <typename R, int KK>
@@ -556,19 +588,11 @@ static int fwd3_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
   a.grec = bp.f4_grec; a.nuv = bp.nuv;
   a.sc = sizeof(R) == 8 ? (const void *)bp.sc64 : (const void *)bp.sc32;
   a.S = S; a.T = T; a.h = h;
-  const int gy = (n + NPB - 1) / NPB;
-  const int per_sm = std::max(1, (int)((228 * 1024) / (smem + 1024)));
-  const int gx = std::max(1, std::min(npts, sm_count_b() * per_sm / gy + 1));
-  dim3 grid(gx, gy);
-  if (train) {
-    auto k = k_bell_fwd3<R, KK, NPB, true>;
-    CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LAUNCH("k_bell_fwd", st, k<<<grid, BELL_WORKERS * 32, smem, st>>>(a));
-  } else {
-    auto k = k_bell_fwd3<R, KK, NPB, false>;
-    CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LAUNCH("k_bell_fwd", st, k<<<grid, BELL_WORKERS * 32, smem, st>>>(a));
-  }
+  a.gy = (n + NPB - 1) / NPB;
+  auto k = train ? k_bell_fwd3<R, KK, NPB, true> : k_bell_fwd3<R, KK, NPB, false>;
+  CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = persistent_grid((const void *)k, BELL_WORKERS * 32, smem, (long)npts * a.gy);
+  LAUNCH("k_bell_fwd", st, k<<<grid, BELL_WORKERS * 32, smem, st>>>(a));
   CKB(cudaGetLastError());
   return RC_OK;
 }
@@ -591,7 +615,7 @@ static int fwd2_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
   a.S = S; a.T = T; a.h = h;
   const int gy = (n + NPB - 1) / NPB;
   const int per_sm = std::max(1, (int)((228 * 1024) / (smem + 1024)));
-  const int gx = std::max(1, std::min(npts, sm_count_b() * per_sm / gy + 1));
+  const int gx = std::max(1, std::min(npts, sm_count_b() * per_sm / gy));
   dim3 grid(gx, gy);
   if (train) {
     auto k = k_bell_fwd2<R, KK, NPB, true>;
@@ -642,12 +666,11 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
     b.orec = (const int4 *)bp.a3_orec; b.pair = bp.a4_pair;
     b.sc = sizeof(R) == 8 ? (const void *)bp.sc64 : (const void *)bp.sc32;
     b.Tb = Tb; b.h = h; b.Sb = Sb; b.gbias = gbias;
-    const int gy = (n + NPB - 1) / NPB;
-    const int per_sm = std::max(1, (int)((228 * 1024) / (smem3 + 1024)));
-    const int gx = std::max(1, std::min(npts, sm_count_b() * per_sm / gy + 1));
+    b.gy = (n + NPB - 1) / NPB;
     auto k = k_bell_adj3<R, NPB>;
     CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
-    LAUNCH("k_bell_adj", st, k<<<dim3(gx, gy), ADJ_WORKERS * 32, smem3, st>>>(b));
+    const int grid = persistent_grid((const void *)k, ADJ_WORKERS * 32, smem3, (long)npts * b.gy);
+    LAUNCH("k_bell_adj", st, k<<<grid, ADJ_WORKERS * 32, smem3, st>>>(b));
     CKB(cudaGetLastError());
     return RC_OK;
   }
@@ -658,7 +681,7 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
   a.Tb = Tb; a.h = h; a.Sb = Sb; a.gbias = gbias;
   const int gy = (n + NPB - 1) / NPB;
   const int per_sm = std::max(1, (int)((228 * 1024) / (smem + 1024)));
-  const int gx = std::max(1, std::min(npts, sm_count_b() * per_sm / gy + 1));
+  const int gx = std::max(1, std::min(npts, sm_count_b() * per_sm / gy));
   dim3 grid(gx, gy);
   auto k = k_bell_adj2<R, NPB>;
   CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

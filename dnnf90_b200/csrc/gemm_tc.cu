@@ -762,6 +762,9 @@ int gemm_tc_flag(const DevNet *net, cudaStream_t st) {
   CKT(cudaMemcpyAsync(&h, w->flag, sizeof(int), cudaMemcpyDeviceToHost, st));
   CKT(cudaStreamSynchronize(st));
   if (h) {
+    // report once, then clear, so that the next call runs afresh
+    cudaMemsetAsync(w->flag, 0, sizeof(int), st);
+    cudaStreamSynchronize(st);
     set_error("tensor-core GEMM: an mbarrier wait timed out (code " + std::to_string(h) + ")");
     return RC_DEVICE;
   }

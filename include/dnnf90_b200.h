@@ -69,7 +69,10 @@ int dnnf90_ngd_step(int nid, int nrow, const double *rows, const double *b,
                     int nb, double mu, int prec, double *u);
 
 /* ---- device-pointer entry points (pointers to device memory; stream is
- * a cudaStream_t, NULL for the legacy default stream) ---- */
+ * a cudaStream_t, NULL for the legacy default stream).  On the split path
+ * the compute entries return after the work on stream has finished, having
+ * checked the tensor-core GEMMs' error flag (-3 if one gave up); while the
+ * stream is being captured into a graph they return without waiting. ---- */
 /* weights from a device array in the flat layout */
 int dnnf90_set_weights_dev(int nid, const double *w_dev, void *stream);
 /* forward of npts points: tm_dev[npts][na][nout] (may be NULL).  keep = 1
