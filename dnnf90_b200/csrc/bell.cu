@@ -31,7 +31,8 @@ namespace dnnf90 {
 void DevBellPlan::release() {
   void *ps[] = {fw_list, fw_arec, fw_grec, fw_gc64, fw_gc32, aj_list, aj_orec, aj_pair,
                 aj_c64, aj_c32, f3_list, f3_arec, f3_grec, f3_gc64, f3_gc32, a3_orec,
-                a3_pair, sc64, sc32, f4_grec, a4_pair};
+                a3_pair, sc64, sc32, f4_grec, a4_pair, f5_list, f5_arec, f5_rec, f5_cpdst,
+                a5_pair};
   for (void *p : ps)
     if (p) cudaFree(p);
   *this = DevBellPlan();
@@ -87,6 +88,20 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
   std::vector<float> sc32(sc.begin(), sc.end());
   if ((rc = put(&d.sc64, sc))) return rc;
   if ((rc = put(&d.sc32, sc32))) return rc;
+  if ((rc = put(&d.f5_list, P.f5_list))) return rc;
+  if ((rc = put(&d.f5_arec, P.f5_arec))) return rc;
+  if ((rc = put(&d.f5_rec, P.f5_rec))) return rc;
+  if ((rc = put(&d.f5_cpdst, P.f5_cpdst))) return rc;
+  {
+    // adjoint pairs as (Tb row, h row) byte offsets; the kernel reads up to
+    // three pairs past the last one of a list
+    std::vector<uint32_t> a5(P.a3_pair.begin(), P.a3_pair.end());
+    for (int i = 0; i < 8; ++i) a5.push_back(0);
+    if ((rc = put(&d.a5_pair, a5))) return rc;
+  }
+  d.f5_ok = P.f5_ok;
+  d.nrows5 = P.nrows5;
+  d.dt_off5 = P.dt_off5;
   d.f3_ok = P.f3_ok;
   d.nrows = P.nrows;
   d.dt_off = P.dt_off;
@@ -260,18 +275,7 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj2(Adj2Args a) {
 }
 
 
-// ---------------------------------------------------------------- v3
-struct Fwd3Args {
-  int n, na, npts, iact, dt_off, nrows, nuv, gy;
-  const double *tpc;
-  const int *list;
-  const int4 *arec;
-  const uint32_t *grec;
-  const void *sc;  // [0, na): a!, [na, 2na): 1/a!
-  const void *S;
-  void *T, *h;
-};
-
+// ---------------------------------------------------------------- v5
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
@@ -306,32 +310,70 @@ __device__ __forceinline__ void stage_rows(unsigned char *dst, const R *src, int
   }
 }
 
-// One state row is 128 bytes: NPB lanes x sizeof(R).  Row r of this lane
-// is at  base + r * 128,  base = smem + lane * sizeof(R).  The S rows of
-// the point being computed sit at rows [0, na) or, for the other buffer,
-// [nrows, nrows + na): the next point's S streams into one buffer while
-// the other is read.
+struct Fwd5Args {
+  int n, na, npts, iact, dt_off, nrows, gy;
+  const double *tpc;
+  const int *list;     // [(K+1) * workers][2]
+  const int4 *arec;    // [*][2]
+  const uint2 *rec;    // flat records (byte offsets into the state)
+  const int *cpdst;    // [na]
+  const void *sc;      // [0, na): a!, [na, 2na): 1/a!
+  const void *S;
+  void *T, *h;
+};
+
+// shared-memory value at byte offset off of the dynamic shared area
+template <typename R>
+__device__ __forceinline__ R &srow(unsigned char *sm, uint32_t off) {
+  return *(R *)(sm + off);
+}
+
+// one band of groups whose g has degree D: acc[q] += S~_b B~_{g,q-1},
+// q = 2..D+1, B~_{g,1} = S~_g.  q0/q1 are the next two records.
+template <typename R, int D, int KK>
+__device__ __forceinline__ void fwd_band(unsigned char *sm, uint32_t los, uint32_t lo,
+                                         const uint2 *&rp, uint2 &q0, uint2 &q1, int cnt,
+                                         R (&acc)[KK + 1]) {
+#pragma unroll 2
+  for (int e = 0; e < cnt; ++e) {
+    const uint2 r = q0;
+    q0 = q1;
+    q1 = __ldg(rp + 2);
+    ++rp;
+    const R x = srow<R>(sm, los + r.x);
+    const uint32_t z = (D == 1 ? los : lo) + r.y;
+#pragma unroll
+    for (int l = 0; l < D; ++l) acc[2 + l] += x * srow<R>(sm, z + l * 128);
+  }
+}
+
+// Bell forward over factorial-normalised state (S~_b = S_b/b!,
+// B~_{a,q} = B_{a,q}/a!): for degree p < K
+//   B~_{a,q} = (1/q) sum_{0<b<a} S~_b B~_{a-b,q-1},  B~_{a,1} = S~_a,
+//   T_a = a! sum_q s^(q) B~_{a,q},  h_a = a! sum_q s^(q+1) B~_{a,q},
+// and U~_a, V~_a (sums with s^(q+1)/(q+1), s^(q+2)/(q+1)) kept for the top
+// degree, where
+//   T_a = a! (s' S~_a + sum_{0<b<a} S~_b U~_{a-b}),  likewise h_a with s'', V~
+// (lib/train_module.f90:297-325 regrouped by b; the q = 1 terms of U, V
+// carry S~_g itself).
 template <typename R, int KK, int NPB, bool TRAIN>
-__global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
+__global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd5(Fwd5Args a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char *sm = smem_raw;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool lact = lane < NPB;
   const int ln = lact ? lane : 0;
   const int n = a.n;
   const size_t plane = (size_t)a.na * n;
-  unsigned char *base = smem_raw + ln * sizeof(R);
-#define ROWV(off) (*(R *)(base + (off)))
-#define ROWS(off) (*(R *)(sbase + (off)))
+  const uint32_t lo = ln * sizeof(R);  // this lane's column in every row
   const R *sc = (const R *)a.sc;
-  const int sbuf1 = a.nrows * 128;
+  const uint32_t sbuf1 = a.nrows * 128;
   int buf = 0;
-  // work items (neuron tile, point), tile-major; each block takes one
-  // contiguous run of them, so the grid is exactly the resident blocks
   const long nitem = (long)a.npts * a.gy;
   const long it0 = (long)blockIdx.x * nitem / gridDim.x;
   const long it1 = (long)(blockIdx.x + 1) * nitem / gridDim.x;
   if (it0 < it1)
-    stage_rows<NPB, R>(smem_raw, (const R *)a.S + (it0 % a.npts) * plane, a.na, n,
+    stage_rows<NPB, R>(sm, (const R *)a.S + (it0 % a.npts) * plane, a.na, n,
                        (int)(it0 / a.npts) * NPB, BELL_WORKERS * 32);
   cp_async_commit();
   for (long it = it0; it < it1; ++it) {
@@ -339,23 +381,29 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
     const int j = (int)(it / a.npts) * NPB + ln;
     const bool act = lact && j < n;
     if (it + 1 < it1)
-      stage_rows<NPB, R>(smem_raw + (buf ? 0 : sbuf1), (const R *)a.S + ((it + 1) % a.npts) * plane,
+      stage_rows<NPB, R>(sm + (buf ? 0 : sbuf1), (const R *)a.S + ((it + 1) % a.npts) * plane,
                          a.na, n, (int)((it + 1) / a.npts) * NPB, BELL_WORKERS * 32);
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
-    unsigned char *sbase = base + (buf ? sbuf1 : 0);
-    // normalise: row b of S becomes S_b / b!  (row 0 keeps S_0)
-    for (int ia = warp; ia < a.na; ia += BELL_WORKERS)
-      if (lact) ROWS(ia * 128) *= __ldg(sc + a.na + ia);
+    const uint32_t los = lo + (buf ? sbuf1 : 0);  // this lane in the current S rows
+    // normalise S_b -> S_b / b! (row 0 keeps S_0); copy level 1 of each B run
+    for (int ia = warp; ia < a.na; ia += BELL_WORKERS) {
+      const int cd = __ldg(a.cpdst + ia);
+      if (lact) {
+        const R v = srow<R>(sm, los + ia * 128) * __ldg(sc + a.na + ia);
+        srow<R>(sm, los + ia * 128) = v;
+        if (cd >= 0) srow<R>(sm, lo + cd) = v;
+      }
+    }
     __syncthreads();
     R *T = (R *)a.T + pt * plane;
     R *H = TRAIN ? (R *)a.h + pt * plane : nullptr;
     if (warp == 0 && lact) {
       double d[KK + 2];
-      sigma_derivs(a.iact, a.tpc, KK, (double)ROWS(0), d);
+      sigma_derivs(a.iact, a.tpc, KK, (double)srow<R>(sm, los), d);
 #pragma unroll
-      for (int q = 0; q <= KK + 1; ++q) ROWV(a.dt_off + q * 128) = (R)d[q];
+      for (int q = 0; q <= KK + 1; ++q) srow<R>(sm, lo + a.dt_off + q * 128) = (R)d[q];
       if (act) {
         T[j] = (R)d[0];
         if (TRAIN) H[j] = (R)d[1];
@@ -364,7 +412,7 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
     __syncthreads();
     R dt[KK + 2];
 #pragma unroll
-    for (int q = 0; q <= KK + 1; ++q) dt[q] = ROWV(a.dt_off + q * 128);
+    for (int q = 0; q <= KK + 1; ++q) dt[q] = srow<R>(sm, lo + a.dt_off + q * 128);
     R uc[KK + 1], vc[KK + 1];
 #pragma unroll
     for (int q = 1; q < KK; ++q) {
@@ -377,25 +425,22 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
       for (int r = rs; r < rs + rn; ++r) {
         const int4 A0 = __ldg(a.arec + 2 * r), A1 = __ldg(a.arec + 2 * r + 1);
         const int ia = A0.x & 0xffff;
-        const R sa = ROWS(ia * 128);
+        const R sa = srow<R>(sm, los + ia * 128);
         const R fa = __ldg(sc + ia);
-        const int gs = A0.y, ge = A0.y + A0.z;
+        const uint2 *rp = a.rec + A0.y;
+        uint2 q0 = __ldg(rp), q1 = __ldg(rp + 1);
         if (p == KK) {
-          // top degree: T_a / a! = s' S~_a + sum_b S~_b U~_{a-b}, likewise h with V~
           R tt = dt[1] * sa, hh = dt[2] * sa;
-          const int voff = a.nuv * 128;
-          for (int g0 = gs; g0 < ge; g0 += BELL_UNROLL) {
-            uint32_t gr[BELL_UNROLL];
-#pragma unroll
-            for (int u = 0; u < BELL_UNROLL; ++u) gr[u] = __ldg(a.grec + min(g0 + u, ge - 1));
-#pragma unroll
-            for (int u = 0; u < BELL_UNROLL; ++u)
-              if (g0 + u < ge) {
-                const R x = ROWS((gr[u] & 0x3ffu) << 7);
-                const int uo = (int)(gr[u] >> 10) << 7;
-                tt += x * ROWV(uo);
-                hh += x * ROWV(uo + voff);
-              }
+#pragma unroll 2
+          for (int e = 0; e < A0.z; ++e) {
+            const uint2 g = q0;
+            q0 = q1;
+            q1 = __ldg(rp + 2);
+            ++rp;
+            const R x = srow<R>(sm, los + g.x);
+            const uint32_t u = lo + g.y;
+            tt += x * srow<R>(sm, u);
+            hh += x * srow<R>(sm, u + 128);
           }
           if (act) {
             T[(size_t)ia * n + j] = fa * tt;
@@ -407,21 +452,19 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
 #pragma unroll
         for (int q = 0; q <= KK; ++q) acc[q] = (R)0;
         const uint64_t bands = ((uint64_t)(uint32_t)A0.w << 32) | (uint32_t)A1.w;
-        int g = gs;
-        // the next record is fetched while the current one is applied
-        uint32_t nr = __ldg(a.grec + min(g, max(ge - 1, 0)));
 #pragma unroll
-        for (int d = KK - 1; d >= 1; --d) {
+        for (int d = KK - 2; d >= 1; --d) {
           if (d < p) {
             const int cnt = (int)((bands >> (8 * (d - 1))) & 0xffu);
-            for (int e = 0; e < cnt; ++e, ++g) {
-              const uint32_t gr = nr;
-              nr = __ldg(a.grec + min(g + 1, ge - 1));
-              const R x = ROWS((gr & 0x3ffu) << 7);
-              acc[2] += x * ROWS(((gr >> 10) & 0x3ffu) << 7);
-              const int zo = (int)(gr >> 20) << 7;
-#pragma unroll
-              for (int q = 3; q <= d + 1; ++q) acc[q] += x * ROWV(zo + (q - 3) * 128);
+            // d is a compile-time constant after unrolling
+            switch (d) {
+              case 1: if constexpr (1 <= KK - 2) fwd_band<R, 1, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
+              case 2: if constexpr (2 <= KK - 2) fwd_band<R, 2, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
+              case 3: if constexpr (3 <= KK - 2) fwd_band<R, 3, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
+              case 4: if constexpr (4 <= KK - 2) fwd_band<R, 4, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
+              case 5: if constexpr (5 <= KK - 2) fwd_band<R, 5, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
+              case 6: if constexpr (6 <= KK - 2) fwd_band<R, 6, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
+              default: break;
             }
           }
         }
@@ -430,7 +473,7 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
         for (int q = 2; q < KK; ++q) {
           if (q <= p) {
             const R b = acc[q] * (R)(1.0 / q);
-            if (A1.x >= 0 && lact) ROWV(A1.x + (q - 2) * 128) = b;
+            if (A1.x >= 0 && lact) srow<R>(sm, lo + A1.x + (q - 1) * 128) = b;
             tt += dt[q] * b;
             hh += dt[q + 1] * b;
             uu += uc[q] * b;
@@ -438,8 +481,8 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
           }
         }
         if (A1.y >= 0 && lact) {
-          ROWV(A1.y) = uu;
-          ROWV(A1.z) = vv;
+          srow<R>(sm, lo + A1.y) = uu;
+          srow<R>(sm, lo + A1.y + 128) = vv;
         }
         if (act) {
           T[(size_t)ia * n + j] = fa * tt;
@@ -451,48 +494,46 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd3(Fwd3Args a) {
     buf ^= 1;
   }
   cp_async_wait<0>();
-#undef ROWS
-#undef ROWV
 }
 
-struct Adj3Args {
+struct Adj5Args {
   int n, na, npts, gstride, gy;
   const int *list;
-  const int4 *orec;
-  const uint32_t *pair;  // Tb row | h row << 16
-  const void *sc;  // [3][na]
+  const int4 *orec;    // ib, pstart, pcount, 0
+  const uint2 *pair;   // byte offsets of the Tb row and the h row in a buffer
+  const void *sc;      // [3][na]
   const void *Tb, *h;
   void *Sb;
   double *gbias;
 };
 
-// Bell adjoint as a correlation: Sb_b b! = sum_{a >= b} (a! Tb_a)(h_{a-b}/(a-b)!).
-// Shared memory holds two buffers of [Tb rows | h rows]; the next point's
+// Bell adjoint as a correlation: Sb_b b! = sum_{a >= b} (a! Tb_a)(h_{a-b}/(a-b)!)
+// (lib/train_module.f90:381-403 with C(a,b) folded into row scales).
+// Shared memory holds two buffers of [Tb rows | h rows]; the next item's
 // rows stream into one while the other is scaled and read.
 template <typename R, int NPB>
-__global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj3(Adj3Args a) {
+__global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj5(Adj5Args a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char *sm = smem_raw;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool lact = lane < NPB;
   const int ln = lact ? lane : 0;
   const int n = a.n, na = a.na;
   const size_t plane = (size_t)na * n;
-  const int bufb = 2 * na * 128;  // bytes per buffer
+  const uint32_t bufb = 2 * na * 128;  // bytes per buffer
   const R *sc = (const R *)a.sc;
   const int rs = __ldg(a.list + warp * 2), rn = __ldg(a.list + warp * 2 + 1);
-  // bias gradient of the neuron this lane holds, flushed when the tile changes
   double gb = 0.0;
   int gj = -1;
   int buf = 0;
-  // work items (neuron tile, point), tile-major, one contiguous run per block
   const long nitem = (long)a.npts * a.gy;
   const long it0 = (long)blockIdx.x * nitem / gridDim.x;
   const long it1 = (long)(blockIdx.x + 1) * nitem / gridDim.x;
   if (it0 < it1) {
     const size_t o = (it0 % a.npts) * plane;
     const int j0 = (int)(it0 / a.npts) * NPB;
-    stage_rows<NPB, R>(smem_raw, (const R *)a.Tb + o, na, n, j0, ADJ_WORKERS * 32);
-    stage_rows<NPB, R>(smem_raw + na * 128, (const R *)a.h + o, na, n, j0, ADJ_WORKERS * 32);
+    stage_rows<NPB, R>(sm, (const R *)a.Tb + o, na, n, j0, ADJ_WORKERS * 32);
+    stage_rows<NPB, R>(sm + na * 128, (const R *)a.h + o, na, n, j0, ADJ_WORKERS * 32);
   }
   cp_async_commit();
   for (long it = it0; it < it1; ++it) {
@@ -505,9 +546,8 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj3(Adj3Args a) {
       gb = 0.0;
       gj = j;
     }
-    unsigned char *cur = smem_raw + buf * bufb;
     if (it + 1 < it1) {
-      unsigned char *oth = smem_raw + (buf ^ 1) * bufb;
+      unsigned char *oth = sm + (buf ^ 1) * bufb;
       const size_t o = ((it + 1) % a.npts) * plane;
       const int j0 = (int)((it + 1) / a.npts) * NPB;
       stage_rows<NPB, R>(oth, (const R *)a.Tb + o, na, n, j0, ADJ_WORKERS * 32);
@@ -516,29 +556,27 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj3(Adj3Args a) {
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
+    const uint32_t lc = buf * bufb + ln * sizeof(R);  // this lane in the current buffer
     // scale: row a of Tb by a!, row g of h by 1/g!
     for (int r = warp; r < 2 * na; r += ADJ_WORKERS)
-      if (lact) *(R *)(cur + r * 128 + lane * sizeof(R)) *= __ldg(sc + r);
+      if (lact) srow<R>(sm, lc + r * 128) *= __ldg(sc + r);
     __syncthreads();
-    unsigned char *base = cur + ln * sizeof(R);
     R *Sb = (R *)a.Sb + pt * plane;
     for (int r = rs; r < rs + rn; ++r) {
       const int4 o = __ldg(a.orec + r);  // ib, pstart, pcount
+      const uint2 *pp = a.pair + o.y;
+      uint2 q0 = __ldg(pp), q1 = __ldg(pp + 1);
       R s0 = (R)0, s1 = (R)0;
-      const int pe = o.y + o.z;
-      for (int ip = o.y; ip < pe; ip += 4) {
-        uint32_t pk[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) pk[u] = __ldg(a.pair + min(ip + u, pe - 1));
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (ip + u < pe) {
-            const R v = *(const R *)(base + ((pk[u] & 0xffffu) << 7)) *
-                        *(const R *)(base + ((pk[u] >> 16) << 7));
-            if (u & 1) s1 += v;
-            else s0 += v;
-          }
+      int e = 0;
+      for (; e + 2 <= o.z; e += 2) {
+        const uint2 u0 = q0, u1 = q1;
+        q0 = __ldg(pp + 2);
+        q1 = __ldg(pp + 3);
+        pp += 2;
+        s0 += srow<R>(sm, lc + u0.x) * srow<R>(sm, lc + u0.y);
+        s1 += srow<R>(sm, lc + u1.x) * srow<R>(sm, lc + u1.y);
       }
+      if (e < o.z) s0 += srow<R>(sm, lc + q0.x) * srow<R>(sm, lc + q0.y);
       const R s = (s0 + s1) * __ldg(sc + 2 * na + o.x);
       if (act) Sb[(size_t)o.x * n + j] = s;
       if (o.x == 0) gb += (double)s;
@@ -575,21 +613,20 @@ static int persistent_grid(const void *k, int threads, size_t smem, long items) 
 }
 
 template <typename R, int KK>
-static int fwd3_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int npts,
+static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int npts,
                          const void *S, void *T, void *h, bool train, cudaStream_t st) {
   constexpr int NPB = sizeof(R) == 8 ? 16 : 32;
   static_assert(NPB * sizeof(R) == 128, "one state row is 128 bytes");
-  const size_t smem = ((size_t)bp.nrows + t.na) * 128;
-  if (!bp.f3_ok || smem > 227 * 1024 || n % (16 / (int)sizeof(R))) return RC_UNSUPPORTED;
-  Fwd3Args a;
-  a.n = n; a.na = t.na; a.npts = npts; a.iact = t.iact; a.dt_off = bp.dt_off;
-  a.nrows = bp.nrows;
-  a.tpc = t.tpc; a.list = bp.f3_list; a.arec = (const int4 *)bp.f3_arec;
-  a.grec = bp.f4_grec; a.nuv = bp.nuv;
+  const size_t smem = ((size_t)bp.nrows5 + t.na) * 128;
+  if (!bp.f5_ok || smem > 227 * 1024 || n % (16 / (int)sizeof(R))) return RC_UNSUPPORTED;
+  Fwd5Args a;
+  a.n = n; a.na = t.na; a.npts = npts; a.iact = t.iact; a.dt_off = bp.dt_off5;
+  a.nrows = bp.nrows5; a.gy = (n + NPB - 1) / NPB;
+  a.tpc = t.tpc; a.list = bp.f5_list; a.arec = (const int4 *)bp.f5_arec;
+  a.rec = (const uint2 *)bp.f5_rec; a.cpdst = bp.f5_cpdst;
   a.sc = sizeof(R) == 8 ? (const void *)bp.sc64 : (const void *)bp.sc32;
   a.S = S; a.T = T; a.h = h;
-  a.gy = (n + NPB - 1) / NPB;
-  auto k = train ? k_bell_fwd3<R, KK, NPB, true> : k_bell_fwd3<R, KK, NPB, false>;
+  auto k = train ? k_bell_fwd5<R, KK, NPB, true> : k_bell_fwd5<R, KK, NPB, false>;
   CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = persistent_grid((const void *)k, BELL_WORKERS * 32, smem, (long)npts * a.gy);
   LAUNCH("k_bell_fwd", st, k<<<grid, BELL_WORKERS * 32, smem, st>>>(a));
@@ -601,7 +638,7 @@ template <typename R, int KK>
 static int fwd2_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int npts,
                          const void *S, void *T, void *h, bool train, cudaStream_t st) {
   {
-    int rc3 = fwd3_dispatch<R, KK>(bp, t, n, npts, S, T, h, train, st);
+    int rc3 = fwd5_dispatch<R, KK>(bp, t, n, npts, S, T, h, train, st);
     if (rc3 != RC_UNSUPPORTED) return rc3;
   }
   constexpr int NPB = sizeof(R) == 8 ? 16 : 32;
@@ -659,18 +696,18 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
   constexpr int NPB = sizeof(R) == 8 ? 16 : 32;
   const size_t smem = (size_t)2 * t.na * NPB * sizeof(R);
   if (smem > 227 * 1024) return RC_UNSUPPORTED;
-  if (bp.a3_orec && (size_t)4 * t.na * 128 <= 227 * 1024 && n % (16 / (int)sizeof(R)) == 0) {
-    const size_t smem3 = (size_t)4 * t.na * 128;
-    Adj3Args b;
+  if (bp.a5_pair && (size_t)4 * t.na * 128 <= 227 * 1024 && n % (16 / (int)sizeof(R)) == 0) {
+    const size_t smem5 = (size_t)4 * t.na * 128;
+    Adj5Args b;
     b.n = n; b.na = t.na; b.npts = npts; b.gstride = gstride; b.list = bp.aj_list;
-    b.orec = (const int4 *)bp.a3_orec; b.pair = bp.a4_pair;
+    b.orec = (const int4 *)bp.a3_orec; b.pair = (const uint2 *)bp.a5_pair;
     b.sc = sizeof(R) == 8 ? (const void *)bp.sc64 : (const void *)bp.sc32;
     b.Tb = Tb; b.h = h; b.Sb = Sb; b.gbias = gbias;
     b.gy = (n + NPB - 1) / NPB;
-    auto k = k_bell_adj3<R, NPB>;
-    CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
-    const int grid = persistent_grid((const void *)k, ADJ_WORKERS * 32, smem3, (long)npts * b.gy);
-    LAUNCH("k_bell_adj", st, k<<<grid, ADJ_WORKERS * 32, smem3, st>>>(b));
+    auto k = k_bell_adj5<R, NPB>;
+    CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem5));
+    const int grid = persistent_grid((const void *)k, ADJ_WORKERS * 32, smem5, (long)npts * b.gy);
+    LAUNCH("k_bell_adj", st, k<<<grid, ADJ_WORKERS * 32, smem5, st>>>(b));
     CKB(cudaGetLastError());
     return RC_OK;
   }

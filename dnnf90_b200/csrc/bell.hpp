@@ -31,6 +31,11 @@ struct DevBellPlan {
   int *a3_orec = nullptr, *a3_pair = nullptr;
   uint32_t *f4_grec = nullptr, *a4_pair = nullptr;
   int nuv = 0;
+  // v5
+  bool f5_ok = false;
+  int nrows5 = 0, dt_off5 = 0;
+  int *f5_list = nullptr, *f5_arec = nullptr, *f5_cpdst = nullptr;
+  uint32_t *f5_rec = nullptr, *a5_pair = nullptr;
   double *sc64 = nullptr;  // [3][na]: a!, 1/a!, 1/a! (Tb, h, Sb scales)
   float *sc32 = nullptr;
   void release();

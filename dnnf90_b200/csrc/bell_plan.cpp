@@ -180,6 +180,84 @@ BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
     }
   }
 
+  // ---- forward v5 (flat records; see bell_plan.hpp)
+  {
+    const int ROW = 128;
+    std::vector<int> b1(na, -1), uv(na, -1);
+    int row = na;
+    for (int ia = 1; ia < na; ++ia)
+      if (t.deg[ia] >= 2 && t.deg[ia] <= k - 2) {
+        b1[ia] = row * ROW;
+        row += t.deg[ia];
+      }
+    for (int ia = 1; ia < na; ++ia)
+      if (t.deg[ia] <= k - 1) {
+        uv[ia] = row * ROW;
+        row += 2;
+      }
+    P.dt_off5 = row * ROW;
+    P.nrows5 = row + k + 2;
+    P.f5_cpdst = b1;
+    P.f5_list.assign((size_t)(k + 1) * workers * 2, 0);
+    bool bands_ok = true;
+    for (int p = 1; p <= k; ++p) {
+      std::vector<int> items;
+      std::vector<long> cost;
+      for (int ia = 1; ia < na; ++ia)
+        if (t.deg[ia] == p) {
+          items.push_back(ia);
+          long c = 6;
+          const int st = p >= 2 ? t.fq_at(ia, 2) : 0, nn = p >= 2 ? t.fq_len(ia, 2) : 0;
+          for (int i = st; i < st + nn; ++i) c += p == k ? 4 : 3 + t.deg[t.fq_id[i]];
+          cost.push_back(c);
+        }
+      auto asg = balance(cost, workers);
+      for (int w = 0; w < workers; ++w) {
+        P.f5_list[((size_t)p * workers + w) * 2] = (int)P.f5_arec.size() / 8;
+        P.f5_list[((size_t)p * workers + w) * 2 + 1] = (int)asg[w].size();
+        for (int it : asg[w]) {
+          const int ia = items[it];
+          const int rstart = (int)P.f5_rec.size() / 2;
+          uint64_t bands = 0;
+          int cnt[9] = {0};
+          if (p >= 2) {
+            const int st = t.fq_at(ia, 2), nn = t.fq_len(ia, 2);
+            std::vector<int> idx;
+            for (int i = st; i < st + nn; ++i) idx.push_back(i);
+            if (p < k)  // bands of |g| = d, longest first
+              std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+                return t.deg[t.fq_id[a]] > t.deg[t.fq_id[b]];
+              });
+            for (int i : idx) {
+              const int ib = t.fq_ib[i], g = t.fq_id[i];
+              P.f5_rec.push_back((uint32_t)(ib * ROW));
+              if (p == k)
+                P.f5_rec.push_back((uint32_t)uv[g]);
+              else
+                P.f5_rec.push_back((uint32_t)(t.deg[g] >= 2 ? b1[g] : g * ROW));
+              if (p < k) cnt[t.deg[g]]++;
+            }
+          }
+          for (int d = 1; d <= 8; ++d) {
+            if (cnt[d] > 255) bands_ok = false;
+            if (d <= 8) bands += (uint64_t)(cnt[d] & 0xff) << (8 * (d - 1));
+          }
+          P.f5_arec.push_back(ia | (p << 16));
+          P.f5_arec.push_back(rstart);
+          P.f5_arec.push_back((int)P.f5_rec.size() / 2 - rstart);
+          P.f5_arec.push_back((int)(bands >> 32));
+          P.f5_arec.push_back(b1[ia]);
+          P.f5_arec.push_back(uv[ia]);
+          P.f5_arec.push_back(0);
+          P.f5_arec.push_back((int)(bands & 0xffffffffu));
+        }
+      }
+    }
+    // the kernels read two records ahead of the one they use
+    for (int i = 0; i < 8; ++i) P.f5_rec.push_back(0);
+    P.f5_ok = bands_ok && k <= 8 && (size_t)(P.nrows5 + na) * ROW <= 227 * 1024;
+  }
+
   // padding: the kernels prefetch the record after the last one of a list
   for (int i = 0; i < 4; ++i) {
     for (int c = 0; c < 4; ++c) P.f3_grec.push_back(0);

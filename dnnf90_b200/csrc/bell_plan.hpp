@@ -44,6 +44,24 @@ struct BellPlan {
   //   p = K : ib | (U row of g) << 10         (V row = U row + nuv)
   std::vector<uint32_t> f4_grec;
   int nuv = 0;
+  // forward v5: the v4 work lists with flat records of two byte offsets
+  // into the shared state, no decoding in the inner loop.  Rows:
+  //   [0, na)       S_b / b!                         (double-buffered)
+  //   B run of g    levels 1..|g| of B_{g,q} / g!, level 1 a copy of S_g/g!
+  //                 (2 <= |g| <= K-2)
+  //   U/V pair of g U_g/g! and, in the next row, V_g/g!  (1 <= |g| <= K-1)
+  //   sigma         K+2 rows of sigma^(q)
+  // Records (uint2):
+  //   p < K : (S row of b, first level row of g)  -- level l at + (l-1) rows;
+  //           for |g| = 1 the level-1 row is S_g itself (S region)
+  //   p = K : (S row of b, U row of g)            -- V one row further
+  int nrows5 = 0, dt_off5 = 0;
+  bool f5_ok = false;
+  std::vector<int> f5_list;        // [(k+1) * workers][2]: start, count into f5_arec
+  std::vector<int> f5_arec;        // [*][8]: ia | p << 16, rstart, rcount, band_hi,
+                                   //         B run of a (or -1), U/V pair of a (or -1), 0, band_lo
+  std::vector<uint32_t> f5_rec;    // [*][2]
+  std::vector<int> f5_cpdst;       // [na]: byte offset of the level-1 copy of S_a, or -1
   // adjoint, v3: Sb_b b! = sum_{a >= b} (a! Tb_a) (h_{a-b} / (a-b)!), the
   // pair coefficient C(a,b) = a!/(b!(a-b)!) folded into per-row scales
   std::vector<int> a3_orec;   // [*][4]: ib, pstart, pcount, 0

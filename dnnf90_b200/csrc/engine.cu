@@ -161,7 +161,7 @@ static int dput(T **p, const T *h, size_t n) {
 
 void DevTables::release() {
   void *ps[] = {deg, alpha, ind_e1, seg, fq_pk, fq_c64, fq_c32, pseg, pair_pk,
-                pair_c64, pair_c32, tpc};
+                pair_c64, pair_c32, tpc, l2par, l2up};
   for (void *p : ps)
     if (p) cudaFree(p);
   bp.release();
@@ -233,6 +233,40 @@ int upload_tables(const TableSet &t, DevTables &d) {
   if ((rc = dput(&d.pair_c64, t.pair_binom.data(), t.pair_binom.size()))) return rc;
   if ((rc = dput(&d.pair_c32, pair32.data(), pair32.size()))) return rc;
   if ((rc = dput(&d.tpc, t.tpc.data(), t.tpc.size()))) return rc;
+  {
+    // parent / child slots along unit steps (downward closure keeps a - e_i)
+    const int d0 = t.d0;
+    std::vector<int> par(na, 0), up((size_t)na * d0, -1);
+    std::vector<int> b(d0);
+    for (int ia = 1; ia < na; ++ia) {
+      const int *al = &t.alpha[(size_t)ia * d0];
+      int i0 = 0;
+      while (i0 < d0 && al[i0] == 0) ++i0;
+      for (int i = 0; i < d0; ++i) b[i] = al[i];
+      b[i0] -= 1;
+      const int ps = t.find(b.data());
+      if (ps < 0) {
+        set_error("table program: the carried set is not downward closed");
+        return RC_BAD_ARG;
+      }
+      par[ia] = ps | (i0 << 16);
+    }
+    for (int ia = 0; ia < na; ++ia)
+      for (int i = 0; i < d0; ++i) {
+        for (int c = 0; c < d0; ++c) b[c] = t.alpha[(size_t)ia * d0 + c];
+        b[i] += 1;
+        const int u = t.find(b.data());
+        if (u >= 0) up[(size_t)ia * d0 + i] = u | (b[i] << 16);
+      }
+    d.graded = true;
+    for (int ia = 1; ia < na; ++ia)
+      if (t.deg[ia] < t.deg[ia - 1]) d.graded = false;
+    d.dstart.assign(k + 2, na);
+    for (int ia = na - 1; ia >= 0; --ia) d.dstart[t.deg[ia]] = ia;
+    for (int p = k; p >= 0; --p) d.dstart[p] = std::min(d.dstart[p], d.dstart[p + 1]);
+    if ((rc = dput(&d.l2par, par.data(), par.size()))) return rc;
+    if ((rc = dput(&d.l2up, up.data(), up.size()))) return rc;
+  }
   if ((rc = upload_bell_plan(t, d.bp))) return rc;
   return RC_OK;
 }
@@ -619,6 +653,270 @@ __global__ void __launch_bounds__(256) k_output_adj(OutAdjArgs a) {
   if (threadIdx.x < nout) atomicAdd(a.g + (size_t)threadIdx.x * (m + 1), acc[threadIdx.x][0]);
 }
 
+
+// ------------------------------------------------- streaming layer kernels
+// One warp per point, the lane index the neuron of a 32-neuron tile
+// (blockIdx.y): every plane row a warp touches is one coalesced line.
+
+struct L2vArgs {
+  int n, na, d0, npts;
+  int ds[KMAX + 2];        // slots of degree p: [ds[p], ds[p + 1])
+  int iact;
+  const int *par;          // [na]
+  const double *tpc;
+  const double *X;         // [P][d0]
+  const double *W;         // [n][d0 + 1]
+  void *T, *h;             // [P][na][n]
+};
+
+// First hidden layer, analytic (see k_layer2): T^a = s^(|a|) W^a with the
+// monomial W^a = prod_i W_i^{a_i} of each neuron built once per block in
+// shared memory along unit steps, M[a] = M[a - e_i] W_i.  The slots are
+// graded, so each degree is one contiguous run sharing s^(p).
+template <typename R, int KK, bool TRAIN>
+__global__ void __launch_bounds__(256) k_layer2v(L2vArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *M = (R *)smem_raw;  // [na][32]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int j = blockIdx.y * 32 + lane;
+  const bool act = j < a.n;
+  const double *wr = a.W + (size_t)(act ? j : a.n - 1) * (a.d0 + 1);
+  if (warp == 0) {
+    M[lane] = (R)1;
+    for (int ia = 1; ia < a.na; ++ia) {
+      const int pk = __ldg(a.par + ia);
+      M[ia * 32 + lane] = (R)((double)M[(pk & 0xffff) * 32 + lane] * wr[1 + (pk >> 16)]);
+    }
+  }
+  __syncthreads();
+  const size_t plane = (size_t)a.na * a.n;
+  for (long pt = (long)blockIdx.x * nw + warp; pt < a.npts; pt += (long)gridDim.x * nw) {
+    const double *x = a.X + pt * a.d0;
+    double s = wr[0];
+    for (int i = 0; i < a.d0; ++i) s = s + wr[1 + i] * x[i];
+    double d[KK + 2];
+    sigma_derivs(a.iact, a.tpc, KK, s, d);
+    R *T = (R *)a.T + pt * plane + j;
+    R *H = TRAIN ? (R *)a.h + pt * plane + j : nullptr;
+#pragma unroll
+    for (int p = 0; p <= KK; ++p) {
+      const R dp = (R)d[p], dq = (R)d[p + 1];
+      const int e = a.ds[p + 1];
+#pragma unroll 4
+      for (int ia = a.ds[p]; ia < e; ++ia) {
+        const R m = M[ia * 32 + lane];
+        if (act) {
+          T[(size_t)ia * a.n] = dp * m;
+          if (TRAIN) H[(size_t)ia * a.n] = dq * m;
+        }
+      }
+    }
+  }
+}
+
+struct AdjL2vArgs {
+  int n, na, npts;
+  const int *up;           // [na][D0]
+  const void *Tb, *h;
+  const double *X;
+  double *g;               // dW_2 [n][D0 + 1], accumulated (null in row mode)
+  double *rows;            // [P][nw] (row mode)
+  size_t nw, woff;
+};
+
+// Bell adjoint of the first hidden layer fused with dW_2 (see k_bell_adj_l2):
+//   Sb^0 = sum_g Tb^g h^g,  Sb^{e_i} = sum_g (g_i + 1) Tb^{g + e_i} h^g,
+//   dW_2[j][0] += Sb^0,  dW_2[j][1 + i] += Sb^0 x_i + Sb^{e_i}.
+template <typename R, int D0>
+__global__ void __launch_bounds__(256) k_adj_l2v(AdjL2vArgs a) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int j = blockIdx.y * 32 + lane;
+  const bool act = j < a.n;
+  const int jc = act ? j : a.n - 1;
+  const size_t plane = (size_t)a.na * a.n;
+  double acc[D0 + 1];
+#pragma unroll
+  for (int i = 0; i <= D0; ++i) acc[i] = 0.0;
+  for (long pt = (long)blockIdx.x * nw + warp; pt < a.npts; pt += (long)gridDim.x * nw) {
+    const R *Tb = (const R *)a.Tb + pt * plane + jc;
+    const R *H = (const R *)a.h + pt * plane + jc;
+    R s[D0 + 1];
+#pragma unroll
+    for (int i = 0; i <= D0; ++i) s[i] = (R)0;
+#pragma unroll 2
+    for (int g = 0; g < a.na; ++g) {
+      const R hg = H[(size_t)g * a.n];
+      s[0] += Tb[(size_t)g * a.n] * hg;
+#pragma unroll
+      for (int i = 0; i < D0; ++i) {
+        const int u = __ldg(a.up + g * D0 + i);
+        if (u >= 0) s[1 + i] += (R)(u >> 16) * Tb[(size_t)(u & 0xffff) * a.n] * hg;
+      }
+    }
+    const double *x = a.X + pt * D0;
+    const double v0 = (double)s[0];
+    if (a.rows) {
+      if (act) {
+        double *row = a.rows + pt * a.nw + a.woff + (size_t)j * (D0 + 1);
+        row[0] = v0;
+#pragma unroll
+        for (int i = 0; i < D0; ++i) row[1 + i] = v0 * x[i] + (double)s[1 + i];
+      }
+    } else {
+      acc[0] += v0;
+#pragma unroll
+      for (int i = 0; i < D0; ++i) acc[1 + i] += v0 * x[i] + (double)s[1 + i];
+    }
+  }
+  if (a.g && act)
+#pragma unroll
+    for (int i = 0; i <= D0; ++i) atomicAdd(a.g + (size_t)j * (D0 + 1) + i, acc[i]);
+}
+
+// Output layer and seed, one warp per point (see k_output_fwd for the
+// formulas).  Shared memory per warp: tl[nout][na], sd[nout][na] (double).
+template <typename R>
+__global__ void __launch_bounds__(256) k_output_fwdv(OutArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int m = a.m, na = a.na, nout = a.nout;
+  double *tl = (double *)smem_raw + (size_t)warp * 2 * nout * na;
+  double *sd = tl + (size_t)nout * na;
+  const size_t plane = (size_t)na * m;
+  double lsum = 0.0;
+  for (long pt = (long)blockIdx.x * nw + warp; pt < a.npts; pt += (long)gridDim.x * nw) {
+    const R *Tm = (const R *)a.Tm + pt * plane;
+    for (int ia = 0; ia < na; ++ia) {
+      const R *row = Tm + (size_t)ia * m;
+      for (int o = 0; o < nout; ++o) {
+        const double *w = a.W + (size_t)o * (m + 1) + 1;
+        double part = 0.0;
+        for (int i = lane; i < m; i += 32) part += __ldg(w + i) * (double)row[i];
+        part = warp_sum(part);
+        if (lane == 0) {
+          const double v = (ia == 0 ? a.W[(size_t)o * (m + 1)] : 0.0) + part;
+          tl[o * na + ia] = v;
+          if (a.out) a.out[(pt * (size_t)na + ia) * nout + o] = v;
+        }
+      }
+    }
+    __syncwarp();
+    if (a.seed) {
+      for (int i = lane; i < nout * na; i += 32) sd[i] = 0.0;
+      __syncwarp();
+      if (lane == 0) {
+        if (a.kind == SEED_HALFSQ) {
+          double l = 0.0;
+          for (int ia = 0; ia < na; ++ia) { sd[ia] = tl[ia]; l += tl[ia] * tl[ia]; }
+          lsum += 0.5 * l;
+        } else {
+          double R0 = 0.0;
+          for (int t = 0; t < a.nterm; ++t) {
+            const int ind = a.ind[t];
+            if (a.nonlin[t]) R0 = R0 + a.coeff[t] * tl[0] * tl[ind];
+            else R0 = R0 + a.coeff[t] * tl[ind];
+          }
+          double Rs = R0, fac = a.fac;
+          if (a.kind == SEED_JROW) { Rs = 1.0; fac = 1.0; }
+          else lsum += 0.5 * a.fac * R0 * R0;
+          for (int t = 0; t < a.nterm; ++t) {
+            const int ind = a.ind[t];
+            if (a.nonlin[t]) {
+              sd[ind] = sd[ind] + fac * Rs * a.coeff[t] * tl[0];
+              sd[0] = sd[0] + fac * Rs * a.coeff[t] * tl[ind];
+            } else {
+              sd[ind] = sd[ind] + fac * Rs * a.coeff[t];
+            }
+          }
+        }
+      }
+      __syncwarp();
+      double *dst = a.seed + pt * (size_t)nout * na;
+      for (int i = lane; i < nout * na; i += 32) dst[i] = sd[i];
+    }
+    __syncwarp();
+  }
+  if (a.loss && lane == 0 && lsum != 0.0) atomicAdd(a.loss, lsum);
+}
+
+// Adjoint of the output layer, one warp per point (see k_output_adj):
+// Tb_{L-1}^a[i] = sum_o W_L[o][1+i] seed[o][a], dW_L[o][1+i] += sum_a
+// seed[o][a] T_{L-1}^a[i].  Lane i + 32 t holds neuron i + 32 t, t < NT.
+template <typename R, int MAXO, int NT>
+__global__ void __launch_bounds__(256) k_output_adjv(OutAdjArgs a) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int m = a.m, na = a.na, nout = a.nout;
+  const size_t plane = (size_t)na * m;
+  double acc[MAXO][NT], acc0[MAXO];
+  double w[MAXO][NT];
+#pragma unroll
+  for (int o = 0; o < MAXO; ++o) {
+    acc0[o] = 0.0;
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int i = lane + 32 * t;
+      acc[o][t] = 0.0;
+      w[o][t] = (o < nout && i < m) ? a.W[(size_t)o * (m + 1) + 1 + i] : 0.0;
+    }
+  }
+  for (long pt = (long)blockIdx.x * nw + warp; pt < a.npts; pt += (long)gridDim.x * nw) {
+    const R *Tm = (const R *)a.Tm + pt * plane;
+    R *Tb = (R *)a.Tb + pt * plane;
+    const double *sd = a.seed + pt * (size_t)nout * na;
+    double pg[MAXO][NT];
+#pragma unroll
+    for (int o = 0; o < MAXO; ++o)
+#pragma unroll
+      for (int t = 0; t < NT; ++t) pg[o][t] = 0.0;
+#pragma unroll 2
+    for (int ia = 0; ia < na; ++ia) {
+      double so[MAXO];
+#pragma unroll
+      for (int o = 0; o < MAXO; ++o) so[o] = o < nout ? __ldg(sd + o * na + ia) : 0.0;
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const int i = lane + 32 * t;
+        if (i < m) {
+          double tb = 0.0;
+#pragma unroll
+          for (int o = 0; o < MAXO; ++o) tb += w[o][t] * so[o];
+          Tb[(size_t)ia * m + i] = (R)tb;
+          const double tv = (double)Tm[(size_t)ia * m + i];
+#pragma unroll
+          for (int o = 0; o < MAXO; ++o) pg[o][t] += so[o] * tv;
+        }
+      }
+    }
+    if (a.rows) {
+      double *row = a.rows + pt * a.nw + a.woff;
+#pragma unroll
+      for (int o = 0; o < MAXO; ++o)
+        if (o < nout) {
+#pragma unroll
+          for (int t = 0; t < NT; ++t)
+            if (lane + 32 * t < m) row[(size_t)o * (m + 1) + 1 + lane + 32 * t] = pg[o][t];
+          if (lane == 0) row[(size_t)o * (m + 1)] = sd[o * na];
+        }
+    } else {
+#pragma unroll
+      for (int o = 0; o < MAXO; ++o) {
+        acc0[o] += sd[o * na];
+#pragma unroll
+        for (int t = 0; t < NT; ++t) acc[o][t] += pg[o][t];
+      }
+    }
+  }
+  if (a.rows || !a.g) return;
+#pragma unroll
+  for (int o = 0; o < MAXO; ++o)
+    if (o < nout) {
+#pragma unroll
+      for (int t = 0; t < NT; ++t)
+        if (lane + 32 * t < m) atomicAdd(a.g + (size_t)o * (m + 1) + 1 + lane + 32 * t, acc[o][t]);
+      if (lane == 0) atomicAdd(a.g + (size_t)o * (m + 1), acc0[o]);
+    }
+}
+
 // --------------------------------------------------------- CUDA-core GEMM
 // Tiled GEMM for the FP64 path (and the split path where the tensor-core
 // kernel does not apply).  Three forms:
@@ -906,6 +1204,118 @@ static int launch_gemm_cc(int mode, int M, int N, int K, int na, const void *A,
   return RC_OK;
 }
 
+
+// blocks of k resident on the whole device at this block shape
+static int occ_grid(const void *k, int threads, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  return sm_count() * per_sm;
+}
+
+template <typename R, int KK>
+static int layer2v_k(const L2vArgs &a, bool train, cudaStream_t st) {
+  const size_t smem = (size_t)a.na * 32 * sizeof(R);
+  const void *k = train ? (const void *)k_layer2v<R, KK, true> : (const void *)k_layer2v<R, KK, false>;
+  CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int gy = (a.n + 31) / 32;
+  const int gx = std::max(1, std::min((a.npts + 7) / 8, occ_grid(k, 256, smem) / gy));
+  dim3 grid(gx, gy);
+  if (train) { LAUNCH("k_layer2", st, (k_layer2v<R, KK, true><<<grid, 256, smem, st>>>(a))); }
+  else { LAUNCH("k_layer2", st, (k_layer2v<R, KK, false><<<grid, 256, smem, st>>>(a))); }
+  CK(cudaGetLastError());
+  return RC_OK;
+}
+
+// streaming first hidden layer; RC_UNSUPPORTED when the shape is outside it
+template <typename R>
+static int launch_layer2v(const DevTables &t, int n, int npts, const double *X, const double *W,
+                          void *T, void *h, bool train, cudaStream_t st) {
+  if (!t.graded || t.k > 8 || (size_t)t.na * 32 * sizeof(R) > 200 * 1024) return RC_UNSUPPORTED;
+  L2vArgs a;
+  a.n = n; a.na = t.na; a.d0 = t.d0; a.npts = npts; a.iact = t.iact;
+  for (int p = 0; p < KMAX + 2; ++p) a.ds[p] = p <= t.k + 1 ? t.dstart[std::min(p, t.k + 1)] : t.na;
+  a.par = t.l2par; a.tpc = t.tpc; a.X = X; a.W = W; a.T = T; a.h = h;
+  switch (t.k) {
+    case 1: return layer2v_k<R, 1>(a, train, st);
+    case 2: return layer2v_k<R, 2>(a, train, st);
+    case 3: return layer2v_k<R, 3>(a, train, st);
+    case 4: return layer2v_k<R, 4>(a, train, st);
+    case 5: return layer2v_k<R, 5>(a, train, st);
+    case 6: return layer2v_k<R, 6>(a, train, st);
+    case 7: return layer2v_k<R, 7>(a, train, st);
+    case 8: return layer2v_k<R, 8>(a, train, st);
+    default: return RC_UNSUPPORTED;
+  }
+}
+
+template <typename R, int D0>
+static int adjl2v_k(const AdjL2vArgs &a, cudaStream_t st) {
+  const void *k = (const void *)k_adj_l2v<R, D0>;
+  const int gy = (a.n + 31) / 32;
+  const int gx = std::max(1, std::min((a.npts + 7) / 8, occ_grid(k, 256, 0) / gy));
+  LAUNCH("k_bell_adj_l2", st, (k_adj_l2v<R, D0><<<dim3(gx, gy), 256, 0, st>>>(a)));
+  CK(cudaGetLastError());
+  return RC_OK;
+}
+
+template <typename R>
+static int launch_adj_l2v(const DevTables &t, const AdjL2vArgs &a, cudaStream_t st) {
+  switch (t.d0) {
+    case 1: return adjl2v_k<R, 1>(a, st);
+    case 2: return adjl2v_k<R, 2>(a, st);
+    case 3: return adjl2v_k<R, 3>(a, st);
+    case 4: return adjl2v_k<R, 4>(a, st);
+    case 5: return adjl2v_k<R, 5>(a, st);
+    case 6: return adjl2v_k<R, 6>(a, st);
+    case 7: return adjl2v_k<R, 7>(a, st);
+    case 8: return adjl2v_k<R, 8>(a, st);
+    default: return RC_UNSUPPORTED;
+  }
+}
+
+template <typename R>
+static int launch_output_fwdv(const OutArgs &o, cudaStream_t st) {
+  const size_t per_warp = (size_t)2 * o.nout * o.na * sizeof(double);
+  const int wpb = (int)std::min<size_t>(8, (200 * 1024) / std::max<size_t>(per_warp, 1));
+  if (wpb < 1) return RC_UNSUPPORTED;
+  const size_t smem = per_warp * wpb;
+  const void *k = (const void *)k_output_fwdv<R>;
+  CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = std::max(1, std::min((o.npts + wpb - 1) / wpb, occ_grid(k, 32 * wpb, smem)));
+  LAUNCH("k_output_fwd", st, (k_output_fwdv<R><<<grid, 32 * wpb, smem, st>>>(o)));
+  CK(cudaGetLastError());
+  return RC_OK;
+}
+
+template <typename R, int NO, int NT>
+static int outadjv_k(const OutAdjArgs &o, cudaStream_t st) {
+  const void *k = (const void *)k_output_adjv<R, NO, NT>;
+  const int grid = std::max(1, std::min((o.npts + 7) / 8, occ_grid(k, 256, 0)));
+  LAUNCH("k_output_adj", st, (k_output_adjv<R, NO, NT><<<grid, 256, 0, st>>>(o)));
+  CK(cudaGetLastError());
+  return RC_OK;
+}
+
+template <typename R, int NO>
+static int outadjv_nt(const OutAdjArgs &o, cudaStream_t st) {
+  const int nt = (o.m + 31) / 32;
+  if (nt <= 1) return outadjv_k<R, NO, 1>(o, st);
+  if (nt <= 2) return outadjv_k<R, NO, 2>(o, st);
+  if (nt <= 4) return outadjv_k<R, NO, 4>(o, st);
+  if (nt <= 8) return outadjv_k<R, NO, 8>(o, st);
+  return RC_UNSUPPORTED;
+}
+
+template <typename R>
+static int launch_output_adjv(const OutAdjArgs &o, cudaStream_t st) {
+  if (o.nout == 1) return outadjv_nt<R, 1>(o, st);
+  if (o.nout == 2) return outadjv_nt<R, 2>(o, st);
+  if (o.nout <= 4) return outadjv_nt<R, 4>(o, st);
+  return RC_UNSUPPORTED;
+}
+
 // ------------------------------------------------------------- the driver
 template <typename R>
 struct Chunk {
@@ -936,10 +1346,15 @@ static int fwd_chunk(Chunk<R> &c, const DevRule *rule, const double *X,
     l2.n = net.dims[1]; l2.na = na; l2.d0 = t.d0; l2.k = t.k; l2.iact = t.iact;
     l2.npts = np; l2.alpha = t.alpha; l2.deg = t.deg; l2.tpc = t.tpc; l2.X = X;
     l2.W = c.W64(2); l2.T = p.T[1]; l2.h = p.h[1];
-    dim3 grid(std::min(np, smc * 8), (l2.n + 127) / 128);
-    if (train) { LAUNCH("k_layer2", c.st, k_layer2<R, true><<<grid, 128, 0, c.st>>>(l2)); }
-    else { LAUNCH("k_layer2", c.st, k_layer2<R, false><<<grid, 128, 0, c.st>>>(l2)); }
-    CK(cudaGetLastError());
+    rc = launch_layer2v<R>(t, l2.n, np, X, l2.W, l2.T, l2.h, train, c.st);
+    if (rc == RC_UNSUPPORTED) {
+      dim3 grid(std::min(np, smc * 8), (l2.n + 127) / 128);
+      if (train) { LAUNCH("k_layer2", c.st, k_layer2<R, true><<<grid, 128, 0, c.st>>>(l2)); }
+      else { LAUNCH("k_layer2", c.st, k_layer2<R, false><<<grid, 128, 0, c.st>>>(l2)); }
+      CK(cudaGetLastError());
+    } else if (rc) {
+      return rc;
+    }
   }
   for (int l = 3; l < L; ++l) {
     const int n = net.dims[l - 1], m = net.dims[l - 2];
@@ -966,6 +1381,8 @@ static int fwd_chunk(Chunk<R> &c, const DevRule *rule, const double *X,
   o.loss = loss;
   size_t smem = (size_t)2 * o.nout * na * sizeof(double);
   if (smem > 200 * 1024) { set_error("output layer too wide"); return RC_UNSUPPORTED; }
+  rc = launch_output_fwdv<R>(o, c.st);
+  if (rc != RC_UNSUPPORTED) return rc;
   CK(cudaFuncSetAttribute(k_output_fwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   LAUNCH("k_output_fwd", c.st, k_output_fwd<R><<<std::min(np, smc * 8), 256, smem, c.st>>>(o));
   CK(cudaGetLastError());
@@ -994,8 +1411,13 @@ static int adj_chunk(Chunk<R> &c, const double *X, const double *seed,
       set_error("output layer shape outside the device path (nout <= 4, width <= 1024)");
       return RC_UNSUPPORTED;
     }
-    LAUNCH("k_output_adj", c.st, k_output_adj<R><<<std::min(np, smc * 8), 256, 0, c.st>>>(o));
-    CK(cudaGetLastError());
+    rc = launch_output_adjv<R>(o, c.st);
+    if (rc == RC_UNSUPPORTED) {
+      LAUNCH("k_output_adj", c.st, k_output_adj<R><<<std::min(np, smc * 8), 256, 0, c.st>>>(o));
+      CK(cudaGetLastError());
+    } else if (rc) {
+      return rc;
+    }
   }
   for (int l = L - 1; l >= 3; --l) {
     const int n = net.dims[l - 1], m = net.dims[l - 2];
@@ -1042,6 +1464,13 @@ static int adj_chunk(Chunk<R> &c, const double *X, const double *seed,
   a2.Tb = p.Tb; a2.h = p.h[1]; a2.X = X;
   a2.g = rows || !grad ? nullptr : grad + net.woff[1];
   a2.rows = rows; a2.nw = net.nw; a2.woff = net.woff[1];
+  {
+    AdjL2vArgs v;
+    v.n = a2.n; v.na = na; v.npts = np; v.up = t.l2up; v.Tb = p.Tb; v.h = p.h[1]; v.X = X;
+    v.g = a2.g; v.rows = rows; v.nw = net.nw; v.woff = net.woff[1];
+    rc = launch_adj_l2v<R>(t, v, c.st);
+    if (rc != RC_UNSUPPORTED) return rc;
+  }
   dim3 grid(std::min(np, smc * 8), (a2.n + 127) / 128);
   LAUNCH("k_bell_adj_l2", c.st, k_bell_adj_l2<R><<<grid, 128, 0, c.st>>>(a2));
   CK(cudaGetLastError());

@@ -74,6 +74,12 @@ struct DevTables {
   float *pair_c32 = nullptr;
   double *tpc = nullptr;     // [(k+2)][(k+3)]
   int iact = 0;
+  // first-hidden-layer tables of the streaming kernels
+  int *l2par = nullptr;      // [na]: slot of a - e_i | i << 16, i the first
+                             // nonzero dimension of a (0 for a = 0)
+  int *l2up = nullptr;       // [na][d0]: slot of g + e_i | (g_i + 1) << 16, or -1
+  bool graded = false;       // slots ordered by degree
+  std::vector<int> dstart;   // [k+2]: first slot of each degree
   DevBellPlan bp;            // work lists of the warp-cooperative kernels
   void release();
 };
