@@ -349,8 +349,14 @@ def main():
     # ---- plain FP64 path on the same workload
     net64, g64, loss64 = make(api.PREC_F64)
     ms64, _, _, _ = timed(net64, g64, loss64, args.f64_steps, warmup=1)
+    _, _, prof64, _ = timed(net64, g64, loss64, args.prof_steps, profile=True, warmup=0)
     value64 = ws * npts / (ms64 / 1000.0)
     net64.free()
+
+    def per_step_ms(pr):
+        if not pr:
+            return None
+        return {k: round(v[1] / args.prof_steps, 3) for k, v in sorted(pr.items(), key=lambda kv: -kv[1][1])}
 
     # ---- end to end through the public host-buffer entry
     net_e, _, _ = make(api.PREC_SPLIT)
@@ -407,7 +413,9 @@ def main():
                        "parallelism": f"dp{ws}: points sharded, dL/dw all-reduced (NCCL)",
                        "l2": "inputs larger than L2 (126 MB): a work chunk's planes are ~48 GB, so no flush"},
             "f64": {"value": value64, "unit": "pts/s", "ms_per_step": ms64,
-                    "steps": args.f64_steps, "split_speedup": value / value64},
+                    "steps": args.f64_steps, "split_speedup": value / value64,
+                    "kernel_ms_per_step": per_step_ms(prof64)},
+            "kernel_ms_per_step": per_step_ms(prof),
             "accuracy": acc,
             "e2e": e2e,
             "gpu_launches": launches,

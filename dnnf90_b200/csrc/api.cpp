@@ -187,10 +187,13 @@ int work_planes(WorkH &w, NetH &n, int want, bool exact) {
   for (int l = 2; l < n.nlayer; ++l) per += 2 * (size_t)n.ts.na * n.dims[l - 1] * rsz;
   per += 3 * (size_t)n.ts.na * nmax * rsz;
   per += 2 * (size_t)n.ts.na * n.dims[n.nlayer - 1] * 8 + n.ts.d0 * 8 + 1024;
+  // at most 48 GiB, and at most half of what is free with this work
+  // space's own planes counted as free (so the cap does not grow by
+  // re-counting them on every call)
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
-  size_t budget = std::min<size_t>((size_t)48 << 30, freeb / 2);
-  if (w.p.base) budget += w.p.bytes;
+  const size_t avail = freeb + (w.p.base ? w.p.bytes : 0);
+  const size_t budget = std::min<size_t>((size_t)48 << 30, avail / 2);
   int cap = (int)std::max<size_t>(1, budget / per);
   if (w.chunk > 0) cap = std::min(cap, w.chunk);
   int need = std::min(want, cap);

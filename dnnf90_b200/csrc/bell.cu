@@ -11,7 +11,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 
 #include "bell.hpp"
 #include "engine.hpp"
@@ -32,7 +36,7 @@ void DevBellPlan::release() {
   void *ps[] = {fw_list, fw_arec, fw_grec, fw_gc64, fw_gc32, aj_list, aj_orec, aj_pair,
                 aj_c64, aj_c32, f3_list, f3_arec, f3_grec, f3_gc64, f3_gc32, a3_orec,
                 a3_pair, sc64, sc32, f4_grec, a4_pair, f5_list, f5_arec, f5_rec, f5_cpdst,
-                a5_pair};
+                a5_pair, f6_rec};
   for (void *p : ps)
     if (p) cudaFree(p);
   *this = DevBellPlan();
@@ -47,7 +51,9 @@ static int put(T **d, const std::vector<T> &h) {
 }
 
 int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
+  static std::atomic<uint64_t> next_id{1};
   d.release();
+  d.id = next_id++;
   BellPlan P = build_bell_plan(t, BELL_WORKERS, ADJ_WORKERS);
   d.workers = P.workers;
   d.k = P.k;
@@ -92,11 +98,16 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
   if ((rc = put(&d.f5_arec, P.f5_arec))) return rc;
   if ((rc = put(&d.f5_rec, P.f5_rec))) return rc;
   if ((rc = put(&d.f5_cpdst, P.f5_cpdst))) return rc;
+  if ((rc = put(&d.f6_rec, P.f6_rec))) return rc;
+  d.nrec32 = (int)P.f6_rec.size();
+  d.norec = (int)P.a3_orec.size() / 4;
   {
     // adjoint pairs as (Tb row, h row) byte offsets; the kernel reads up to
     // three pairs past the last one of a list
     std::vector<uint32_t> a5(P.a3_pair.begin(), P.a3_pair.end());
     for (int i = 0; i < 8; ++i) a5.push_back(0);
+    while (a5.size() % 4) a5.push_back(0);  // whole 16-byte pieces
+    d.npair5 = (int)a5.size() / 2;
     if ((rc = put(&d.a5_pair, a5))) return rc;
   }
   d.f5_ok = P.f5_ok;
@@ -312,10 +323,12 @@ __device__ __forceinline__ void stage_rows(unsigned char *dst, const R *src, int
 
 struct Fwd5Args {
   int n, na, npts, iact, dt_off, nrows, gy;
+  int nrec32;          // 32-bit records copied to shared memory (SREC)
   const double *tpc;
   const int *list;     // [(K+1) * workers][2]
   const int4 *arec;    // [*][2]
   const uint2 *rec;    // flat records (byte offsets into the state)
+  const uint32_t *rec32;  // the same records as row indices
   const int *cpdst;    // [na]
   const void *sc;      // [0, na): a!, [na, 2na): 1/a!
   const void *S;
@@ -328,18 +341,36 @@ __device__ __forceinline__ R &srow(unsigned char *sm, uint32_t off) {
   return *(R *)(sm + off);
 }
 
+// Records of the forward: from global memory as two byte offsets, or from
+// a copy in shared memory as two row indices (x row | z row << 16).
+template <bool SREC>
+struct RecSrc;
+template <>
+struct RecSrc<false> {
+  const uint2 *p;
+  __device__ __forceinline__ uint2 get(int i) const { return __ldg(p + i); }
+};
+template <>
+struct RecSrc<true> {
+  const uint32_t *p;  // shared memory
+  __device__ __forceinline__ uint2 get(int i) const {
+    const uint32_t r = p[i];
+    return make_uint2((r & 0xffffu) << 7, (r >> 16) << 7);
+  }
+};
+
 // one band of groups whose g has degree D: acc[q] += S~_b B~_{g,q-1},
 // q = 2..D+1, B~_{g,1} = S~_g.  q0/q1 are the next two records.
-template <typename R, int D, int KK>
+template <typename R, int D, int KK, bool SREC>
 __device__ __forceinline__ void fwd_band(unsigned char *sm, uint32_t los, uint32_t lo,
-                                         const uint2 *&rp, uint2 &q0, uint2 &q1, int cnt,
-                                         R (&acc)[KK + 1]) {
+                                         const RecSrc<SREC> &src, int &ri, uint2 &q0, uint2 &q1,
+                                         int cnt, R (&acc)[KK + 1]) {
 #pragma unroll 2
   for (int e = 0; e < cnt; ++e) {
     const uint2 r = q0;
     q0 = q1;
-    q1 = __ldg(rp + 2);
-    ++rp;
+    q1 = src.get(ri + 2);
+    ++ri;
     const R x = srow<R>(sm, los + r.x);
     const uint32_t z = (D == 1 ? los : lo) + r.y;
 #pragma unroll
@@ -356,10 +387,20 @@ __device__ __forceinline__ void fwd_band(unsigned char *sm, uint32_t los, uint32
 //   T_a = a! (s' S~_a + sum_{0<b<a} S~_b U~_{a-b}),  likewise h_a with s'', V~
 // (lib/train_module.f90:297-325 regrouped by b; the q = 1 terms of U, V
 // carry S~_g itself).
-template <typename R, int KK, int NPB, bool TRAIN>
+template <typename R, int KK, int NPB, bool TRAIN, bool SREC>
 __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd5(Fwd5Args a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char *sm = smem_raw;
+  RecSrc<SREC> src;
+  if constexpr (SREC) {
+    // the records follow the state; copied once, read by every item
+    uint32_t *rs = (uint32_t *)(sm + (size_t)(a.nrows + a.na) * 128);
+    for (int i = threadIdx.x; i < a.nrec32 / 4; i += blockDim.x)
+      ((uint4 *)rs)[i] = __ldg((const uint4 *)a.rec32 + i);
+    src.p = rs;
+  } else {
+    src.p = a.rec;
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool lact = lane < NPB;
   const int ln = lact ? lane : 0;
@@ -427,16 +468,16 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd5(Fwd5Args a) {
         const int ia = A0.x & 0xffff;
         const R sa = srow<R>(sm, los + ia * 128);
         const R fa = __ldg(sc + ia);
-        const uint2 *rp = a.rec + A0.y;
-        uint2 q0 = __ldg(rp), q1 = __ldg(rp + 1);
+        int ri = A0.y;
+        uint2 q0 = src.get(ri), q1 = src.get(ri + 1);
         if (p == KK) {
           R tt = dt[1] * sa, hh = dt[2] * sa;
 #pragma unroll 2
           for (int e = 0; e < A0.z; ++e) {
             const uint2 g = q0;
             q0 = q1;
-            q1 = __ldg(rp + 2);
-            ++rp;
+            q1 = src.get(ri + 2);
+            ++ri;
             const R x = srow<R>(sm, los + g.x);
             const uint32_t u = lo + g.y;
             tt += x * srow<R>(sm, u);
@@ -458,12 +499,12 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd5(Fwd5Args a) {
             const int cnt = (int)((bands >> (8 * (d - 1))) & 0xffu);
             // d is a compile-time constant after unrolling
             switch (d) {
-              case 1: if constexpr (1 <= KK - 2) fwd_band<R, 1, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
-              case 2: if constexpr (2 <= KK - 2) fwd_band<R, 2, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
-              case 3: if constexpr (3 <= KK - 2) fwd_band<R, 3, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
-              case 4: if constexpr (4 <= KK - 2) fwd_band<R, 4, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
-              case 5: if constexpr (5 <= KK - 2) fwd_band<R, 5, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
-              case 6: if constexpr (6 <= KK - 2) fwd_band<R, 6, KK>(sm, los, lo, rp, q0, q1, cnt, acc); break;
+              case 1: if constexpr (1 <= KK - 2) fwd_band<R, 1, KK, SREC>(sm, los, lo, src, ri, q0, q1, cnt, acc); break;
+              case 2: if constexpr (2 <= KK - 2) fwd_band<R, 2, KK, SREC>(sm, los, lo, src, ri, q0, q1, cnt, acc); break;
+              case 3: if constexpr (3 <= KK - 2) fwd_band<R, 3, KK, SREC>(sm, los, lo, src, ri, q0, q1, cnt, acc); break;
+              case 4: if constexpr (4 <= KK - 2) fwd_band<R, 4, KK, SREC>(sm, los, lo, src, ri, q0, q1, cnt, acc); break;
+              case 5: if constexpr (5 <= KK - 2) fwd_band<R, 5, KK, SREC>(sm, los, lo, src, ri, q0, q1, cnt, acc); break;
+              case 6: if constexpr (6 <= KK - 2) fwd_band<R, 6, KK, SREC>(sm, los, lo, src, ri, q0, q1, cnt, acc); break;
               default: break;
             }
           }
@@ -498,6 +539,7 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd5(Fwd5Args a) {
 
 struct Adj5Args {
   int n, na, npts, gstride, gy;
+  int norec, npair;    // counts copied to shared memory (SREC)
   const int *list;
   const int4 *orec;    // ib, pstart, pcount, 0
   const uint2 *pair;   // byte offsets of the Tb row and the h row in a buffer
@@ -511,7 +553,7 @@ struct Adj5Args {
 // (lib/train_module.f90:381-403 with C(a,b) folded into row scales).
 // Shared memory holds two buffers of [Tb rows | h rows]; the next item's
 // rows stream into one while the other is scaled and read.
-template <typename R, int NPB>
+template <typename R, int NPB, bool SREC>
 __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj5(Adj5Args a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char *sm = smem_raw;
@@ -521,6 +563,18 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj5(Adj5Args a) {
   const int n = a.n, na = a.na;
   const size_t plane = (size_t)na * n;
   const uint32_t bufb = 2 * na * 128;  // bytes per buffer
+  const int4 *orec = a.orec;
+  const uint2 *pair = a.pair;
+  if constexpr (SREC) {
+    // output records and pairs follow the two buffers; copied once
+    int4 *so = (int4 *)(sm + (size_t)2 * bufb);
+    uint2 *sp = (uint2 *)(so + a.norec);
+    for (int i = threadIdx.x; i < a.norec; i += blockDim.x) so[i] = __ldg(a.orec + i);
+    for (int i = threadIdx.x; i < a.npair / 2; i += blockDim.x)
+      ((uint4 *)sp)[i] = __ldg((const uint4 *)a.pair + i);
+    orec = so;
+    pair = sp;
+  }
   const R *sc = (const R *)a.sc;
   const int rs = __ldg(a.list + warp * 2), rn = __ldg(a.list + warp * 2 + 1);
   double gb = 0.0;
@@ -563,15 +617,15 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj5(Adj5Args a) {
     __syncthreads();
     R *Sb = (R *)a.Sb + pt * plane;
     for (int r = rs; r < rs + rn; ++r) {
-      const int4 o = __ldg(a.orec + r);  // ib, pstart, pcount
-      const uint2 *pp = a.pair + o.y;
-      uint2 q0 = __ldg(pp), q1 = __ldg(pp + 1);
+      const int4 o = SREC ? orec[r] : __ldg(orec + r);  // ib, pstart, pcount
+      const uint2 *pp = pair + o.y;
+      uint2 q0 = SREC ? pp[0] : __ldg(pp), q1 = SREC ? pp[1] : __ldg(pp + 1);
       R s0 = (R)0, s1 = (R)0;
       int e = 0;
       for (; e + 2 <= o.z; e += 2) {
         const uint2 u0 = q0, u1 = q1;
-        q0 = __ldg(pp + 2);
-        q1 = __ldg(pp + 3);
+        q0 = SREC ? pp[2] : __ldg(pp + 2);
+        q1 = SREC ? pp[3] : __ldg(pp + 3);
         pp += 2;
         s0 += srow<R>(sm, lc + u0.x) * srow<R>(sm, lc + u0.y);
         s1 += srow<R>(sm, lc + u1.x) * srow<R>(sm, lc + u1.y);
@@ -612,26 +666,102 @@ static int persistent_grid(const void *k, int threads, size_t smem, long items) 
   return (int)std::max(1L, std::min(g, items));
 }
 
+// ------------------------------------------------------------- autotuner
+// The v5 kernels come in variants that compute bit-identical outputs (table
+// records read from global memory, or copied once into the shared memory
+// left beside the state).  Which is faster depends on the precision and on
+// the table sizes, so the first launch for a (plan, kernel, width,
+// precision) with at least a few waves of work runs every variant once on
+// the caller's stream, timed with CUDA events, and keeps the fastest for the
+// later launches.  While the stream is being captured into a graph no
+// timing is possible and the default variant runs.  launch(v, last) runs
+// variant v; side effects that accumulate (the adjoint's bias gradient)
+// happen only when last is set, which it is for exactly one launch.
+struct TuneKey {
+  uint64_t plan;
+  int which, n, prec;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(plan, which, n, prec) < std::tie(o.plan, o.which, o.n, o.prec);
+  }
+};
+static std::map<TuneKey, int> g_tune;
+static std::mutex g_tune_mu;
+
+template <typename L>
+static int tuned_launch(const TuneKey &key, int nvar, int dflt, long items, cudaStream_t st,
+                        L launch) {
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return launch(it->second, true);
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (nvar < 2 || cudaStreamIsCapturing(st, &cs) != cudaSuccess ||
+      cs != cudaStreamCaptureStatusNone || items < (long)sm_count_b() * 8)
+    return launch(dflt, true);
+  cudaEvent_t e0, e1;
+  CKB(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    set_error("autotuner: cudaEventCreate failed");
+    return RC_DEVICE;
+  }
+  float best = 0.f;
+  int bv = dflt, rc = RC_OK;
+  // one untimed run of each first, so that module loading and first-touch
+  // costs do not favour the variant that runs later
+  for (int v = 0; v < nvar && rc == RC_OK; ++v) rc = launch(v, false);
+  for (int v = 0; v < nvar && rc == RC_OK; ++v) {
+    cudaEventRecord(e0, st);
+    rc = launch(v, v == nvar - 1);
+    cudaEventRecord(e1, st);
+    if (rc == RC_OK && cudaEventSynchronize(e1) == cudaSuccess) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (v == 0 || ms < best) {
+        best = ms;
+        bv = v;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = bv;
+  return RC_OK;  // every variant wrote the same values
+}
+
 template <typename R, int KK>
 static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int npts,
                          const void *S, void *T, void *h, bool train, cudaStream_t st) {
   constexpr int NPB = sizeof(R) == 8 ? 16 : 32;
   static_assert(NPB * sizeof(R) == 128, "one state row is 128 bytes");
-  const size_t smem = ((size_t)bp.nrows5 + t.na) * 128;
+  size_t smem = ((size_t)bp.nrows5 + t.na) * 128;
   if (!bp.f5_ok || smem > 227 * 1024 || n % (16 / (int)sizeof(R))) return RC_UNSUPPORTED;
   Fwd5Args a;
   a.n = n; a.na = t.na; a.npts = npts; a.iact = t.iact; a.dt_off = bp.dt_off5;
   a.nrows = bp.nrows5; a.gy = (n + NPB - 1) / NPB;
+  a.nrec32 = bp.nrec32;
   a.tpc = t.tpc; a.list = bp.f5_list; a.arec = (const int4 *)bp.f5_arec;
-  a.rec = (const uint2 *)bp.f5_rec; a.cpdst = bp.f5_cpdst;
+  a.rec = (const uint2 *)bp.f5_rec; a.rec32 = bp.f6_rec; a.cpdst = bp.f5_cpdst;
   a.sc = sizeof(R) == 8 ? (const void *)bp.sc64 : (const void *)bp.sc32;
   a.S = S; a.T = T; a.h = h;
-  auto k = train ? k_bell_fwd5<R, KK, NPB, true> : k_bell_fwd5<R, KK, NPB, false>;
-  CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int grid = persistent_grid((const void *)k, BELL_WORKERS * 32, smem, (long)npts * a.gy);
-  LAUNCH("k_bell_fwd", st, k<<<grid, BELL_WORKERS * 32, smem, st>>>(a));
-  CKB(cudaGetLastError());
-  return RC_OK;
+  // variant 0: records in global memory; 1: records in shared memory
+  const bool srec_fits = smem + (size_t)bp.nrec32 * 4 <= 227 * 1024;
+  auto launch = [&](int v, bool) -> int {
+    const bool srec = v == 1;
+    const size_t sm = smem + (srec ? (size_t)bp.nrec32 * 4 : 0);
+    auto k = srec ? (train ? k_bell_fwd5<R, KK, NPB, true, true> : k_bell_fwd5<R, KK, NPB, false, true>)
+                  : (train ? k_bell_fwd5<R, KK, NPB, true, false> : k_bell_fwd5<R, KK, NPB, false, false>);
+    CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int grid = persistent_grid((const void *)k, BELL_WORKERS * 32, sm, (long)npts * a.gy);
+    LAUNCH("k_bell_fwd", st, k<<<grid, BELL_WORKERS * 32, sm, st>>>(a));
+    CKB(cudaGetLastError());
+    return RC_OK;
+  };
+  return tuned_launch(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)}, srec_fits ? 2 : 1,
+                      srec_fits ? 1 : 0, (long)npts * a.gy, st, launch);
 }
 
 template <typename R, int KK>
@@ -697,19 +827,31 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
   const size_t smem = (size_t)2 * t.na * NPB * sizeof(R);
   if (smem > 227 * 1024) return RC_UNSUPPORTED;
   if (bp.a5_pair && (size_t)4 * t.na * 128 <= 227 * 1024 && n % (16 / (int)sizeof(R)) == 0) {
-    const size_t smem5 = (size_t)4 * t.na * 128;
+    size_t smem5 = (size_t)4 * t.na * 128;
     Adj5Args b;
     b.n = n; b.na = t.na; b.npts = npts; b.gstride = gstride; b.list = bp.aj_list;
     b.orec = (const int4 *)bp.a3_orec; b.pair = (const uint2 *)bp.a5_pair;
+    b.norec = bp.norec; b.npair = bp.npair5;
     b.sc = sizeof(R) == 8 ? (const void *)bp.sc64 : (const void *)bp.sc32;
     b.Tb = Tb; b.h = h; b.Sb = Sb; b.gbias = gbias;
     b.gy = (n + NPB - 1) / NPB;
-    auto k = k_bell_adj5<R, NPB>;
-    CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem5));
-    const int grid = persistent_grid((const void *)k, ADJ_WORKERS * 32, smem5, (long)npts * b.gy);
-    LAUNCH("k_bell_adj", st, k<<<grid, ADJ_WORKERS * 32, smem5, st>>>(b));
-    CKB(cudaGetLastError());
-    return RC_OK;
+    const size_t extra = (size_t)bp.norec * 16 + (size_t)bp.npair5 * 8;
+    const bool srec_fits = smem5 + extra <= 227 * 1024;
+    // variant 0: pairs in global memory; 1: pairs in shared memory
+    auto launch = [&](int v, bool last) -> int {
+      const bool srec = v == 1;
+      const size_t sm = smem5 + (srec ? extra : 0);
+      auto k = srec ? k_bell_adj5<R, NPB, true> : k_bell_adj5<R, NPB, false>;
+      CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      const int grid = persistent_grid((const void *)k, ADJ_WORKERS * 32, sm, (long)npts * b.gy);
+      Adj5Args bv = b;
+      if (!last) bv.gbias = nullptr;  // a timing run adds nothing
+      LAUNCH("k_bell_adj", st, k<<<grid, ADJ_WORKERS * 32, sm, st>>>(bv));
+      CKB(cudaGetLastError());
+      return RC_OK;
+    };
+    return tuned_launch(TuneKey{bp.id, 2, n, (int)sizeof(R)}, srec_fits ? 2 : 1,
+                        srec_fits ? 1 : 0, (long)npts * b.gy, st, launch);
   }
   Adj2Args a;
   a.n = n; a.na = t.na; a.npts = npts; a.gstride = gstride; a.list = bp.aj_list;

@@ -15,6 +15,7 @@ constexpr int ADJ_UNROLL = 2;     // pairs fetched ahead: 2 * ADJ_UNROLL
 
 struct DevBellPlan {
   bool ready = false;
+  uint64_t id = 0;              // distinct per upload (autotuner key)
   int workers = 0, k = 0, na = 0, nslot = 0;
   int *fw_list = nullptr, *fw_arec = nullptr, *fw_grec = nullptr;
   double *fw_gc64 = nullptr;
@@ -36,6 +37,8 @@ struct DevBellPlan {
   int nrows5 = 0, dt_off5 = 0;
   int *f5_list = nullptr, *f5_arec = nullptr, *f5_cpdst = nullptr;
   uint32_t *f5_rec = nullptr, *a5_pair = nullptr;
+  uint32_t *f6_rec = nullptr;   // forward records as row indices
+  int nrec32 = 0, norec = 0, npair5 = 0;
   double *sc64 = nullptr;  // [3][na]: a!, 1/a!, 1/a! (Tb, h, Sb scales)
   float *sc32 = nullptr;
   void release();

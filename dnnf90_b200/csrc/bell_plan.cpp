@@ -255,6 +255,9 @@ BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
     }
     // the kernels read two records ahead of the one they use
     for (int i = 0; i < 8; ++i) P.f5_rec.push_back(0);
+    for (size_t i = 0; i < P.f5_rec.size(); i += 2)
+      P.f6_rec.push_back((P.f5_rec[i] / ROW) | ((P.f5_rec[i + 1] / ROW) << 16));
+    while (P.f6_rec.size() % 4) P.f6_rec.push_back(0);  // whole 16-byte pieces
     P.f5_ok = bands_ok && k <= 8 && (size_t)(P.nrows5 + na) * ROW <= 227 * 1024;
   }
 

@@ -62,6 +62,7 @@ struct BellPlan {
                                    //         B run of a (or -1), U/V pair of a (or -1), 0, band_lo
   std::vector<uint32_t> f5_rec;    // [*][2]
   std::vector<int> f5_cpdst;       // [na]: byte offset of the level-1 copy of S_a, or -1
+  std::vector<uint32_t> f6_rec;    // the f5 records as rows: x row | z row << 16
   // adjoint, v3: Sb_b b! = sum_{a >= b} (a! Tb_a) (h_{a-b} / (a-b)!), the
   // pair coefficient C(a,b) = a!/(b!(a-b)!) folded into per-row scales
   std::vector<int> a3_orec;   // [*][4]: ib, pstart, pcount, 0
