@@ -332,16 +332,24 @@ def main():
             roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                     "frac": achieved / hbm, "traffic": None, "kernel": name,
                     "launches": cnt, "avg_launch_ms": tot_ms / cnt,
-                    "peak_source": peak_kind}
+                    "algorithmic_bytes_per_launch": bytes_total / cnt,
+                    "peak_source": peak_kind,
+                    "note": "the Bell step is bound by shared-memory and issue throughput, "
+                            "not HBM; frac is its HBM fraction"}
         else:
             roof = {"bound": "tensor", "achieved": None, "peak": tc, "unit": "TFLOP/s",
                     "frac": None, "traffic": None, "kernel": name, "launches": cnt,
                     "avg_launch_ms": tot_ms / cnt, "peak_source": peak_kind}
         tf = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tf):
+        if os.path.exists(tf) and name in per_pt:
             t = json.load(open(tf)).get(roof["kernel"])
             if t:
-                roof["traffic"] = t.get("bytes_per_launch")
+                # points one launch carries through one layer, times the
+                # measured DRAM bytes per point and layer
+                pts_per_launch = npts * len(hid[1:]) * args.prof_steps / cnt
+                roof["traffic"] = t["bytes_per_point_layer"] * pts_per_launch
+                roof["traffic_per_algorithmic"] = (t["bytes_per_point_layer"]
+                                                   / t["algorithmic_bytes_per_point_layer"])
         roof["kernel_shares"] = {k: round(v[1] / sum(x[1] for x in prof.values()), 4)
                                  for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
     net.free()
