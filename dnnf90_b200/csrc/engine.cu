@@ -730,11 +730,15 @@ struct AdjL2vArgs {
 //   dW_2[j][0] += Sb^0,  dW_2[j][1 + i] += Sb^0 x_i + Sb^{e_i}.
 template <typename R, int D0>
 __global__ void __launch_bounds__(256) k_adj_l2v(AdjL2vArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int *up = (int *)smem_raw;  // [na][D0], copied once per block
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int j = blockIdx.y * 32 + lane;
   const bool act = j < a.n;
   const int jc = act ? j : a.n - 1;
   const size_t plane = (size_t)a.na * a.n;
+  for (int e = threadIdx.x; e < a.na * D0; e += blockDim.x) up[e] = __ldg(a.up + e);
+  __syncthreads();
   double acc[D0 + 1];
 #pragma unroll
   for (int i = 0; i <= D0; ++i) acc[i] = 0.0;
@@ -744,13 +748,35 @@ __global__ void __launch_bounds__(256) k_adj_l2v(AdjL2vArgs a) {
     R s[D0 + 1];
 #pragma unroll
     for (int i = 0; i <= D0; ++i) s[i] = (R)0;
-#pragma unroll 2
-    for (int g = 0; g < a.na; ++g) {
+    // four multi-indices per step: their loads are independent and issue
+    // together; a missing child (u < 0) reads row 0 with weight 0
+    int g = 0;
+    for (; g + 4 <= a.na; g += 4) {
+      R hv[4], tv[4], cv[4][D0], wv[4][D0];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        hv[q] = H[(size_t)(g + q) * a.n];
+        tv[q] = Tb[(size_t)(g + q) * a.n];
+#pragma unroll
+        for (int i = 0; i < D0; ++i) {
+          const int u = up[(g + q) * D0 + i];
+          wv[q][i] = u >= 0 ? (R)(u >> 16) : (R)0;
+          cv[q][i] = Tb[(size_t)(u >= 0 ? (u & 0xffff) : 0) * a.n];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        s[0] += tv[q] * hv[q];
+#pragma unroll
+        for (int i = 0; i < D0; ++i) s[1 + i] += wv[q][i] * cv[q][i] * hv[q];
+      }
+    }
+    for (; g < a.na; ++g) {
       const R hg = H[(size_t)g * a.n];
       s[0] += Tb[(size_t)g * a.n] * hg;
 #pragma unroll
       for (int i = 0; i < D0; ++i) {
-        const int u = __ldg(a.up + g * D0 + i);
+        const int u = up[g * D0 + i];
         if (u >= 0) s[1 + i] += (R)(u >> 16) * Tb[(size_t)(u & 0xffff) * a.n] * hg;
       }
     }
@@ -787,15 +813,23 @@ __global__ void __launch_bounds__(256) k_output_fwdv(OutArgs a) {
   double lsum = 0.0;
   for (long pt = (long)blockIdx.x * nw + warp; pt < a.npts; pt += (long)gridDim.x * nw) {
     const R *Tm = (const R *)a.Tm + pt * plane;
-    for (int ia = 0; ia < na; ++ia) {
-      const R *row = Tm + (size_t)ia * m;
-      for (int o = 0; o < nout; ++o) {
-        const double *w = a.W + (size_t)o * (m + 1) + 1;
-        double part = 0.0;
-        for (int i = lane; i < m; i += 32) part += __ldg(w + i) * (double)row[i];
-        part = warp_sum(part);
-        if (lane == 0) {
-          const double v = (ia == 0 ? a.W[(size_t)o * (m + 1)] : 0.0) + part;
+    for (int o = 0; o < nout; ++o) {
+      const double *w = a.W + (size_t)o * (m + 1) + 1;
+      // four multi-indices per step, independent loads and reductions
+      for (int ia0 = 0; ia0 < na; ia0 += 4) {
+        double part[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int i = lane; i < m; i += 32) {
+          const double wi = __ldg(w + i);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (ia0 + q < na) part[q] += wi * (double)Tm[(size_t)(ia0 + q) * m + i];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) part[q] = warp_sum(part[q]);
+        if (lane < 4 && ia0 + lane < na) {
+          const int ia = ia0 + lane;
+          const double pv = lane == 0 ? part[0] : lane == 1 ? part[1] : lane == 2 ? part[2] : part[3];
+          const double v = (ia == 0 ? a.W[(size_t)o * (m + 1)] : 0.0) + pv;
           tl[o * na + ia] = v;
           if (a.out) a.out[(pt * (size_t)na + ia) * nout + o] = v;
         }
@@ -1317,9 +1351,12 @@ static int launch_layer2v(const DevTables &t, int n, int npts, const double *X, 
 template <typename R, int D0>
 static int adjl2v_k(const AdjL2vArgs &a, cudaStream_t st) {
   const void *k = (const void *)k_adj_l2v<R, D0>;
+  const size_t smem = (size_t)a.na * D0 * sizeof(int);
+  if (smem > 96 * 1024) return RC_UNSUPPORTED;
+  CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int gy = (a.n + 31) / 32;
-  const int gx = std::max(1, std::min((a.npts + 7) / 8, occ_grid(k, 256, 0) / gy));
-  LAUNCH("k_bell_adj_l2", st, (k_adj_l2v<R, D0><<<dim3(gx, gy), 256, 0, st>>>(a)));
+  const int gx = std::max(1, std::min((a.npts + 7) / 8, occ_grid(k, 256, smem) / gy));
+  LAUNCH("k_bell_adj_l2", st, (k_adj_l2v<R, D0><<<dim3(gx, gy), 256, smem, st>>>(a)));
   CK(cudaGetLastError());
   return RC_OK;
 }
