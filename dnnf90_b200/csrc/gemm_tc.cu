@@ -194,6 +194,7 @@ struct Args {
   int ntn;              // N tiles
   int kchunk;           // DW: K blocks per TMEM partial
   int kblocks_per_cta;  // DW: K blocks per block of the grid
+  int gcol0;            // DW: first column of G written (1 past the bias column, or 0)
   int *flag;            // wait time-out / error flag
 };
 
@@ -222,6 +223,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_gemm(Args g) {
   const int ntn = g.ntn;
   const int tn = blockIdx.y;  // N tile of this block
   const int n0 = tn * BN;
+  const int m0 = (MODE == MODE_DW) ? blockIdx.z * BM : 0;  // DW: output-row tile
   // tile sequence of this block
   int tiles_m = 0, first_m = 0, step_m = 1, kb_begin = 0, kb_end = 0;
   if (MODE == MODE_DW) {
@@ -330,8 +332,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_gemm(Args g) {
           const int e = it * NPROD + t;
           const int kr = e >> 5, j = (e & 31) * 4;
           const int gr = r0 + kr;
-          va[it] = (gr < g.K && j < Mdw) ? __ldg((const float4 *)(g.A + (size_t)gr * g.lda + j))
-                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+          va[it] = (gr < g.K && m0 + j < Mdw)
+                       ? __ldg((const float4 *)(g.A + (size_t)gr * g.lda + m0 + j))
+                       : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
         for (int it = 0; it < PB; ++it) {
@@ -519,8 +522,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_gemm(Args g) {
         mbar_arrive(tempty + buf);
         if (++buf == 2) { buf = 0; tph ^= 1u; }
       }
-      if (row < g.M && nch > 0) {
-        double *dst = g.G + (size_t)row * g.gld + 1 + n0;
+      if (m0 + row < g.M && nch > 0) {
+        double *dst = g.G + (size_t)(m0 + row) * g.gld + g.gcol0 + n0;
 #pragma unroll
         for (int i = 0; i < 64; ++i)
           if (n0 + i < g.N) atomicAdd(dst + i, acc[i]);
@@ -744,7 +747,7 @@ int gemm_tc_dw(const DevNet *net, int l, int M, int n, int m, const void *Sb, co
   std::memset(&a, 0, sizeof a);
   a.mode = tc::MODE_DW; a.M = n; a.N = m; a.K = M; a.na = 1;
   a.A = (const float *)Sb; a.lda = n; a.B = (const float *)Tm; a.ldb = m;
-  a.G = G; a.gld = m + 1; a.BN = BN; a.ntn = ntn; a.kchunk = 8;
+  a.G = G; a.gld = m + 1; a.gcol0 = 1; a.BN = BN; a.ntn = ntn; a.kchunk = 8;
   a.kblocks_per_cta = (nkb_all + ctas_k - 1) / ctas_k;
   a.flag = w->flag;
   const size_t stage = 3 * (8 * 2 * 1024) + 3 * (8 * 1 * 1024);
@@ -753,7 +756,44 @@ int gemm_tc_dw(const DevNet *net, int l, int M, int n, int m, const void *Sb, co
   return launch(a, tc::MODE_DW, grid, smem, st);
 }
 
-int gemm_tc_syrk(const double *, int, int, double *, cudaStream_t) { return RC_UNSUPPORTED; }
+// G[i][j] += sum_r J[r][i] J[r][j] over an FP32 copy J[nrow][ldj] (ldj a
+// multiple of 4, zero past nw): the DW form with both operands J, output
+// tiles of 128 rows x 64 columns, the row reduction split across blocks.
+int gemm_tc_syrk(const float *J, int nrow, int nw, int ldj, double *G, cudaStream_t st) {
+  if (!gemm_tc_available() || nrow < 1 || nw < 1 || ldj % 4 || ldj < nw) return RC_UNSUPPORTED;
+  static int *flag = nullptr;
+  if (!flag) {
+    CKT(cudaMalloc(&flag, sizeof(int)));
+    CKT(cudaMemset(flag, 0, sizeof(int)));
+  }
+  const int BN = 64;
+  const int ntn = (nw + BN - 1) / BN, ntm = (nw + tc::BM - 1) / tc::BM;
+  if (ntm > 65535) return RC_UNSUPPORTED;
+  const int nkb_all = (nrow + tc::BK - 1) / tc::BK;
+  const long tiles = (long)ntn * ntm;
+  const int ctas_k = (int)std::max<long>(1, std::min<long>(nkb_all, 2 * sm_count_t() / std::max(1L, tiles)));
+  tc::Args a;
+  std::memset(&a, 0, sizeof a);
+  a.mode = tc::MODE_DW; a.M = nw; a.N = nw; a.K = nrow; a.na = 1;
+  a.A = J; a.lda = ldj; a.B = J; a.ldb = ldj;
+  a.G = G; a.gld = nw; a.gcol0 = 0; a.BN = BN; a.ntn = ntn; a.kchunk = 8;
+  a.kblocks_per_cta = (nkb_all + ctas_k - 1) / ctas_k;
+  a.flag = flag;
+  const size_t stage = 3 * (8 * 2 * 1024) + 3 * (8 * 1 * 1024);
+  const size_t smem = 1024 + 3 * stage + 1024;
+  dim3 grid((nkb_all + a.kblocks_per_cta - 1) / a.kblocks_per_cta, ntn, ntm);
+  int rc = launch(a, tc::MODE_DW, grid, smem, st);
+  if (rc) return rc;
+  int h = 0;
+  CKT(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKT(cudaStreamSynchronize(st));
+  if (h) {
+    cudaMemset(flag, 0, sizeof(int));
+    set_error("tensor-core metric: an mbarrier wait timed out (code " + std::to_string(h) + ")");
+    return RC_DEVICE;
+  }
+  return RC_OK;
+}
 
 int gemm_tc_flag(const DevNet *net, cudaStream_t st) {
   TcWeights *w = (TcWeights *)net->tc;

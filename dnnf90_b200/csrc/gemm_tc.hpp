@@ -34,7 +34,9 @@ int gemm_tc_dw(const DevNet *net, int l, int M, int n, int m, const void *Sb,
 
 // G[i][j] += sum_r J[r][i] J[r][j] on the lower triangle (FP64 G), J in FP64
 // rows carried as three bf16 terms on the tensor cores
-int gemm_tc_syrk(const double *J, int nrow, int nw, double *G, cudaStream_t st);
+// G[i][j] += sum_r J[r][i] J[r][j] from an FP32 copy J[nrow][ldj] (ldj a
+// multiple of 4, columns nw..ldj-1 zero), G [nw][nw] FP64; synchronises st
+int gemm_tc_syrk(const float *J, int nrow, int nw, int ldj, double *G, cudaStream_t st);
 
 int weights_to_f32(const double *w, float *w32, size_t n, cudaStream_t st);
 

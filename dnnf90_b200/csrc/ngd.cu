@@ -217,6 +217,18 @@ __global__ void __launch_bounds__(1024) k_chol_solve(const double *G, int nw, do
   }
 }
 
+// FP32 copy of the rows with a padded leading dimension (zero past nw), the
+// operand of the tensor-core metric
+__global__ void k_rows_f32(const double *rows, int nrow, int nw, float *J, int ldj) {
+  const long tot = (long)nrow * ldj;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long)gridDim.x * blockDim.x) {
+    const long r = e / ldj;
+    const int c = (int)(e - r * ldj);
+    J[e] = c < nw ? (float)rows[(size_t)r * nw + c] : 0.f;
+  }
+}
+
 int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
                double mu, double *u, int prec, cudaStream_t st) {
   double *G = nullptr;
@@ -227,7 +239,17 @@ int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
   CKN(cudaMemsetAsync(info, 0, sizeof(int), st));
   const int tiles = (nw + 63) / 64;
   int rc = RC_UNSUPPORTED;
-  if (prec == PREC_SPLIT && gemm_tc_available()) rc = gemm_tc_syrk(rows, nrow, nw, G, st);
+  if (prec == PREC_SPLIT && gemm_tc_available()) {
+    // the metric on the tensor cores: split-BF16 products of the FP32 rows
+    // with FP32 accumulation per 512 rows, FP64 across them
+    const int ldj = (nw + 3) / 4 * 4;
+    float *J = nullptr;
+    if (cudaMalloc(&J, sizeof(float) * (size_t)nrow * ldj) == cudaSuccess) {
+      LAUNCH("k_rows_f32", st, k_rows_f32<<<1024, 256, 0, st>>>(rows, nrow, nw, J, ldj));
+      rc = gemm_tc_syrk(J, nrow, nw, ldj, G, st);
+      cudaFree(J);
+    }
+  }
   if (rc == RC_UNSUPPORTED) {
     rc = RC_OK;
     int rchunk = std::max(64, (nrow + 7) / 8);

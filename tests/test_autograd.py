@@ -153,6 +153,6 @@ def test_nested_autograd_reference():
     Tt = np.stack([v.detach().cpu().numpy() for v in (u, u_t, u_x, u_xxx)], axis=1)
     Td = T[:, 0, [0, slots["t"], slots["x"], slots["xxx"]]]
     assert rel_err(Td, Tt) < 1e-11
-    assert abs(L - float(Lt)) <= 1e-11 * abs(float(Lt))
+    assert abs(L - float(Lt.detach())) <= 1e-11 * abs(float(Lt.detach()))
     assert rel_err(g, gt.cpu().numpy()) < 1e-10, rel_err(g, gt.cpu().numpy())
     net.free()

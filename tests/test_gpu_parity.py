@@ -193,3 +193,37 @@ def test_directional_known_answers_on_the_device(golden):
         assert abs(loss / lref - 1) < 1e-11, (K, loss, lref)
         assert abs(g.read()[1] / gref - 1) < 5e-9
         r.free(); g.free(); net.free()
+
+
+def test_ngd_step_at_heat_scale():
+    """Damped Gauss-Newton step on the heat residual at full size: 4096
+    points, 3-64-64-1 (4481 weights).  The split path forms J^T J on the
+    tensor cores (split-BF16 products, FP32 accumulation per 512 rows, FP64
+    across them) and solves in FP64; both are judged by backward error on
+    the FP64 system, the metric itself against numpy."""
+    dims = [3, 64, 64, 1]
+    seeds = [[1, 0, 0], [0, 2, 0], [0, 0, 2]]
+    ts = api.TableSet(3, 2, seeds)
+    terms = [(1.0, ts.slot((1, 0, 0)), 0), (-1.0, ts.slot((0, 2, 0)), 0),
+             (-1.0, ts.slot((0, 0, 2)), 0)]
+    w = xavier_weights(dims, 5)
+    X = np.random.default_rng(8).uniform(0, 1, (4096, 3))
+    net = _net(ts, dims, w, api.PREC_F64)
+    r = api.SeedRule(api.SEED_JROW, terms)
+    rows, resid, _ = api.jacobian_rows(net, X, r)
+    assert rows.shape == (4096, 4481)
+    nb, mu = len(X), 1e-6
+    b = (resid[:, None] * rows).sum(axis=0)
+    G = rows.T @ rows / nb + mu * np.eye(rows.shape[1])
+    bn = b / nb
+    v = np.random.default_rng(0).normal(size=G.shape[0])
+    for _ in range(30):  # power iteration for ||G||_2
+        v = G @ v
+        v /= np.linalg.norm(v)
+    g2 = float(v @ (G @ v))
+    for prec, bound in ((api.PREC_F64, 1e-12), (api.PREC_SPLIT, 1e-6)):
+        u = api.ngd_step(net, rows, b, nb, mu, prec)
+        assert np.all(np.isfinite(u))
+        berr = np.linalg.norm(G @ u - bn) / (g2 * np.linalg.norm(u) + np.linalg.norm(bn))
+        assert berr < bound, (prec, berr)
+    r.free(); net.free()
