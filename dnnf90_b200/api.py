@@ -43,7 +43,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_backward_dev", "dnnf90_grad_rule_dev", "dnnf90_jrow_dev",
     "dnnf90_twork_set_chunk", "dnnf90_last_error", "dnnf90_device_available",
     "dnnf90_launch_count", "dnnf90_profile_enable", "dnnf90_profile_read",
-    "dnnf90_ngd_step_noalloc",
+    "dnnf90_ngd_step_noalloc", "dnnf90_committee_step", "dnnf90_committee_info",
 ]
 
 _lib = None
@@ -121,6 +121,8 @@ def lib():
         "dnnf90_profile_enable": [i],
         "dnnf90_profile_read": [ctypes.c_char_p, i],
         "dnnf90_ngd_step_noalloc": [i, i, p, p, i, d, p, p],
+        "dnnf90_committee_step": [i, pi, pi, pi, pi, p, p, p, p],
+        "dnnf90_committee_info": [pi, P(ctypes.c_float)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -350,3 +352,29 @@ def ngd_step(net: Net, rows, b, nb: int, mu: float, prec: int = PREC_F64):
     call("dnnf90_ngd_step", net.nid, rows.shape[0], _pd(rows), _pd(b), int(nb), float(mu),
          int(prec), _pd(u))
     return u
+
+
+def committee_step(nets, rules, xs, grads, loss, stream=None):
+    """One training step of independent networks in one CUDA graph
+    (dnnf90_committee_step).  xs, grads: per-member torch CUDA tensors
+    (points [npts][d0] FP64, gradients [nw] FP64, overwritten); loss: a
+    torch CUDA FP64 tensor [len(nets)] (overwritten).  Returns (policy,
+    graph ms) of the graph that ran."""
+    n = len(nets)
+    ia = ctypes.c_int * n
+    pa = ctypes.c_void_p * n
+    nids = ia(*[m.nid for m in nets])
+    tids = ia(*[m.tid for m in nets])
+    rids = ia(*[r.rid for r in rules])
+    npts = ia(*[int(x.shape[0]) for x in xs])
+    xp = pa(*[x.data_ptr() for x in xs])
+    gp = pa(*[g.data_ptr() for g in grads])
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream().cuda_stream
+    call("dnnf90_committee_step", n, nids, tids, rids, npts, ctypes.cast(xp, ctypes.c_void_p),
+         ctypes.cast(gp, ctypes.c_void_p), loss.data_ptr(), stream)
+    pol = ctypes.c_int(-1)
+    ms = ctypes.c_float(0.0)
+    lib().dnnf90_committee_info(ctypes.byref(pol), ctypes.byref(ms))
+    return pol.value, ms.value

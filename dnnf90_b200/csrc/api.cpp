@@ -179,7 +179,11 @@ int work_stream(WorkH &w) {
 }
 
 // planes for up to want points (bounded by a device memory budget)
-int work_planes(WorkH &w, NetH &n, int want, bool exact) {
+// drops cached committee graphs that use a network or work space being freed
+void comm_forget(int nid, int tid);
+
+// device bytes of one point's planes on a network's work space
+size_t plane_bytes_per_point(const NetH &n) {
   const size_t rsz = n.prec == PREC_F64 ? 8 : 4;
   size_t per = 0;
   int nmax = 0;
@@ -187,6 +191,11 @@ int work_planes(WorkH &w, NetH &n, int want, bool exact) {
   for (int l = 2; l < n.nlayer; ++l) per += 2 * (size_t)n.ts.na * n.dims[l - 1] * rsz;
   per += 3 * (size_t)n.ts.na * nmax * rsz;
   per += 2 * (size_t)n.ts.na * n.dims[n.nlayer - 1] * 8 + n.ts.d0 * 8 + 1024;
+  return per;
+}
+
+int work_planes(WorkH &w, NetH &n, int want, bool exact) {
+  const size_t per = plane_bytes_per_point(n);
   // at most 48 GiB, and at most half of what is free with this work
   // space's own planes counted as free (so the cap does not grow by
   // re-counting them on every call)
@@ -701,6 +710,7 @@ int dnnf90_net_set_layer(int nid, int l, const double *wrow) {
 int dnnf90_net_free(int nid) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (bad_net(nid)) return RC_BAD_ARG;
+  comm_forget(nid, 0);
   NetH &n = g_net[nid];
   n.dt.release();
   n.dn.release();
@@ -792,6 +802,7 @@ int dnnf90_twork_free(int tid) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (tid < 1 || tid > MAXH || !g_twk[tid].used) return RC_BAD_ARG;
   flush_queue(tid);
+  comm_forget(0, tid);
   free_work(g_twk[tid]);
   return RC_OK;
 }
@@ -1162,6 +1173,290 @@ int dnnf90_jrow_dev(int nid, int tid, int npts, const double *x_dev, int rid,
   a.npts = npts; a.X = x_dev; a.out = tm_dev; a.rows = rows_dev;
   a.train = true; a.prec = n.prec;
   return dev_finish(n, st, run_batch(n.dt, n.dn, g_rule[rid].d, w.p, a, st));
+}
+
+
+// ------------------------------------------------------------- committee
+extern "C++" {
+namespace {
+// One committee: its members, the streams and events of its graph, and the
+// instantiated graph with the device addresses it baked in.
+struct Committee {
+  std::vector<int> nids, tids, rids, npts;
+  std::vector<const double *> x;
+  std::vector<double *> g;
+  double *loss = nullptr;
+  cudaStream_t caller = nullptr;
+  cudaStream_t origin = nullptr;  // private stream the graph is captured on and
+                                  // replayed on (the caller's may be the legacy
+                                  // stream, which cannot be captured)
+  cudaEvent_t ready = nullptr;    // caller's work before the step
+  std::vector<cudaStream_t> st;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<uintptr_t> sig;
+  std::vector<double> work;
+  int policy = -1;
+  float ms = 0.f;
+  ~Committee() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (auto s : st) if (s) cudaStreamDestroy(s);
+    for (auto e : join) if (e) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (ready) cudaEventDestroy(ready);
+    if (origin) cudaStreamDestroy(origin);
+  }
+};
+std::vector<std::unique_ptr<Committee>> g_comm;  // most recent last
+int g_comm_policy = -1;
+float g_comm_ms = 0.f;
+
+// device addresses a captured graph depends on
+std::vector<uintptr_t> comm_signature(const Committee &C) {
+  std::vector<uintptr_t> v;
+  for (size_t i = 0; i < C.nids.size(); ++i) {
+    const NetH &n = g_net[C.nids[i]];
+    const WorkH &w = g_twk[C.tids[i]];
+    const RuleH &r = g_rule[C.rids[i]];
+    v.push_back((uintptr_t)w.p.base);
+    v.push_back((uintptr_t)w.p.cap_pts);
+    v.push_back((uintptr_t)n.dn.w64);
+    v.push_back((uintptr_t)n.dn.w32);
+    v.push_back((uintptr_t)n.dn.tc);
+    v.push_back((uintptr_t)n.dt.bp.id);
+    v.push_back((uintptr_t)r.d.coeff);
+    v.push_back((uintptr_t)n.prec);
+  }
+  return v;
+}
+
+// SMs member i may fill under a policy: 0 in proportion to its work,
+// 1 in proportion to the square root of its work, 2 no cap
+int comm_cap(const Committee &C, int i, int policy) {
+  if (policy == 2) return 0;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  double tot = 0.0;
+  for (double wv : C.work) tot += policy == 0 ? wv : std::sqrt(wv);
+  const double mine = policy == 0 ? C.work[i] : std::sqrt(C.work[i]);
+  return std::max(1, (int)std::lround(sms * mine / std::max(tot, 1e-300)));
+}
+
+// every member's zeroing and forward -> seed -> adjoint on its own stream,
+// forked from and joined back into the origin stream
+int comm_issue(Committee &C, int policy) {
+  int rc = ck(cudaEventRecord(C.fork, C.origin), "committee fork");
+  for (size_t i = 0; i < C.nids.size() && !rc; ++i) {
+    NetH &n = g_net[C.nids[i]];
+    WorkH &w = g_twk[C.tids[i]];
+    RuleH &r = g_rule[C.rids[i]];
+    cudaStream_t s = C.st[i];
+    if ((rc = ck(cudaStreamWaitEvent(s, C.fork, 0), "committee wait"))) break;
+    if ((rc = ck(cudaMemsetAsync(C.g[i], 0, sizeof(double) * n.w.size(), s), "memset"))) break;
+    if ((rc = ck(cudaMemsetAsync(C.loss + i, 0, sizeof(double), s), "memset"))) break;
+    set_grid_cap(comm_cap(C, (int)i, policy));
+    BatchArgs a;
+    a.npts = C.npts[i]; a.X = C.x[i]; a.grad = C.g[i]; a.loss = C.loss + i;
+    a.train = true; a.prec = n.prec;
+    rc = run_batch(n.dt, n.dn, r.d, w.p, a, s);
+    set_grid_cap(0);
+    if (rc) break;
+    if ((rc = ck(cudaEventRecord(C.join[i], s), "committee join"))) break;
+    rc = ck(cudaStreamWaitEvent(C.origin, C.join[i], 0), "committee wait");
+  }
+  return rc;
+}
+
+int comm_capture(Committee &C, int policy, cudaGraphExec_t *exec) {
+  int rc = ck(cudaStreamBeginCapture(C.origin, cudaStreamCaptureModeRelaxed), "begin capture");
+  if (rc) return rc;
+  int rci = comm_issue(C, policy);
+  cudaGraph_t graph = nullptr;
+  rc = ck(cudaStreamEndCapture(C.origin, &graph), "end capture");
+  if (rci) rc = rci;
+  if (!rc) rc = ck(cudaGraphInstantiate(exec, graph, 0), "graph instantiate");
+  if (graph) cudaGraphDestroy(graph);
+  return rc;
+}
+
+// replays of an instantiated graph, the second one timed
+int comm_time(Committee &C, cudaGraphExec_t exec, float *ms) {
+  cudaEvent_t e0, e1;
+  int rc = ck(cudaEventCreate(&e0), "event");
+  if (rc) return rc;
+  if ((rc = ck(cudaEventCreate(&e1), "event"))) { cudaEventDestroy(e0); return rc; }
+  rc = ck(cudaGraphLaunch(exec, C.origin), "graph launch");
+  if (!rc) rc = ck(cudaEventRecord(e0, C.origin), "event");
+  if (!rc) rc = ck(cudaGraphLaunch(exec, C.origin), "graph launch");
+  if (!rc) rc = ck(cudaEventRecord(e1, C.origin), "event");
+  if (!rc) rc = ck(cudaEventSynchronize(e1), "graph replay");
+  if (!rc) cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+// First call of a committee: work spaces under one memory budget, one
+// untimed step outside any graph (it settles every allocation and the Bell
+// kernels' variant choices), then one graph per SM-sharing policy, each
+// replayed and timed; the fastest is kept.
+int comm_build(Committee &C) {
+  const int nn = (int)C.nids.size();
+  C.exec = nullptr;
+  if (C.st.empty()) {
+    C.st.assign(nn, nullptr);
+    C.join.assign(nn, nullptr);
+    int rc = ck(cudaEventCreateWithFlags(&C.fork, cudaEventDisableTiming), "event");
+    if (!rc) rc = ck(cudaEventCreateWithFlags(&C.ready, cudaEventDisableTiming), "event");
+    if (!rc) rc = ck(cudaStreamCreateWithFlags(&C.origin, cudaStreamNonBlocking), "stream");
+    for (int i = 0; i < nn && !rc; ++i) {
+      rc = ck(cudaStreamCreateWithFlags(&C.st[i], cudaStreamNonBlocking), "stream");
+      if (!rc) rc = ck(cudaEventCreateWithFlags(&C.join[i], cudaEventDisableTiming), "event");
+    }
+    if (rc) return rc;
+  }
+  // memory: half of what is free (the members' own planes counted as free)
+  // split in proportion to each member's need
+  size_t freeb = 0, totb = 0, own = 0;
+  cudaMemGetInfo(&freeb, &totb);
+  double need = 0.0;
+  for (int i = 0; i < nn; ++i) {
+    own += g_twk[C.tids[i]].p.bytes;
+    need += (double)C.npts[i] * plane_bytes_per_point(g_net[C.nids[i]]);
+  }
+  const double budget = 0.5 * (double)(freeb + own);
+  const double scale = std::min(1.0, budget / std::max(need, 1.0));
+  C.work.assign(nn, 0.0);
+  for (int i = 0; i < nn; ++i) {
+    NetH &n = g_net[C.nids[i]];
+    WorkH &w = g_twk[C.tids[i]];
+    w.chunk = std::max(std::min(C.npts[i], 64), (int)std::floor(C.npts[i] * scale));
+    w.kept = false;
+    int rc = work_planes(w, n, C.npts[i], false);
+    if (rc) return rc;
+    double per = 0.0;
+    for (int l = 2; l < n.nlayer; ++l)
+      per += (double)n.dims[l - 1] * ((double)n.ts.fq_ib.size() + n.ts.pair_ia.size() + 2.0 * n.ts.na);
+    C.work[i] = per * C.npts[i];
+  }
+  int rc = ck(cudaEventRecord(C.ready, C.caller), "event");
+  if (!rc) rc = ck(cudaStreamWaitEvent(C.origin, C.ready, 0), "wait");
+  if (!rc) rc = comm_issue(C, 0);
+  if (!rc) rc = ck(cudaStreamSynchronize(C.origin), "committee warm-up");
+  if (rc) return rc;
+  float best = 0.f;
+  for (int pol = 0; pol < 3; ++pol) {
+    cudaGraphExec_t ex = nullptr;
+    if ((rc = comm_capture(C, pol, &ex))) return rc;
+    float ms = 0.f;
+    if ((rc = comm_time(C, ex, &ms))) {
+      cudaGraphExecDestroy(ex);
+      return rc;
+    }
+    if (!C.exec || ms < best) {
+      if (C.exec) cudaGraphExecDestroy(C.exec);
+      C.exec = ex;
+      best = ms;
+      C.policy = pol;
+    } else {
+      cudaGraphExecDestroy(ex);
+    }
+  }
+  C.ms = best;
+  C.sig = comm_signature(C);
+  return RC_OK;
+}
+
+void comm_forget(int nid, int tid) {
+  if (g_comm.empty()) return;
+  cudaDeviceSynchronize();  // no replay of a graph may still run on these planes
+  for (size_t i = 0; i < g_comm.size();) {
+    const Committee &c = *g_comm[i];
+    const bool hit = std::find(c.nids.begin(), c.nids.end(), nid) != c.nids.end() ||
+                     std::find(c.tids.begin(), c.tids.end(), tid) != c.tids.end();
+    if (hit) g_comm.erase(g_comm.begin() + i);
+    else ++i;
+  }
+}
+}  // namespace
+}  // extern "C++"
+
+int dnnf90_committee_step(int nnet, const int *nids, const int *tids, const int *rids,
+                          const int *npts, const double *const *x_dev, double *const *grad_dev,
+                          double *loss_dev, void *stream) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (nnet < 1 || nnet > MAXH || !nids || !tids || !rids || !npts || !x_dev || !grad_dev ||
+      !loss_dev)
+    return RC_BAD_ARG;
+  for (int i = 0; i < nnet; ++i) {
+    if (check_train(nids[i], tids[i], 0, false)) return RC_BAD_ARG;
+    if (bad_rule(rids[i]) || g_rule[rids[i]].r.kind == SEED_JROW) return RC_BAD_ARG;
+    if (npts[i] < 1 || !x_dev[i] || !grad_dev[i]) return RC_BAD_ARG;
+    for (int k = 0; k < i; ++k)
+      if (tids[k] == tids[i]) {
+        set_error("committee members need distinct training work spaces");
+        return RC_BAD_ARG;
+      }
+  }
+  int rc = device_ready();
+  if (rc) return rc;
+  cudaStream_t caller = (cudaStream_t)stream;
+  // weights, tables and rules on the device (rewritten in place when they
+  // change, outside the graph)
+  for (int i = 0; i < nnet; ++i) {
+    NetH &n = g_net[nids[i]];
+    flush_for_net(nids[i]);
+    if ((rc = net_device(n, caller))) return rc;
+    if ((rc = rule_device(g_rule[rids[i]], n.ts))) return rc;
+  }
+  Committee *C = nullptr;
+  for (auto &c : g_comm)
+    if (c->caller == caller && c->loss == loss_dev &&
+        c->nids == std::vector<int>(nids, nids + nnet) &&
+        c->tids == std::vector<int>(tids, tids + nnet) &&
+        c->rids == std::vector<int>(rids, rids + nnet) &&
+        c->npts == std::vector<int>(npts, npts + nnet) &&
+        c->x == std::vector<const double *>(x_dev, x_dev + nnet) &&
+        c->g == std::vector<double *>(grad_dev, grad_dev + nnet))
+      C = c.get();
+  if (!C) {
+    if (g_comm.size() >= 8) g_comm.erase(g_comm.begin());
+    auto c = std::make_unique<Committee>();
+    c->nids.assign(nids, nids + nnet);
+    c->tids.assign(tids, tids + nnet);
+    c->rids.assign(rids, rids + nnet);
+    c->npts.assign(npts, npts + nnet);
+    c->x.assign(x_dev, x_dev + nnet);
+    c->g.assign(grad_dev, grad_dev + nnet);
+    c->loss = loss_dev;
+    c->caller = caller;
+    C = c.get();
+    g_comm.push_back(std::move(c));
+  }
+  if (!C->exec || C->sig != comm_signature(*C)) {
+    if (C->exec) {
+      cudaGraphExecDestroy(C->exec);
+      C->exec = nullptr;
+    }
+    if ((rc = comm_build(*C))) return rc;
+  }
+  if ((rc = ck(cudaEventRecord(C->ready, caller), "event"))) return rc;
+  if ((rc = ck(cudaStreamWaitEvent(C->origin, C->ready, 0), "wait"))) return rc;
+  if ((rc = ck(cudaGraphLaunch(C->exec, C->origin), "graph launch"))) return rc;
+  if ((rc = ck(cudaStreamSynchronize(C->origin), "committee step"))) return rc;
+  for (int i = 0; i < nnet; ++i)
+    if (g_net[nids[i]].prec == PREC_SPLIT && (rc = gemm_tc_flag(&g_net[nids[i]].dn, caller)))
+      return rc;
+  g_comm_policy = C->policy;
+  g_comm_ms = C->ms;
+  return RC_OK;
+}
+
+int dnnf90_committee_info(int *policy, float *graph_ms) {
+  if (policy) *policy = g_comm_policy;
+  if (graph_ms) *graph_ms = g_comm_ms;
+  return g_comm_policy >= 0 ? RC_OK : RC_BAD_ARG;
 }
 
 int dnnf90_ngd_step_noalloc(int nrow, int nw, const double *rows_dev, const double *b_dev,

@@ -662,7 +662,7 @@ static int persistent_grid(const void *k, int threads, size_t smem, long items) 
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  const long g = (long)sm_count_b() * per_sm;
+  const long g = (long)grid_sms() * per_sm;
   return (int)std::max(1L, std::min(g, items));
 }
 
@@ -782,7 +782,7 @@ static int fwd2_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
   a.S = S; a.T = T; a.h = h;
   const int gy = (n + NPB - 1) / NPB;
   const int per_sm = std::max(1, (int)((228 * 1024) / (smem + 1024)));
-  const int gx = std::max(1, std::min(npts, sm_count_b() * per_sm / gy));
+  const int gx = std::max(1, std::min(npts, grid_sms() * per_sm / gy));
   dim3 grid(gx, gy);
   if (train) {
     auto k = k_bell_fwd2<R, KK, NPB, true>;
@@ -860,7 +860,7 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
   a.Tb = Tb; a.h = h; a.Sb = Sb; a.gbias = gbias;
   const int gy = (n + NPB - 1) / NPB;
   const int per_sm = std::max(1, (int)((228 * 1024) / (smem + 1024)));
-  const int gx = std::max(1, std::min(npts, sm_count_b() * per_sm / gy));
+  const int gx = std::max(1, std::min(npts, grid_sms() * per_sm / gy));
   dim3 grid(gx, gy);
   auto k = k_bell_adj2<R, NPB>;
   CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

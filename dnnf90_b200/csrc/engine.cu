@@ -1195,7 +1195,7 @@ static int launch_bell_fwd(const DevTables &t, int n, int npts, const void *S,
   if (smem > 200 * 1024) {
     if (!p.scratch) { set_error("Bell state spill missing"); return RC_DEVICE; }
     a.scratch = p.scratch;
-    gx = std::min(npts, sm_count() * 4);
+    gx = std::min(npts, grid_sms() * 4);
     smem = 0;
   }
   dim3 grid(gx, gy);
@@ -1290,7 +1290,7 @@ static int launch_gemm_cc(int mode, int M, int N, int K, int na, const void *A,
     LAUNCH("k_gemm", st, k_gemm<R, G_DT><<<grid, 256, 0, st>>>(g));
   } else {
     int tiles = ((N + 63) / 64) * ((M + 63) / 64);
-    int splits = std::max(1, std::min((K + 255) / 256, sm_count() * 8 / std::max(1, tiles)));
+    int splits = std::max(1, std::min((K + 255) / 256, grid_sms() * 8 / std::max(1, tiles)));
     g.kchunk = ((K + splits - 1) / splits + 15) / 16 * 16;
     // FP32 partial sums stay short: the reduction across blocks is FP64
     if (sizeof(R) == 4) g.kchunk = std::min(g.kchunk, 4096);
@@ -1303,13 +1303,17 @@ static int launch_gemm_cc(int mode, int M, int N, int K, int na, const void *A,
 }
 
 
-// blocks of k resident on the whole device at this block shape
+static thread_local int g_grid_cap = 0;
+int grid_sms() { return g_grid_cap > 0 ? std::min(g_grid_cap, sm_count()) : sm_count(); }
+void set_grid_cap(int sms) { g_grid_cap = sms; }
+
+// blocks of k resident at once on the SMs a launch may fill
 static int occ_grid(const void *k, int threads, size_t smem) {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  return sm_count() * per_sm;
+  return grid_sms() * per_sm;
 }
 
 template <typename R, int KK>
@@ -1440,7 +1444,7 @@ static int fwd_chunk(Chunk<R> &c, const DevRule *rule, const double *X,
   const DevTables &t = c.t;
   const DevNet &net = c.net;
   Planes &p = c.p;
-  const int L = net.nlayer, na = t.na, np = c.np, smc = sm_count();
+  const int L = net.nlayer, na = t.na, np = c.np, smc = grid_sms();
   int rc;
   {
     L2Args l2;
@@ -1499,7 +1503,7 @@ static int adj_chunk(Chunk<R> &c, const double *X, const double *seed,
   const DevTables &t = c.t;
   const DevNet &net = c.net;
   Planes &p = c.p;
-  const int L = net.nlayer, na = t.na, np = c.np, smc = sm_count();
+  const int L = net.nlayer, na = t.na, np = c.np, smc = grid_sms();
   const bool split = c.split();
   int rc;
   {

@@ -182,6 +182,13 @@ int ngd_device_noalloc(const double *rows, int nrow, int nw, const double *b, in
                        double mu, double *u, cudaStream_t st);
 int ngd_noalloc_maxw();
 
+// SMs a persistent launch may fill: the device's count, or a cap that the
+// committee step sets on its host thread while it issues one member's
+// launches, so that concurrent members share the device instead of each
+// sizing its grid for all of it.
+int grid_sms();
+void set_grid_cap(int sms);
+
 // count of kernel launches issued by this library (process-wide)
 void note_launch();
 long long launch_count();

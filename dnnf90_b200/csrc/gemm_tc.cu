@@ -632,39 +632,47 @@ static bool tc_shape_ok(int N, int K) {
   return smem <= 227 * 1024;
 }
 
+// Pre-split weights of a network.  The buffers are allocated on the first
+// call and rewritten in place afterwards (a network's shapes never change),
+// so kernels captured in a graph keep valid weight addresses across weight
+// updates.  The copies are ordered on st and complete before the return.
 int gemm_tc_prepare(DevNet *net, const double *hw, cudaStream_t st) {
   if (!gemm_tc_available()) return RC_OK;
-  gemm_tc_release_weights(net);
-  TcWeights *w = new TcWeights();
-  net->tc = w;
+  TcWeights *w = (TcWeights *)net->tc;
   const int L = net->nlayer;
-  w->fwd.assign(L, nullptr);
-  w->dt.assign(L, nullptr);
-  w->bias.assign(L, nullptr);
-  w->bn_fwd.assign(L, 0);
-  w->bn_dt.assign(L, 0);
-  CKT(cudaMalloc(&w->flag, sizeof(int)));
-  CKT(cudaMemsetAsync(w->flag, 0, sizeof(int), st));
+  if (!w) {
+    w = new TcWeights();
+    net->tc = w;
+    w->fwd.assign(L, nullptr);
+    w->dt.assign(L, nullptr);
+    w->bias.assign(L, nullptr);
+    w->bn_fwd.assign(L, 0);
+    w->bn_dt.assign(L, 0);
+    CKT(cudaMalloc(&w->flag, sizeof(int)));
+    CKT(cudaMemsetAsync(w->flag, 0, sizeof(int), st));
+  }
   for (int l = 3; l < L; ++l) {  // hidden layers with a GEMM
     const int n = net->dims[l - 1], m = net->dims[l - 2];
     const double *Wl = hw + net->woff[l - 1];
     if (tc_shape_ok(n, m)) {
       const int BN = std::min(n, 128);
       auto b = tc::prep_b(n, m, BN, [&](int j, int k) { return (float)Wl[(size_t)j * (m + 1) + 1 + k]; });
-      CKT(cudaMalloc(&w->fwd[l - 1], b.size()));
-      CKT(cudaMemcpy(w->fwd[l - 1], b.data(), b.size(), cudaMemcpyHostToDevice));
+      if (!w->fwd[l - 1]) CKT(cudaMalloc(&w->fwd[l - 1], b.size()));
+      CKT(cudaMemcpyAsync(w->fwd[l - 1], b.data(), b.size(), cudaMemcpyHostToDevice, st));
       std::vector<float> bias(n);
       for (int j = 0; j < n; ++j) bias[j] = (float)Wl[(size_t)j * (m + 1)];
-      CKT(cudaMalloc(&w->bias[l - 1], n * sizeof(float)));
-      CKT(cudaMemcpy(w->bias[l - 1], bias.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+      if (!w->bias[l - 1]) CKT(cudaMalloc(&w->bias[l - 1], n * sizeof(float)));
+      CKT(cudaMemcpyAsync(w->bias[l - 1], bias.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
       w->bn_fwd[l - 1] = BN;
+      CKT(cudaStreamSynchronize(st));  // b and bias leave scope
     }
     if (tc_shape_ok(m, n)) {
       const int BN = std::min(m, 128);
       auto b = tc::prep_b(m, n, BN, [&](int i, int j) { return (float)Wl[(size_t)j * (m + 1) + 1 + i]; });
-      CKT(cudaMalloc(&w->dt[l - 1], b.size()));
-      CKT(cudaMemcpy(w->dt[l - 1], b.data(), b.size(), cudaMemcpyHostToDevice));
+      if (!w->dt[l - 1]) CKT(cudaMalloc(&w->dt[l - 1], b.size()));
+      CKT(cudaMemcpyAsync(w->dt[l - 1], b.data(), b.size(), cudaMemcpyHostToDevice, st));
       w->bn_dt[l - 1] = BN;
+      CKT(cudaStreamSynchronize(st));
     }
   }
   return RC_OK;
@@ -715,7 +723,7 @@ static int fwd_like(int mode, const uint8_t *W, const float *bias, int BN, int M
   a.A = (const float *)A; a.lda = K; a.W = W; a.bias = bias;
   a.C = (float *)C; a.ldc = N; a.BN = BN; a.ntn = ntn; a.flag = flag;
   const int tiles_m = (M + tc::BM - 1) / tc::BM;
-  dim3 grid(std::max(1, std::min(tiles_m, sm_count_t() / ntn)), ntn);
+  dim3 grid(std::max(1, std::min(tiles_m, grid_sms() / ntn)), ntn);
   return launch(a, mode, grid, smem, st);
 }
 
@@ -742,7 +750,7 @@ int gemm_tc_dw(const DevNet *net, int l, int M, int n, int m, const void *Sb, co
   const int BN = 64;
   const int ntn = (m + BN - 1) / BN;
   const int nkb_all = (M + tc::BK - 1) / tc::BK;
-  const int ctas_k = std::max(1, std::min(nkb_all, sm_count_t() / ntn));
+  const int ctas_k = std::max(1, std::min(nkb_all, grid_sms() / ntn));
   tc::Args a;
   std::memset(&a, 0, sizeof a);
   a.mode = tc::MODE_DW; a.M = n; a.N = m; a.K = M; a.na = 1;

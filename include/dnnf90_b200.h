@@ -96,6 +96,26 @@ int dnnf90_jrow_dev(int nid, int tid, int npts, const double *x_dev, int rid,
 /* points per device chunk of a training work space (0 = automatic) */
 int dnnf90_twork_set_chunk(int tid, int npts);
 
+/* One training step of nnet independent networks (a committee) of any
+ * widths, depths, table sets, point counts and precisions: for member i,
+ * grad_dev[i] = dL_i/dw_i and loss_dev[i] = L_i (both overwritten) from
+ * rule rids[i] over npts[i] points x_dev[i][npts][d0], on work space
+ * tids[i] (distinct per member).  The members run as concurrent branches of
+ * one CUDA graph, each member's kernels sized to a share of the SMs.  The
+ * first call with a given set of members and buffers builds the graph: it
+ * sizes every member's work chunk under one memory budget, runs one untimed
+ * step, captures one graph per SM-sharing policy (by work, by its square
+ * root, none) and keeps the fastest replay; later calls replay it (weights
+ * changed in between are re-uploaded in place first).  Returns after the
+ * step has finished on stream.  Members replace the reference's per-network
+ * loop over net_grad_point (lib/train_module.f90:478-489); new. */
+int dnnf90_committee_step(int nnet, const int *nids, const int *tids, const int *rids,
+                          const int *npts, const double *const *x_dev,
+                          double *const *grad_dev, double *loss_dev, void *stream);
+/* policy (0 work, 1 square root, 2 none) and timed replay ms of the graph
+ * the last committee step used; new */
+int dnnf90_committee_info(int *policy, float *graph_ms);
+
 /* dnnf90_ngd_step (plain FP64 route) on device buffers rows_dev[nrow][nw],
  * b_dev[nw], u_dev[nw], for callers that cannot allocate device memory
  * while they run: a host whose device memory is all handed out up front by
