@@ -25,9 +25,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -71,52 +69,72 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """SM clock and throttle reasons sampled every 200 ms during the timed
+    region, by NVML from a thread of this process (read-only queries; the
+    same fields nvidia-smi's clocks line reports)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # nvmlClocksEventReason bits
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40,
+               "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
     def __init__(self, dev):
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.p = None
         self.dev = dev
+        self.rows = []
+        self.skip = 0
+        self.stop = None
+        self.th = None
 
     def __enter__(self):
+        import threading
+
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
-                                      stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml
+
+            pynvml.nvmlInit()
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            idx = int(vis.split(",")[self.dev]) if vis and vis.split(",")[0].isdigit() else self.dev
+            h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self.mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
         except Exception:
-            self.p = None
+            return self
+        self.stop = threading.Event()
+
+        def run():
+            while not self.stop.is_set():
+                try:
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.rows.append((sm, rs))
+                except Exception:
+                    pass
+                self.stop.wait(0.2)
+
+        self.th = threading.Thread(target=run, daemon=True)
+        self.th.start()
         return self
 
+    def wait_first(self, limit=5.0):
+        t0 = time.perf_counter()
+        while self.th and not self.rows and time.perf_counter() - t0 < limit:
+            time.sleep(0.02)
+
+    def mark(self):
+        """Samples before this call (warm-up) are left out of the summary."""
+        self.skip = len(self.rows)
+
     def __exit__(self, *a):
-        if self.p:
-            self.p.terminate()
-            try:
-                self.p.wait(5)
-            except Exception:
-                self.p.kill()
+        if self.stop:
+            self.stop.set()
+            self.th.join(2)
 
     def summary(self):
-        try:
-            rows = [l.split(",") for l in open(self.f.name).read().splitlines() if l.strip()]
-            os.unlink(self.f.name)
-        except Exception:
-            return None
+        rows = self.rows[self.skip:] or self.rows[-1:]
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows]
-        mx = max(float(r[2]) for r in rows)
-        reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            for n, v in zip(names, r[5:9]):
-                if v.strip().lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(rows)}
+        reasons = sorted({n for _, r in rows for n, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(float(sm) for sm, _ in rows),
+                "sm_max_mhz": float(self.mx), "reasons": reasons, "samples": len(rows),
+                "source": "NVML, 200 ms"}
 
 
 def dist_init():
@@ -218,6 +236,60 @@ def accuracy(api, ts, w, rule_terms, nsample=6):
     return out
 
 
+# ------------------------------------------------------------------ committee
+def committee_bench(api, dev, nsteps, nnet=64):
+    """Uneven committee: nnet independent networks, widths from
+    {32, 64, 128, 256}, 2-4 hidden tanh layers, D0 from 2-4 and K from 2-7
+    (dense sets), 1k-64k points log-uniform in [-1,1]^D0, split precision,
+    L = sum T^2/2 per network; one step = forward + seed + adjoint of every
+    member, replayed as one CUDA graph.  Returns the summary object."""
+    import torch
+
+    rng = np.random.default_rng(20260804)
+    tabs, nets, xs, grads = {}, [], [], []
+    rule = api.SeedRule(api.SEED_HALFSQ)
+    total = 0
+    shapes = []
+    for i in range(nnet):
+        width = int(rng.choice([32, 64, 128, 256]))
+        depth = int(rng.integers(2, 5))
+        d0 = int(rng.integers(2, 5))
+        k = int(rng.integers(2, 8))
+        npts = int(np.exp(rng.uniform(np.log(1000.0), np.log(64000.0))))
+        if (d0, k) not in tabs:
+            tabs[(d0, k)] = api.TableSet(d0, k)
+        dims = [d0] + [width] * depth + [1]
+        nets.append(api.Net(tabs[(d0, k)], dims, weights=xavier(dims, 1000 + i),
+                            precision=api.PREC_SPLIT))
+        xs.append(torch.tensor(rng.uniform(-1.0, 1.0, (npts, d0)), device=dev))
+        grads.append(torch.zeros(nets[-1].nw, dtype=torch.float64, device=dev))
+        total += npts
+        shapes.append([d0, k, width, depth, npts])
+    loss = torch.zeros(nnet, dtype=torch.float64, device=dev)
+    rules = [rule] * nnet
+    t0 = time.perf_counter()
+    policy, graph_ms = api.committee_step(nets, rules, xs, grads, loss)
+    build_s = time.perf_counter() - t0
+    api.committee_step(nets, rules, xs, grads, loss)
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(st)
+    for _ in range(nsteps):
+        api.committee_step(nets, rules, xs, grads, loss)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / nsteps
+    finite = bool(torch.isfinite(loss).all().item())
+    for m in nets:
+        m.free()
+    rule.free()
+    return {"nets": nnet, "points": total, "ms_per_step": ms, "pts_per_s": total / (ms / 1e3),
+            "steps": nsteps, "graph_policy": ["by work", "by sqrt(work)", "uncapped"][policy],
+            "graph_replay_ms": graph_ms, "first_call_s": build_s, "losses_finite": finite,
+            "precision": "split", "shapes_d0_k_width_depth_points": shapes}
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -229,6 +301,8 @@ def main():
     ap.add_argument("--f64-steps", type=int, default=2)
     ap.add_argument("--ref-points", type=int, default=24)
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--committee-steps", type=int, default=3,
+                    help="timed steps of the 64-network committee (0 skips it)")
     ap.add_argument("--prof-steps", type=int, default=1,
                     help="steps of the per-kernel event-profiled pass (untimed)")
     args = ap.parse_args()
@@ -243,6 +317,7 @@ def main():
 
     ws, rank, local = dist_init()
     dev = torch.device("cuda", local)
+    hbm_free0 = torch.cuda.mem_get_info(dev)[0] / 2**30
     npts = args.points
     ts = api.TableSet(D0, K)
     w = xavier(DIMS, 20260801)
@@ -267,9 +342,16 @@ def main():
         red.step(local)
 
     def timed(net, g, loss, nsteps, clocks=False, profile=False, warmup=None):
+        # the clock sampler starts before the warm-up and has produced a
+        # sample before the timed region, so its start-up stays outside it
+        ck = Clocks(local)
+        if clocks:
+            ck.__enter__()
         for _ in range(args.warmup if warmup is None else warmup):
             step(net, g, loss)
         torch.cuda.synchronize(dev)
+        if clocks:
+            ck.wait_first()
         if ws > 1:
             dist.barrier()
         n0 = api.launch_count()
@@ -277,9 +359,8 @@ def main():
             api.profile_read()
             api.profile_enable(True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ck = Clocks(local)
         if clocks:
-            ck.__enter__()
+            ck.mark()
         e0.record(stream)
         for _ in range(nsteps):
             step(net, g, loss)
@@ -408,6 +489,7 @@ def main():
     acc = None
     if rank == 0 and not args.no_accuracy:
         acc = accuracy(api, ts, w, terms)
+    committee = committee_bench(api, dev, args.committee_steps) if args.committee_steps > 0 else None
     cpu = cpu_baseline(args.ref_points, 1) if (rank == 0 and ws == 1) else None
 
     if rank == 0:
@@ -419,12 +501,15 @@ def main():
             "data": "synthetic (seeded uniform points, Xavier-normal weights)",
             "config": {"workload": WORKLOAD, "points_per_gpu": npts, "global_points": ws * npts,
                        "parallelism": f"dp{ws}: points sharded, dL/dw all-reduced (NCCL)",
-                       "l2": "inputs larger than L2 (126 MB): a work chunk's planes are ~48 GB, so no flush"},
+                       "l2": "inputs larger than L2 (126 MB): a work chunk's planes are ~48 GB, so no flush",
+                       "hbm_free_gib_at_start": round(hbm_free0, 1),
+                       "launches_per_step": launches / max(args.steps, 1)},
             "f64": {"value": value64, "unit": "pts/s", "ms_per_step": ms64,
                     "steps": args.f64_steps, "split_speedup": value / value64,
                     "kernel_ms_per_step": per_step_ms(prof64)},
             "kernel_ms_per_step": per_step_ms(prof),
             "accuracy": acc,
+            "committee": committee,
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": roof,
