@@ -17,6 +17,7 @@
 
 struct orc_tables {
   int d0, k, na;
+  int iact;  /* activation: 0 tanh, 1 sin, 2 erf (the tabset's iact) */
   int *alpha;   /* [na][d0] */
   int *deg;     /* [na] */
   int *ind_e1;  /* [d0], 1-based slot or 0 */
@@ -351,6 +352,43 @@ void orc_tanh_derivs(const orc_tables *t, double a, int nq, double *d) {
   }
 }
 
+/* sin_derivs (lib/multi_index_bell_module.f90:745-755): every derivative is
+ * a phase shift, sigma^(q)(a) = sin(a + q pi/2) */
+static void sin_derivs(double a, int nq, double *d) {
+  const double pio2 = 1.57079632679489661923;
+  for (int q = 0; q <= nq; ++q) d[q] = sin(a + (double)q * pio2);
+}
+
+/* erf_derivs (:831-850): sigma' = (2/sqrt(pi)) exp(-a^2) and the higher
+ * derivatives through the Hermite-function recurrence
+ * psi_{n+1} = 2 a psi_n - 2 n psi_{n-1}, psi_0 = exp(-a^2).  The value
+ * itself is libm's erf (the reference carries its own series / continued
+ * fraction; both are correctly rounded to a few ulps). */
+static void erf_derivs(double a, int nq, double *d) {
+  const double c2spi = 1.12837916709551257390;
+  d[0] = erf(a);
+  if (nq < 1) return;
+  double psi[64];
+  psi[0] = exp(-a * a);
+  psi[1] = 2.0 * a * psi[0];
+  for (int n = 1; n <= nq - 2 && n + 1 < 64; ++n)
+    psi[n + 1] = 2.0 * a * psi[n] - 2.0 * (double)n * psi[n - 1];
+  for (int q = 1; q <= nq; ++q) d[q] = c2spi * ((q - 1) % 2 ? -1.0 : 1.0) * psi[q - 1];
+}
+
+/* act_derivs_ts (:723-741): the activation contract, sigma^(q), q = 0..nq */
+void orc_act_derivs(const orc_tables *t, double a, int nq, double *d) {
+  if (t->iact == 1) sin_derivs(a, nq, d);
+  else if (t->iact == 2) erf_derivs(a, nq, d);
+  else orc_tanh_derivs(t, a, nq, d);
+}
+
+int orc_tables_set_activation(orc_tables *t, int iact) {
+  if (iact < 0 || iact > 2) return -1;
+  t->iact = iact;
+  return 0;
+}
+
 int orc_weight_count(int nlayer, const int *dims) {
   int n = 0;
   for (int l = 1; l < nlayer; ++l) n += dims[l] * (dims[l - 1] + 1);
@@ -440,7 +478,7 @@ static void forward_core(const orc_tables *t, work *wk, const int *dims,
     }
     if (l < nlayer) {
       for (int j = 0; j < nd; ++j) {
-        orc_tanh_derivs(t, PL(wk->S, wk, j, 0), t->k + 1, dsc);
+        orc_act_derivs(t, PL(wk->S, wk, j, 0), t->k + 1, dsc);
         for (int q = 0; q <= t->k + 1; ++q) DT(wk, j, q) = dsc[q];
       }
       for (int j = 0; j < nd; ++j) {

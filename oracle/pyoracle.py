@@ -50,6 +50,8 @@ def lib():
         L.orc_tables_sizes.argtypes = [vp, P(ci), P(ci), P(ci), P(ci)]
         L.orc_tables_copy.argtypes = [vp] + [vp] * 14
         L.orc_tanh_derivs.argtypes = [vp, cd, ci, vp]
+        L.orc_act_derivs.argtypes = [vp, cd, ci, vp]
+        L.orc_tables_set_activation.argtypes = [vp, ci]
         L.orc_weight_count.argtypes = [ci, P(ci)]
         L.orc_eval_point.argtypes = [vp, ci, P(ci), vp, vp, vp, vp]
         L.orc_grad_point.argtypes = [vp, ci, P(ci), vp, vp, vp, vp, vp]
@@ -75,7 +77,7 @@ class _SeedRule(ctypes.Structure):
 class Tables:
     """One multi-index table set (init_hod_tables)."""
 
-    def __init__(self, d0: int, k: int, seeds=None):
+    def __init__(self, d0: int, k: int, seeds=None, activation: int = 0):
         L = lib()
         self.d0, self.k = d0, k
         if seeds is None or len(seeds) == 0:
@@ -87,6 +89,9 @@ class Tables:
         if not h:
             raise ValueError("oracle: bad table arguments")
         self._h = h
+        if activation and L.orc_tables_set_activation(h, int(activation)) != 0:
+            raise ValueError("oracle: activation not restated")
+        self.activation = int(activation)
         na, nfq, npair, nbell = (ctypes.c_int(), ctypes.c_int(), ctypes.c_int(),
                                  ctypes.c_int())
         L.orc_tables_sizes(h, ctypes.byref(na), ctypes.byref(nfq),
@@ -126,6 +131,11 @@ class Tables:
             if tuple(int(v) for v in b) == a:
                 return i + 1
         return 0
+
+    def act_derivs(self, a: float, nq: int) -> np.ndarray:
+        d = np.zeros(nq + 1)
+        lib().orc_act_derivs(self._h, float(a), nq, _p(d))
+        return d
 
     def tanh_derivs(self, a: float, nq: int) -> np.ndarray:
         d = np.zeros(nq + 1)

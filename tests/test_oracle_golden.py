@@ -111,3 +111,23 @@ def test_adam_matches_the_formula():
     gv = g / 2
     exp = np.array([0.5, -0.2]) - 0.01 * gv / (np.abs(gv) + 1e-8)
     assert np.max(np.abs(w - exp)) < 1e-12
+
+
+def test_oracle_sin_and_erf_derivatives():
+    """sigma^(q) of the sin and erf activations against their closed forms
+    (act_derivs_ts, lib/multi_index_bell_module.f90:723-850)."""
+    import math
+    ts = po.Tables(2, 5, activation=1)
+    for a in (-1.3, 0.0, 0.7, 2.9):
+        d = ts.act_derivs(a, 6)
+        ref = [math.sin(a), math.cos(a), -math.sin(a), -math.cos(a)] * 2
+        assert np.allclose(d, ref[:7], rtol=0, atol=1e-15)
+    te = po.Tables(2, 5, activation=2)
+    for a in (-2.5, -0.4, 0.0, 1.1, 3.0):
+        d = te.act_derivs(a, 5)
+        g = 2.0 / math.sqrt(math.pi) * math.exp(-a * a)
+        # erf' = g, erf'' = -2a g, erf''' = (4a^2 - 2) g, erf'''' = (12a - 8a^3) g,
+        # erf''''' = (16a^4 - 48a^2 + 12) g
+        ref = [math.erf(a), g, -2 * a * g, (4 * a * a - 2) * g, (12 * a - 8 * a ** 3) * g,
+               (16 * a ** 4 - 48 * a * a + 12) * g]
+        assert np.allclose(d, ref, rtol=1e-13, atol=1e-15), (a, d, ref)
