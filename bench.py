@@ -510,6 +510,7 @@ def main():
             "kernel_ms_per_step": per_step_ms(prof),
             "accuracy": acc,
             "committee": committee,
+            "autotuner": [list(t) for t in api.tune_report()],
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": roof,

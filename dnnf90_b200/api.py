@@ -44,6 +44,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_twork_set_chunk", "dnnf90_last_error", "dnnf90_device_available",
     "dnnf90_launch_count", "dnnf90_profile_enable", "dnnf90_profile_read",
     "dnnf90_ngd_step_noalloc", "dnnf90_committee_step", "dnnf90_committee_info",
+    "dnnf90_tune_report",
 ]
 
 _lib = None
@@ -123,6 +124,7 @@ def lib():
         "dnnf90_ngd_step_noalloc": [i, i, p, p, i, d, p, p],
         "dnnf90_committee_step": [i, pi, pi, pi, pi, p, p, p, p],
         "dnnf90_committee_info": [pi, P(ctypes.c_float)],
+        "dnnf90_tune_report": [ctypes.c_char_p, i],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -166,6 +168,19 @@ def launch_count() -> int:
 
 def profile_enable(on: bool = True):
     lib().dnnf90_profile_enable(1 if on else 0)
+
+
+def tune_report() -> list:
+    """The Bell kernels' autotuner choices: (kernel, width, precision,
+    chosen variant, [trial ms per variant])."""
+    n = lib().dnnf90_tune_report(None, 0)
+    buf = ctypes.create_string_buffer(n + 64)
+    lib().dnnf90_tune_report(buf, len(buf))
+    out = []
+    for line in buf.value.decode().splitlines():
+        f = line.split()
+        out.append((f[0], int(f[1]), f[2], int(f[3]), [float(v) for v in f[4:]]))
+    return out
 
 
 def profile_read() -> dict:

@@ -1453,6 +1453,16 @@ int dnnf90_committee_step(int nnet, const int *nids, const int *tids, const int 
   return RC_OK;
 }
 
+int dnnf90_tune_report(char *buf, int len) {
+  static std::string pending;
+  pending = tune_report();
+  if (buf && len > 0) {
+    std::strncpy(buf, pending.c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
+  }
+  return (int)pending.size();
+}
+
 int dnnf90_committee_info(int *policy, float *graph_ms) {
   if (policy) *policy = g_comm_policy;
   if (graph_ms) *graph_ms = g_comm_ms;

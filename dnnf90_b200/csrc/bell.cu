@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdio>
 #include <map>
 #include <mutex>
 #include <string>
@@ -685,7 +686,29 @@ struct TuneKey {
   }
 };
 static std::map<TuneKey, int> g_tune;
+static std::map<TuneKey, std::vector<float>> g_tune_ms;  // timed trial per variant
 static std::mutex g_tune_mu;
+
+// "kernel width prec chosen ms0 ms1 ..." lines, one per tuned launch shape
+std::string tune_report() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  static const char *names[] = {"bell_fwd", "bell_fwd_train", "bell_adj"};
+  std::string out;
+  char b[64];
+  for (auto &kv : g_tune) {
+    std::snprintf(b, sizeof b, "%s %d %s %d", names[kv.first.which], kv.first.n,
+                  kv.first.prec == 8 ? "f64" : "f32", kv.second);
+    out += b;
+    auto it = g_tune_ms.find(kv.first);
+    if (it != g_tune_ms.end())
+      for (float ms : it->second) {
+        std::snprintf(b, sizeof b, " %.4f", ms);
+        out += b;
+      }
+    out += "\n";
+  }
+  return out;
+}
 
 template <typename L>
 static int tuned_launch(const TuneKey &key, int nvar, int dflt, long items, cudaStream_t st,
@@ -708,6 +731,7 @@ static int tuned_launch(const TuneKey &key, int nvar, int dflt, long items, cuda
   }
   float best = 0.f;
   int bv = dflt, rc = RC_OK;
+  std::vector<float> times(nvar, -1.f);
   // one untimed run of each first, so that module loading and first-touch
   // costs do not favour the variant that runs later
   for (int v = 0; v < nvar && rc == RC_OK; ++v) rc = launch(v, false);
@@ -718,6 +742,7 @@ static int tuned_launch(const TuneKey &key, int nvar, int dflt, long items, cuda
     if (rc == RC_OK && cudaEventSynchronize(e1) == cudaSuccess) {
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
+      times[v] = ms;
       if (v == 0 || ms < best) {
         best = ms;
         bv = v;
@@ -729,6 +754,7 @@ static int tuned_launch(const TuneKey &key, int nvar, int dflt, long items, cuda
   if (rc) return rc;
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[key] = bv;
+  g_tune_ms[key] = times;
   return RC_OK;  // every variant wrote the same values
 }
 
@@ -839,19 +865,20 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
     const bool srec_fits = smem5 + extra <= 227 * 1024;
     // variant 0: pairs in global memory; 1: pairs in shared memory
     auto launch = [&](int v, bool last) -> int {
+      Adj5Args bv = b;
+      if (!last) bv.gbias = nullptr;  // a timing run adds nothing
       const bool srec = v == 1;
       const size_t sm = smem5 + (srec ? extra : 0);
       auto k = srec ? k_bell_adj5<R, NPB, true> : k_bell_adj5<R, NPB, false>;
       CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       const int grid = persistent_grid((const void *)k, ADJ_WORKERS * 32, sm, (long)npts * b.gy);
-      Adj5Args bv = b;
-      if (!last) bv.gbias = nullptr;  // a timing run adds nothing
       LAUNCH("k_bell_adj", st, k<<<grid, ADJ_WORKERS * 32, sm, st>>>(bv));
       CKB(cudaGetLastError());
       return RC_OK;
     };
-    return tuned_launch(TuneKey{bp.id, 2, n, (int)sizeof(R)}, srec_fits ? 2 : 1,
-                        srec_fits ? 1 : 0, (long)npts * b.gy, st, launch);
+    const int nvar = srec_fits ? 2 : 1;
+    return tuned_launch(TuneKey{bp.id, 2, n, (int)sizeof(R)}, nvar, nvar - 1,
+                        (long)npts * b.gy, st, launch);
   }
   Adj2Args a;
   a.n = n; a.na = t.na; a.npts = npts; a.gstride = gstride; a.list = bp.aj_list;

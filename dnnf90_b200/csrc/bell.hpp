@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "bell_plan.hpp"
 
 namespace dnnf90 {
@@ -45,6 +47,9 @@ struct DevBellPlan {
 };
 
 int upload_bell_plan(const TableSet &t, DevBellPlan &d);
+
+// the autotuner's choices: "kernel width precision variant ms..." lines
+std::string tune_report();
 
 // RC_UNSUPPORTED when the set does not fit (K > 8 or the per-point state
 // exceeds shared memory): the caller then uses the generic kernels.

@@ -112,6 +112,10 @@ int dnnf90_twork_set_chunk(int tid, int npts);
 int dnnf90_committee_step(int nnet, const int *nids, const int *tids, const int *rids,
                           const int *npts, const double *const *x_dev,
                           double *const *grad_dev, double *loss_dev, void *stream);
+/* the Bell kernels' autotuner: one line per tuned launch shape, "kernel
+ * width precision chosen-variant ms-of-each-variant"; returns the length
+ * (buf may be NULL); new */
+int dnnf90_tune_report(char *buf, int len);
 /* policy (0 work, 1 square root, 2 none) and timed replay ms of the graph
  * the last committee step used; new */
 int dnnf90_committee_info(int *policy, float *graph_ms);
