@@ -113,6 +113,7 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
   }
   d.f5_ok = P.f5_ok;
   d.nrows5 = P.nrows5;
+  d.zuv5 = P.zuv5;
   d.dt_off5 = P.dt_off5;
   d.f3_ok = P.f3_ok;
   d.nrows = P.nrows;
@@ -324,6 +325,7 @@ __device__ __forceinline__ void stage_rows(unsigned char *dst, const R *src, int
 
 struct Fwd5Args {
   int n, na, npts, iact, dt_off, nrows, gy;
+  int zuv;             // byte offset of the zero U/V pair
   int nrec32;          // 32-bit records copied to shared memory (SREC)
   const double *tpc;
   const int *list;     // [(K+1) * workers][2]
@@ -411,6 +413,8 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd5(Fwd5Args a) {
   const R *sc = (const R *)a.sc;
   const uint32_t sbuf1 = a.nrows * 128;
   int buf = 0;
+  if (threadIdx.x < 16)  // the zero U/V pair (read by the padding records)
+    *(uint4 *)(sm + a.zuv + threadIdx.x * 16) = make_uint4(0, 0, 0, 0);
   const long nitem = (long)a.npts * a.gy;
   const long it0 = (long)blockIdx.x * nitem / gridDim.x;
   const long it1 = (long)(blockIdx.x + 1) * nitem / gridDim.x;
@@ -473,16 +477,37 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd5(Fwd5Args a) {
         uint2 q0 = src.get(ri), q1 = src.get(ri + 1);
         if (p == KK) {
           R tt = dt[1] * sa, hh = dt[2] * sa;
+          if constexpr (SREC) {
+            // four records per 16-byte load (lists aligned and padded to 4)
+            const uint4 *rq = (const uint4 *)(src.p + A0.y);
+            uint4 q = rq[0];
+            auto top = [&](uint32_t r) {
+              const R x = srow<R>(sm, los + ((r & 0xffffu) << 7));
+              const uint32_t u = lo + ((r >> 16) << 7);
+              tt += x * srow<R>(sm, u);
+              hh += x * srow<R>(sm, u + 128);
+            };
+            const int m = A0.z >> 2;
+            for (int e = 0; e < m; ++e) {
+              const uint4 g4 = q;
+              q = rq[e + 1];
+              top(g4.x);
+              top(g4.y);
+              top(g4.z);
+              top(g4.w);
+            }
+          } else {
 #pragma unroll 2
-          for (int e = 0; e < A0.z; ++e) {
-            const uint2 g = q0;
-            q0 = q1;
-            q1 = src.get(ri + 2);
-            ++ri;
-            const R x = srow<R>(sm, los + g.x);
-            const uint32_t u = lo + g.y;
-            tt += x * srow<R>(sm, u);
-            hh += x * srow<R>(sm, u + 128);
+            for (int e = 0; e < A0.z; ++e) {
+              const uint2 g = q0;
+              q0 = q1;
+              q1 = src.get(ri + 2);
+              ++ri;
+              const R x = srow<R>(sm, los + g.x);
+              const uint32_t u = lo + g.y;
+              tt += x * srow<R>(sm, u);
+              hh += x * srow<R>(sm, u + 128);
+            }
           }
           if (act) {
             T[(size_t)ia * n + j] = fa * tt;
@@ -767,7 +792,7 @@ static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
   if (!bp.f5_ok || smem > 227 * 1024 || n % (16 / (int)sizeof(R))) return RC_UNSUPPORTED;
   Fwd5Args a;
   a.n = n; a.na = t.na; a.npts = npts; a.iact = t.iact; a.dt_off = bp.dt_off5;
-  a.nrows = bp.nrows5; a.gy = (n + NPB - 1) / NPB;
+  a.nrows = bp.nrows5; a.gy = (n + NPB - 1) / NPB; a.zuv = bp.zuv5;
   a.nrec32 = bp.nrec32;
   a.tpc = t.tpc; a.list = bp.f5_list; a.arec = (const int4 *)bp.f5_arec;
   a.rec = (const uint2 *)bp.f5_rec; a.rec32 = bp.f6_rec; a.cpdst = bp.f5_cpdst;

@@ -36,7 +36,7 @@ struct DevBellPlan {
   int nuv = 0;
   // v5
   bool f5_ok = false;
-  int nrows5 = 0, dt_off5 = 0;
+  int nrows5 = 0, dt_off5 = 0, zuv5 = 0;
   int *f5_list = nullptr, *f5_arec = nullptr, *f5_cpdst = nullptr;
   uint32_t *f5_rec = nullptr, *a5_pair = nullptr;
   uint32_t *f6_rec = nullptr;   // forward records as row indices

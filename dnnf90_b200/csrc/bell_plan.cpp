@@ -195,6 +195,8 @@ BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
         uv[ia] = row * ROW;
         row += 2;
       }
+    P.zuv5 = row * ROW;  // a U/V pair of zeros, target of the padding records
+    row += 2;
     P.dt_off5 = row * ROW;
     P.nrows5 = row + k + 2;
     P.f5_cpdst = b1;
@@ -217,6 +219,11 @@ BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
         P.f5_list[((size_t)p * workers + w) * 2 + 1] = (int)asg[w].size();
         for (int it : asg[w]) {
           const int ia = items[it];
+          if (p == k)  // top-degree lists start on a 4-record boundary
+            while ((P.f5_rec.size() / 2) % 4) {
+              P.f5_rec.push_back(0);
+              P.f5_rec.push_back((uint32_t)P.zuv5);
+            }
           const int rstart = (int)P.f5_rec.size() / 2;
           uint64_t bands = 0;
           int cnt[9] = {0};
@@ -238,9 +245,14 @@ BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
               if (p < k) cnt[t.deg[g]]++;
             }
           }
+          if (p == k)  // and hold a multiple of 4: padding adds S_0 x 0
+            while ((P.f5_rec.size() / 2 - rstart) % 4) {
+              P.f5_rec.push_back(0);
+              P.f5_rec.push_back((uint32_t)P.zuv5);
+            }
           for (int d = 1; d <= 8; ++d) {
             if (cnt[d] > 255) bands_ok = false;
-            if (d <= 8) bands += (uint64_t)(cnt[d] & 0xff) << (8 * (d - 1));
+            bands += (uint64_t)(cnt[d] & 0xff) << (8 * (d - 1));
           }
           P.f5_arec.push_back(ia | (p << 16));
           P.f5_arec.push_back(rstart);

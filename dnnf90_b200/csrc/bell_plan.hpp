@@ -56,6 +56,9 @@ struct BellPlan {
   //           for |g| = 1 the level-1 row is S_g itself (S region)
   //   p = K : (S row of b, U row of g)            -- V one row further
   int nrows5 = 0, dt_off5 = 0;
+  int zuv5 = 0;                    // byte offset of the zero U/V pair
+  // top-degree lists (p = K) start on a 4-record boundary and are padded to a
+  // multiple of 4 with (S row 0, zero U/V pair) records
   bool f5_ok = false;
   std::vector<int> f5_list;        // [(k+1) * workers][2]: start, count into f5_arec
   std::vector<int> f5_arec;        // [*][8]: ia | p << 16, rstart, rcount, band_hi,
