@@ -1,17 +1,18 @@
 // gemm_tc.cu - split-BF16 layer GEMMs on the tcgen05 tensor cores.
 //
-// One persistent kernel, warp-specialised (416 threads):
-//   warps 0-7  producers: read FP32 operand rows from HBM (coalesced 16-byte
-//              loads, the next K block prefetched into registers), split every value x into three bf16 terms
+// One persistent kernel, warp-specialised (FWD/DT 672 threads, DW 416):
+//   producers  warps 0-15 (FWD/DT; 0-7 for DW): read FP32 operand rows from
+//              HBM (coalesced 16-byte loads; FWD/DT keep the next two K
+//              blocks in flight in registers), split every value x into three bf16 terms
 //              x1 = bf16(x), x2 = bf16(x - x1), x3 = bf16(x - x1 - x2) and
 //              store them in the 128-byte-swizzled canonical layout the
 //              tensor core reads (one tile per term)
-//   warp 12    MMA issuer: per 16-deep k-step six tcgen05.mma (kind::f16,
+//   MMA warp   (the last) issuer: per 16-deep k-step six tcgen05.mma (kind::f16,
 //              bf16 x bf16 -> FP32) for the cross terms of order <= 2:
 //              a3b1, a2b2, a1b3, a2b1, a1b2, a1b1, smallest first, into an
 //              accumulator in tensor memory (two buffers, so the epilogue of
 //              one tile overlaps the products of the next)
-//   warps 8-11 epilogue: tcgen05.ld of the accumulator (lane = row), bias
+//   epilogue   4 warps after the producers: tcgen05.ld of the accumulator (lane = row), bias
 //              on the alpha = 0 rows, FP32 store; or, for the weight
 //              gradient, FP32 partials of 512 rows added into FP64
 //              registers and reduced to HBM with FP64 atomics
@@ -51,14 +52,20 @@ namespace dnnf90 {
 
 namespace tc {
 
-constexpr int NPROD_WARPS = 8, NPROD = NPROD_WARPS * 32;  // producers
-constexpr int EPI_WARP0 = 8;                              // warps 8-11: epilogue
-constexpr int MMA_WARP = 12;
-constexpr int NTHREADS = 13 * 32;
+constexpr int MODE_FWD = 0, MODE_DT = 1, MODE_DW = 2;
+// Warp roles per mode: producers first, then 4 epilogue warps, then the MMA
+// warp.  FWD/DT run 16 producer warps that keep two K blocks of loads in
+// flight; DW keeps 8 (its epilogue holds 64 FP64 partials per thread).
+template <int MODE>
+struct Roles {
+  static constexpr int PW = MODE == MODE_DW ? 8 : 16;  // producer warps
+  static constexpr int NPROD = PW * 32;
+  static constexpr int MMA = PW + 4;
+  static constexpr int NT = (PW + 5) * 32;
+};
 constexpr int BM = 128;       // rows per tile (MMA M)
 constexpr int BK = 64;        // K per block: one 128-byte bf16 swizzle row
 constexpr int ROWB = 128;     // bytes per swizzled row
-constexpr int MODE_FWD = 0, MODE_DT = 1, MODE_DW = 2;
 constexpr long WAIT_LIMIT = 1L << 26;  // polls before a wait gives up (seconds)
 
 __device__ __forceinline__ uint32_t su32(const void *p) {
@@ -199,7 +206,9 @@ struct Args {
 };
 
 template <int MODE>
-__global__ void __launch_bounds__(NTHREADS, 1) k_tc_gemm(Args g) {
+__global__ void __launch_bounds__(Roles<MODE>::NT, 1) k_tc_gemm(Args g) {
+  constexpr int NPROD_WARPS = Roles<MODE>::PW, NPROD = Roles<MODE>::NPROD;
+  constexpr int MMA_WARP = Roles<MODE>::MMA;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *sm = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -292,21 +301,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_gemm(Args g) {
                                          : make_float4(0.f, 0.f, 0.f, 0.f);
         }
       };
-      float4 cur[PF], nxt[PF];
-      int mt = first_m, kb = 0;
-      if (mt < tiles_m) load(cur, mt, 0);
-      while (mt < tiles_m) {
-        int nmt = mt, nkb2 = kb + 1;
-        if (nkb2 == nkb) { nkb2 = 0; nmt += step_m; }
-        if (nmt < tiles_m) load(nxt, nmt, nkb2);
-        if (!mbar_wait(empty + stage, ph ^ 1u, flag, 1)) goto done;
+      // split one block into the next free stage
+      auto consume = [&](const float4 (&v)[PF]) -> bool {
+        if (!mbar_wait(empty + stage, ph ^ 1u, flag, 1)) return false;
         uint8_t *st = sStage + stage * stage_bytes;
 #pragma unroll
         for (int it = 0; it < PF; ++it) {
           const int e = it * NPROD + t;
           const int row = e >> 4, c4 = e & 15;
           uint2 p1, p2, p3;
-          split4(cur[it], p1, p2, p3);
+          split4(v[it], p1, p2, p3);
           const uint32_t off = kmaj_off(row, c4 * 4);
           *(uint2 *)(st + off) = p1;
           *(uint2 *)(st + a_tile + off) = p2;
@@ -315,10 +319,34 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_gemm(Args g) {
         fence_proxy_async();
         mbar_arrive(full + stage);
         next_stage();
-#pragma unroll
-        for (int it = 0; it < PF; ++it) cur[it] = nxt[it];
-        mt = nmt;
-        kb = nkb2;
+        return true;
+      };
+      // blocks (M tile, K block) in order; b0/b1/b2 rotate roles so that the
+      // loads of the two blocks after the one being split are in flight
+      int pm0 = first_m, pk0 = 0, pm1 = pm0, pk1 = 1, pm2, pk2;
+      if (pk1 == nkb) { pk1 = 0; pm1 += step_m; }
+      pm2 = pm1; pk2 = pk1 + 1;
+      if (pk2 == nkb) { pk2 = 0; pm2 += step_m; }
+      auto rotate = [&]() {
+        pm0 = pm1; pk0 = pk1; pm1 = pm2; pk1 = pk2;
+        if (++pk2 == nkb) { pk2 = 0; pm2 += step_m; }
+      };
+      float4 b0[PF], b1[PF], b2[PF];
+      if (pm0 < tiles_m) load(b0, pm0, pk0);
+      if (pm1 < tiles_m) load(b1, pm1, pk1);
+      for (;;) {
+        if (pm0 >= tiles_m) break;
+        if (pm2 < tiles_m) load(b2, pm2, pk2);
+        if (!consume(b0)) goto done;
+        rotate();
+        if (pm0 >= tiles_m) break;
+        if (pm2 < tiles_m) load(b0, pm2, pk2);
+        if (!consume(b1)) goto done;
+        rotate();
+        if (pm0 >= tiles_m) break;
+        if (pm2 < tiles_m) load(b1, pm2, pk2);
+        if (!consume(b2)) goto done;
+        rotate();
       }
     } else {
       // A: 64 rows x 128 j of Sb (32 threads per row); B: 64 rows x 64 i
@@ -699,13 +727,13 @@ static int check_flag(int *flag, cudaStream_t st, const char *what) {
 static int launch(const tc::Args &a, int mode, dim3 grid, size_t smem, cudaStream_t st) {
   if (mode == tc::MODE_FWD) {
     CKT(cudaFuncSetAttribute(tc::k_tc_gemm<tc::MODE_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LAUNCH("k_tc_gemm_fwd", st, tc::k_tc_gemm<tc::MODE_FWD><<<grid, tc::NTHREADS, smem, st>>>(a));
+    LAUNCH("k_tc_gemm_fwd", st, tc::k_tc_gemm<tc::MODE_FWD><<<grid, tc::Roles<tc::MODE_FWD>::NT, smem, st>>>(a));
   } else if (mode == tc::MODE_DT) {
     CKT(cudaFuncSetAttribute(tc::k_tc_gemm<tc::MODE_DT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LAUNCH("k_tc_gemm_dt", st, tc::k_tc_gemm<tc::MODE_DT><<<grid, tc::NTHREADS, smem, st>>>(a));
+    LAUNCH("k_tc_gemm_dt", st, tc::k_tc_gemm<tc::MODE_DT><<<grid, tc::Roles<tc::MODE_DT>::NT, smem, st>>>(a));
   } else {
     CKT(cudaFuncSetAttribute(tc::k_tc_gemm<tc::MODE_DW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LAUNCH("k_tc_gemm_dw", st, tc::k_tc_gemm<tc::MODE_DW><<<grid, tc::NTHREADS, smem, st>>>(a));
+    LAUNCH("k_tc_gemm_dw", st, tc::k_tc_gemm<tc::MODE_DW><<<grid, tc::Roles<tc::MODE_DW>::NT, smem, st>>>(a));
   }
   CKT(cudaGetLastError());
   return RC_OK;
