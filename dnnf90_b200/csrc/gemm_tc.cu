@@ -27,6 +27,7 @@
 //   DT   Tb[M][N] = A[M][K] W    (A = Sb plane, K = n, N = m)
 //   DW   G[j][1+i] += sum_r A[r][j] B[r][i]  (A = Sb, B = T_{l-1}, both
 //        MN-major tiles, K = rows split across blocks)
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -205,8 +206,14 @@ struct Args {
   int *flag;            // wait time-out / error flag
 };
 
+// FWD/DT epilogue staging: per epilogue warp one 32 x 32 FP32 box, rows of
+// 128 bytes with the 16-byte pieces in the 128-byte swizzle the tensor map
+// of C names, stored to HBM by one TMA bulk tensor store per box
+constexpr int STG_BYTES = 4 * 32 * 32 * 4;
+
 template <int MODE>
-__global__ void __launch_bounds__(Roles<MODE>::NT, 1) k_tc_gemm(Args g) {
+__global__ void __launch_bounds__(Roles<MODE>::NT, 1)
+    k_tc_gemm(Args g, const __grid_constant__ CUtensorMap cmap) {
   constexpr int NPROD_WARPS = Roles<MODE>::PW, NPROD = Roles<MODE>::NPROD;
   constexpr int MMA_WARP = Roles<MODE>::MMA;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -228,6 +235,8 @@ __global__ void __launch_bounds__(Roles<MODE>::NT, 1) k_tc_gemm(Args g) {
   uint64_t *bars = (uint64_t *)(sStage + NST * stage_bytes);
   uint64_t *full = bars, *empty = bars + NST, *tfull = bars + 2 * NST, *tempty = bars + 2 * NST + 2;
   uint32_t *tmem_hold = (uint32_t *)(bars + 2 * NST + 4);
+  // FWD/DT: epilogue staging, 1024-aligned after the barriers
+  uint8_t *sStg = sStage + NST * stage_bytes + 1024;
 
   const int ntn = g.ntn;
   const int tn = blockIdx.y;  // N tile of this block
@@ -507,22 +516,32 @@ __global__ void __launch_bounds__(Roles<MODE>::NT, 1) k_tc_gemm(Args g) {
         const int gr = mt * BM + row;
         const bool ok = gr < g.M;
         const bool brow = (MODE == MODE_FWD) && ok && (gr % g.na == 0);
+        uint8_t *stg = sStg + q * (32 * 32 * 4);
         for (int c0 = 0; c0 < BN; c0 += 32) {
           float v[32];
           tmem_ld32(lane_addr + (uint32_t)(buf * BN + c0), v);
-          if (ok) {
-            float *dst = g.C + (size_t)gr * g.ldc + n0 + c0;
+          if (brow) {
 #pragma unroll
-            for (int i = 0; i < 32; i += 4) {
-              float4 o = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
-              if (brow) {
-                o.x += g.bias[n0 + c0 + i];
-                o.y += g.bias[n0 + c0 + i + 1];
-                o.z += g.bias[n0 + c0 + i + 2];
-                o.w += g.bias[n0 + c0 + i + 3];
-              }
-              if (n0 + c0 + i < g.N) *(float4 *)(dst + i) = o;
-            }
+            for (int i = 0; i < 32; ++i)
+              if (n0 + c0 + i < g.N) v[i] += g.bias[n0 + c0 + i];
+          }
+          // the previous store of this box has read the staging
+          if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          __syncwarp();
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            *(float4 *)(stg + lane * 128 + ((j ^ (lane & 7)) << 4)) =
+                make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+          fence_proxy_async();
+          __syncwarp();
+          if (lane == 0) {
+            // rows past M and columns past N are clipped by the tensor map
+            asm volatile(
+                "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                    &cmap),
+                "r"(n0 + c0), "r"(mt * BM + q * 32), "r"(su32(stg))
+                : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
           }
         }
         tc_fence_before();
@@ -559,6 +578,8 @@ __global__ void __launch_bounds__(Roles<MODE>::NT, 1) k_tc_gemm(Args g) {
     }
   }
 done:
+  if (MODE != MODE_DW && warp >= NPROD_WARPS && warp < MMA_WARP && lane == 0)
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // epilogue stores complete
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -656,7 +677,7 @@ static bool tc_shape_ok(int N, int K) {
   if (N % 16 || K % 16 || N < 16 || K < 16) return false;
   if (N > 128 && N % 128) return false;
   const int BN = std::min(N, 128), nkb = (K + 63) / 64;
-  const size_t smem = (size_t)3 * nkb * BN * 128 + 2 * 3 * 128 * 128 + 2048;
+  const size_t smem = (size_t)3 * nkb * BN * 128 + 2 * 3 * 128 * 128 + 2048 + tc::STG_BYTES;
   return smem <= 227 * 1024;
 }
 
@@ -724,16 +745,42 @@ static int check_flag(int *flag, cudaStream_t st, const char *what) {
   return RC_OK;
 }
 
+// tensor map of the FWD/DT output C[M][N] (row stride ldc floats): boxes of
+// 32 rows x 32 columns in the 128-byte swizzle
+static int c_tensor_map(CUtensorMap *m, float *C, int M, int N, int ldc) {
+  const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)M};
+  const cuuint64_t strides[1] = {(cuuint64_t)ldc * sizeof(float)};
+  const cuuint32_t box[2] = {32, 32};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = cuTensorMapEncodeTiled(
+      m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, estr,
+      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed for a layer GEMM output (code " +
+              std::to_string((int)r) + ")");
+    return RC_DEVICE;
+  }
+  return RC_OK;
+}
+
 static int launch(const tc::Args &a, int mode, dim3 grid, size_t smem, cudaStream_t st) {
+  CUtensorMap cmap;
+  std::memset(&cmap, 0, sizeof cmap);
+  if (mode != tc::MODE_DW) {
+    int rc = c_tensor_map(&cmap, a.C, a.M, a.N, a.ldc);
+    if (rc) return rc;
+    smem += tc::STG_BYTES;
+  }
   if (mode == tc::MODE_FWD) {
     CKT(cudaFuncSetAttribute(tc::k_tc_gemm<tc::MODE_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LAUNCH("k_tc_gemm_fwd", st, tc::k_tc_gemm<tc::MODE_FWD><<<grid, tc::Roles<tc::MODE_FWD>::NT, smem, st>>>(a));
+    LAUNCH("k_tc_gemm_fwd", st, tc::k_tc_gemm<tc::MODE_FWD><<<grid, tc::Roles<tc::MODE_FWD>::NT, smem, st>>>(a, cmap));
   } else if (mode == tc::MODE_DT) {
     CKT(cudaFuncSetAttribute(tc::k_tc_gemm<tc::MODE_DT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LAUNCH("k_tc_gemm_dt", st, tc::k_tc_gemm<tc::MODE_DT><<<grid, tc::Roles<tc::MODE_DT>::NT, smem, st>>>(a));
+    LAUNCH("k_tc_gemm_dt", st, tc::k_tc_gemm<tc::MODE_DT><<<grid, tc::Roles<tc::MODE_DT>::NT, smem, st>>>(a, cmap));
   } else {
     CKT(cudaFuncSetAttribute(tc::k_tc_gemm<tc::MODE_DW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LAUNCH("k_tc_gemm_dw", st, tc::k_tc_gemm<tc::MODE_DW><<<grid, tc::Roles<tc::MODE_DW>::NT, smem, st>>>(a));
+    LAUNCH("k_tc_gemm_dw", st, tc::k_tc_gemm<tc::MODE_DW><<<grid, tc::Roles<tc::MODE_DW>::NT, smem, st>>>(a, cmap));
   }
   CKT(cudaGetLastError());
   return RC_OK;
