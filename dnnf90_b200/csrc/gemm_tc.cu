@@ -152,25 +152,26 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// the three bf16 terms of four FP32 values, packed two per word
+// the three bf16 terms of four FP32 values, packed two per word: x1 =
+// bf16(x), x2 = bf16(x - x1), x3 = bf16(x - x1 - x2), rounded to nearest
+// even two at a time (the residuals are exact in FP32)
+__device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) {
+  return *reinterpret_cast<uint32_t *>(&v);
+}
 __device__ __forceinline__ void split4(float4 x, uint2 &p1, uint2 &p2, uint2 &p3) {
-  float xs[4] = {x.x, x.y, x.z, x.w};
-  uint16_t h[3][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    float r = xs[i];
-    __nv_bfloat16 b1 = __float2bfloat16_rn(r);
-    r = r - __bfloat162float(b1);
-    __nv_bfloat16 b2 = __float2bfloat16_rn(r);
-    r = r - __bfloat162float(b2);
-    __nv_bfloat16 b3 = __float2bfloat16_rn(r);
-    h[0][i] = __bfloat16_as_ushort(b1);
-    h[1][i] = __bfloat16_as_ushort(b2);
-    h[2][i] = __bfloat16_as_ushort(b3);
-  }
-  p1 = make_uint2(h[0][0] | ((uint32_t)h[0][1] << 16), h[0][2] | ((uint32_t)h[0][3] << 16));
-  p2 = make_uint2(h[1][0] | ((uint32_t)h[1][1] << 16), h[1][2] | ((uint32_t)h[1][3] << 16));
-  p3 = make_uint2(h[2][0] | ((uint32_t)h[2][1] << 16), h[2][2] | ((uint32_t)h[2][3] << 16));
+  const __nv_bfloat162 a1 = __floats2bfloat162_rn(x.x, x.y), b1 = __floats2bfloat162_rn(x.z, x.w);
+  const float2 fa = __bfloat1622float2(a1), fb = __bfloat1622float2(b1);
+  float r0 = x.x - fa.x, r1 = x.y - fa.y, r2 = x.z - fb.x, r3 = x.w - fb.y;
+  const __nv_bfloat162 a2 = __floats2bfloat162_rn(r0, r1), b2 = __floats2bfloat162_rn(r2, r3);
+  const float2 ga = __bfloat1622float2(a2), gb = __bfloat1622float2(b2);
+  r0 -= ga.x;
+  r1 -= ga.y;
+  r2 -= gb.x;
+  r3 -= gb.y;
+  const __nv_bfloat162 a3 = __floats2bfloat162_rn(r0, r1), b3 = __floats2bfloat162_rn(r2, r3);
+  p1 = make_uint2(bf2_bits(a1), bf2_bits(b1));
+  p2 = make_uint2(bf2_bits(a2), bf2_bits(b2));
+  p3 = make_uint2(bf2_bits(a3), bf2_bits(b3));
 }
 
 // byte offset of (row, k) in a K-major SW128 tile of 8-row atoms
