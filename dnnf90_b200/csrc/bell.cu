@@ -37,7 +37,7 @@ void DevBellPlan::release() {
   void *ps[] = {fw_list, fw_arec, fw_grec, fw_gc64, fw_gc32, aj_list, aj_orec, aj_pair,
                 aj_c64, aj_c32, f3_list, f3_arec, f3_grec, f3_gc64, f3_gc32, a3_orec,
                 a3_pair, sc64, sc32, f4_grec, a4_pair, f5_list, f5_arec, f5_rec, f5_cpdst,
-                a5_pair, f6_rec};
+                a5_pair, f6_rec, a7_list, a7_unit, a7_out, a7_glist, a7_rec, a7_fin};
   for (void *p : ps)
     if (p) cudaFree(p);
   *this = DevBellPlan();
@@ -111,6 +111,19 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
     d.npair5 = (int)a5.size() / 2;
     if ((rc = put(&d.a5_pair, a5))) return rc;
   }
+  if ((rc = put(&d.a7_list, P.a7_list))) return rc;
+  if ((rc = put(&d.a7_unit, P.a7_unit))) return rc;
+  if ((rc = put(&d.a7_out, P.a7_out))) return rc;
+  if ((rc = put(&d.a7_glist, P.a7_glist))) return rc;
+  if ((rc = put(&d.a7_rec, P.a7_rec))) return rc;
+  if ((rc = put(&d.a7_fin, P.a7_fin))) return rc;
+  d.a7_nunit = (int)P.a7_unit.size() / 8;
+  d.a7_nout = (int)P.a7_out.size();
+  d.a7_nglist = (int)P.a7_glist.size();
+  d.a7_nrec = (int)P.a7_rec.size();
+  d.a7_nfin = (int)P.a7_fin.size() / 2;
+  d.a7_nscratch = P.a7_nscratch;
+  d.a7_ok = P.a7_ok;
   d.f5_ok = P.f5_ok;
   d.nrows5 = P.nrows5;
   d.zuv5 = P.zuv5;
@@ -669,6 +682,175 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj5(Adj5Args a) {
     atomicAdd(a.gbias + (size_t)gj * a.gstride, gb);
 }
 
+// ---------------------------------------------------------------- v7
+struct Adj7Args {
+  int n, na, npts, gstride, gy;
+  int nunit, nout, nglist, nrec, nfin, nscratch;
+  const int *list;
+  const int4 *unit;     // [nunit][2]
+  const int *out;
+  const uint32_t *glist, *rec;
+  const int *fin;       // [nfin][2]
+  const void *sc;       // [3][na]
+  const void *Tb, *h;
+  void *Sb;
+  double *gbias;
+};
+
+// shared-memory layout of the v7 adjoint: two buffers of [Tb | h] rows, the
+// scratch rows, then the tables (16-byte aligned pieces)
+struct Adj7Layout {
+  uint32_t scr, unit, out, gl, rec, fin, total;
+  __host__ __device__ static uint32_t al16(uint32_t v) { return (v + 15u) & ~15u; }
+  __host__ __device__ Adj7Layout(int na, int nscratch, int nunit, int nout, int nglist, int nrec,
+                                 int nfin) {
+    scr = 4u * na * 128u;
+    unit = scr + (uint32_t)nscratch * 128u;
+    out = unit + (uint32_t)nunit * 32u;
+    gl = al16(out + (uint32_t)nout * 4u);
+    rec = al16(gl + (uint32_t)nglist * 4u);
+    fin = al16(rec + (uint32_t)nrec * 4u);
+    total = al16(fin + (uint32_t)nfin * 8u);
+  }
+};
+
+// one unit: acc[k] += (a! Tb)_{b_k + g} (h/g!)_g over its g range
+template <typename R, int NK>
+__device__ __forceinline__ void adj7_unit(unsigned char *sm, uint32_t lc, const uint32_t *rec,
+                                          const uint32_t *gl, int ng, R (&acc)[16]) {
+  constexpr int ST = NK <= 2 ? NK : (NK + 3) / 4 * 4;
+#pragma unroll 2
+  for (int g = 0; g < ng; ++g) {
+    const R hv = srow<R>(sm, lc + gl[g]);
+    const uint32_t *r = rec + g * ST;
+    uint32_t o[ST];
+    if constexpr (ST % 4 == 0) {
+#pragma unroll
+      for (int q = 0; q < ST / 4; ++q) *(uint4 *)&o[4 * q] = ((const uint4 *)r)[q];
+    } else if constexpr (ST == 2) {
+      *(uint2 *)o = *(const uint2 *)r;
+    } else {
+      o[0] = r[0];
+    }
+#pragma unroll
+    for (int k = 0; k < NK; ++k) acc[k] += srow<R>(sm, lc + o[k]) * hv;
+  }
+}
+
+// Bell adjoint v7, grouped correlation (bell_plan.hpp): units of up to 16
+// outputs sharing each h_g load; split outputs summed in scratch rows.
+template <typename R, int NPB>
+__global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj7(Adj7Args a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char *sm = smem_raw;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool lact = lane < NPB;
+  const int ln = lact ? lane : 0;
+  const int n = a.n, na = a.na;
+  const size_t plane = (size_t)na * n;
+  const uint32_t bufb = 2 * na * 128;
+  const Adj7Layout L(na, a.nscratch, a.nunit, a.nout, a.nglist, a.nrec, a.nfin);
+  int4 *su = (int4 *)(sm + L.unit);
+  int *so = (int *)(sm + L.out);
+  uint32_t *sg = (uint32_t *)(sm + L.gl);
+  uint32_t *sr = (uint32_t *)(sm + L.rec);
+  int *sf = (int *)(sm + L.fin);
+  for (int i = threadIdx.x; i < 2 * a.nunit; i += blockDim.x) su[i] = __ldg(a.unit + i);
+  for (int i = threadIdx.x; i < a.nout; i += blockDim.x) so[i] = __ldg(a.out + i);
+  for (int i = threadIdx.x; i < a.nglist; i += blockDim.x) sg[i] = __ldg(a.glist + i);
+  for (int i = threadIdx.x; i < a.nrec; i += blockDim.x) sr[i] = __ldg(a.rec + i);
+  for (int i = threadIdx.x; i < 2 * a.nfin; i += blockDim.x) sf[i] = __ldg(a.fin + i);
+  for (int i = threadIdx.x; i < a.nscratch * 32; i += blockDim.x) ((uint32_t *)(sm + L.scr))[i] = 0u;
+  const R *sc = (const R *)a.sc;
+  const int rs = __ldg(a.list + warp * 2), rn = __ldg(a.list + warp * 2 + 1);
+  double gb = 0.0;
+  int gj = -1;
+  int buf = 0;
+  const long nitem = (long)a.npts * a.gy;
+  const long it0 = (long)blockIdx.x * nitem / gridDim.x;
+  const long it1 = (long)(blockIdx.x + 1) * nitem / gridDim.x;
+  if (it0 < it1) {
+    const size_t o = (it0 % a.npts) * plane;
+    const int j0 = (int)(it0 / a.npts) * NPB;
+    stage_rows<NPB, R>(sm, (const R *)a.Tb + o, na, n, j0, ADJ_WORKERS * 32);
+    stage_rows<NPB, R>(sm + na * 128, (const R *)a.h + o, na, n, j0, ADJ_WORKERS * 32);
+  }
+  cp_async_commit();
+  for (long it = it0; it < it1; ++it) {
+    const int pt = (int)(it % a.npts);
+    const int j = (int)(it / a.npts) * NPB + ln;
+    const bool act = lact && j < n;
+    if (j != gj) {
+      if (a.gbias && gj >= 0 && gj < n && lact && gb != 0.0)
+        atomicAdd(a.gbias + (size_t)gj * a.gstride, gb);
+      gb = 0.0;
+      gj = j;
+    }
+    if (it + 1 < it1) {
+      unsigned char *oth = sm + (buf ^ 1) * bufb;
+      const size_t o = ((it + 1) % a.npts) * plane;
+      const int j0 = (int)((it + 1) / a.npts) * NPB;
+      stage_rows<NPB, R>(oth, (const R *)a.Tb + o, na, n, j0, ADJ_WORKERS * 32);
+      stage_rows<NPB, R>(oth + na * 128, (const R *)a.h + o, na, n, j0, ADJ_WORKERS * 32);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const uint32_t lc = buf * bufb + ln * sizeof(R);
+    for (int r = warp; r < 2 * na; r += ADJ_WORKERS)
+      if (lact) srow<R>(sm, lc + r * 128) *= __ldg(sc + r);
+    __syncthreads();
+    R *Sb = (R *)a.Sb + pt * plane;
+    for (int u = rs; u < rs + rn; ++u) {
+      const int4 U0 = su[2 * u], U1 = su[2 * u + 1];
+      const int nk = U0.z & 0xff;
+      const bool partial = (U0.z >> 8) != 0;
+      R acc[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) acc[k] = (R)0;
+      const uint32_t *rec = sr + U0.x;
+      const uint32_t *gl = sg + U1.x;
+      switch (nk) {
+#define A7CASE(N) case N: adj7_unit<R, N>(sm, lc, rec, gl, U0.y, acc); break;
+        A7CASE(1) A7CASE(2) A7CASE(3) A7CASE(4) A7CASE(5) A7CASE(6) A7CASE(7) A7CASE(8)
+        A7CASE(9) A7CASE(10) A7CASE(11) A7CASE(12) A7CASE(13) A7CASE(14) A7CASE(15) A7CASE(16)
+#undef A7CASE
+        default: break;
+      }
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        if (k < nk) {
+          const int ob = so[U0.w + k];
+          const int b = ob & 0xffff;
+          if (partial) {
+            if (lact) atomicAdd((R *)(sm + L.scr + (ob >> 16) * 128) + ln, acc[k]);
+          } else {
+            const R v = acc[k] * __ldg(sc + 2 * na + b);
+            if (act) Sb[(size_t)b * n + j] = v;
+            if (b == 0) gb += (double)v;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // outputs whose g lists were split: scale, store, and clear the row
+    for (int i = warp; i < a.nfin; i += ADJ_WORKERS) {
+      const int b = sf[2 * i], row = sf[2 * i + 1];
+      R *cell = (R *)(sm + L.scr + row * 128) + ln;
+      const R v = *cell * __ldg(sc + 2 * na + b);
+      __syncwarp();
+      if (lact) *cell = (R)0;
+      if (act) Sb[(size_t)b * n + j] = v;
+      if (b == 0) gb += (double)v;
+    }
+    __syncthreads();
+    buf ^= 1;
+  }
+  cp_async_wait<0>();
+  if (a.gbias && gj >= 0 && gj < n && lact && gb != 0.0)
+    atomicAdd(a.gbias + (size_t)gj * a.gstride, gb);
+}
+
 static int sm_count_b() {
   static int n = 0;
   if (!n) {
@@ -901,9 +1083,29 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
       CKB(cudaGetLastError());
       return RC_OK;
     };
-    const int nvar = srec_fits ? 2 : 1;
+    const Adj7Layout L7(t.na, bp.a7_nscratch, bp.a7_nunit, bp.a7_nout, bp.a7_nglist,
+                        bp.a7_nrec, bp.a7_nfin);
+    const bool v7_fits = bp.a7_ok && L7.total <= 227 * 1024;
+    auto launch_all = [&](int v, bool last) -> int {
+      if (v < 2) return launch(v, last);
+      // variant 2: grouped correlation (v7)
+      Adj7Args c;
+      c.n = n; c.na = t.na; c.npts = npts; c.gstride = gstride; c.gy = b.gy;
+      c.nunit = bp.a7_nunit; c.nout = bp.a7_nout; c.nglist = bp.a7_nglist; c.nrec = bp.a7_nrec;
+      c.nfin = bp.a7_nfin; c.nscratch = bp.a7_nscratch;
+      c.list = bp.a7_list; c.unit = (const int4 *)bp.a7_unit; c.out = bp.a7_out;
+      c.glist = bp.a7_glist; c.rec = bp.a7_rec; c.fin = bp.a7_fin;
+      c.sc = b.sc; c.Tb = Tb; c.h = h; c.Sb = Sb; c.gbias = last ? gbias : nullptr;
+      auto k = k_bell_adj7<R, NPB>;
+      CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L7.total));
+      const int grid = persistent_grid((const void *)k, ADJ_WORKERS * 32, L7.total, (long)npts * b.gy);
+      LAUNCH("k_bell_adj", st, k<<<grid, ADJ_WORKERS * 32, L7.total, st>>>(c));
+      CKB(cudaGetLastError());
+      return RC_OK;
+    };
+    const int nvar = v7_fits ? 3 : srec_fits ? 2 : 1;
     return tuned_launch(TuneKey{bp.id, 2, n, (int)sizeof(R)}, nvar, nvar - 1,
-                        (long)npts * b.gy, st, launch);
+                        (long)npts * b.gy, st, launch_all);
   }
   Adj2Args a;
   a.n = n; a.na = t.na; a.npts = npts; a.gstride = gstride; a.list = bp.aj_list;
