@@ -34,10 +34,15 @@ namespace dnnf90 {
   } while (0)
 
 void DevBellPlan::release() {
+  for (auto &D : a7) {
+    void *q[] = {D.list, D.unit, D.out, D.fin, D.glist, D.rec};
+    for (void *p : q)
+      if (p) cudaFree(p);
+  }
   void *ps[] = {fw_list, fw_arec, fw_grec, fw_gc64, fw_gc32, aj_list, aj_orec, aj_pair,
                 aj_c64, aj_c32, f3_list, f3_arec, f3_grec, f3_gc64, f3_gc32, a3_orec,
                 a3_pair, sc64, sc32, f4_grec, a4_pair, f5_list, f5_arec, f5_rec, f5_cpdst,
-                a5_pair, f6_rec, a7_list, a7_unit, a7_out, a7_glist, a7_rec, a7_fin};
+                a5_pair, f6_rec};
   for (void *p : ps)
     if (p) cudaFree(p);
   *this = DevBellPlan();
@@ -111,19 +116,23 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
     d.npair5 = (int)a5.size() / 2;
     if ((rc = put(&d.a5_pair, a5))) return rc;
   }
-  if ((rc = put(&d.a7_list, P.a7_list))) return rc;
-  if ((rc = put(&d.a7_unit, P.a7_unit))) return rc;
-  if ((rc = put(&d.a7_out, P.a7_out))) return rc;
-  if ((rc = put(&d.a7_glist, P.a7_glist))) return rc;
-  if ((rc = put(&d.a7_rec, P.a7_rec))) return rc;
-  if ((rc = put(&d.a7_fin, P.a7_fin))) return rc;
-  d.a7_nunit = (int)P.a7_unit.size() / 8;
-  d.a7_nout = (int)P.a7_out.size();
-  d.a7_nglist = (int)P.a7_glist.size();
-  d.a7_nrec = (int)P.a7_rec.size();
-  d.a7_nfin = (int)P.a7_fin.size() / 2;
-  d.a7_nscratch = P.a7_nscratch;
-  d.a7_ok = P.a7_ok;
+  for (int v = 0; v < 2; ++v) {
+    const A7Plan &Q = v ? P.a7d : P.a7f;
+    DevBellPlan::A7Dev &D = d.a7[v];
+    if ((rc = put(&D.list, Q.list))) return rc;
+    if ((rc = put(&D.unit, Q.unit))) return rc;
+    if ((rc = put(&D.out, Q.out))) return rc;
+    if ((rc = put(&D.glist, Q.glist))) return rc;
+    if ((rc = put(&D.rec, Q.rec))) return rc;
+    if ((rc = put(&D.fin, Q.fin))) return rc;
+    D.nunit = (int)Q.unit.size() / 8;
+    D.nout = (int)Q.out.size();
+    D.nglist = (int)Q.glist.size();
+    D.nrec = (int)Q.rec.size();
+    D.nfin = (int)Q.fin.size() / 2;
+    D.nscratch = Q.nscratch;
+    D.ok = Q.ok;
+  }
   d.f5_ok = P.f5_ok;
   d.nrows5 = P.nrows5;
   d.zuv5 = P.zuv5;
@@ -714,26 +723,88 @@ struct Adj7Layout {
   }
 };
 
-// one unit: acc[k] += (a! Tb)_{b_k + g} (h/g!)_g over its g range
+// 32-bit shared-window loads (the operands live in dynamic shared memory;
+// volatile keeps them between the block's barriers)
+__device__ __forceinline__ uint32_t ld_s32(uint32_t a) {
+  uint32_t v;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint2 ld_s64(uint32_t a) {
+  uint2 v;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint4 ld_s128(uint32_t a) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(a));
+  return v;
+}
+template <typename R>
+__device__ __forceinline__ R ld_sr(uint32_t a);
+template <>
+__device__ __forceinline__ float ld_sr<float>(uint32_t a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+template <>
+__device__ __forceinline__ double ld_sr<double>(uint32_t a) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
+  return v;
+}
+
+// one unit: acc[k] += (a! Tb)_{b_k + g} (h/g!)_g over its g range, then
+// its nk outputs: scaled by 1/b! and stored (or added to the output's
+// scratch row when its g list is split).  lcs is this lane's shared address
+// in the current buffer; rec, gl shared addresses of the unit's tables.
 template <typename R, int NK>
-__device__ __forceinline__ void adj7_unit(unsigned char *sm, uint32_t lc, const uint32_t *rec,
-                                          const uint32_t *gl, int ng, R (&acc)[16]) {
+__device__ __forceinline__ void adj7_unit(uint32_t lcs, uint32_t rec, uint32_t gl, int ng,
+                                          bool partial, const int *outs, unsigned char *scr,
+                                          const R *scb, R *Sb, int n, int j, int ln, bool lact,
+                                          bool act, double &gb) {
   constexpr int ST = NK <= 2 ? NK : (NK + 3) / 4 * 4;
+  R acc[NK];
+#pragma unroll
+  for (int k = 0; k < NK; ++k) acc[k] = (R)0;
 #pragma unroll 2
   for (int g = 0; g < ng; ++g) {
-    const R hv = srow<R>(sm, lc + gl[g]);
-    const uint32_t *r = rec + g * ST;
+    const R hv = ld_sr<R>(lcs + ld_s32(gl + 4 * g));
+    const uint32_t r = rec + 4 * ST * g;
     uint32_t o[ST];
     if constexpr (ST % 4 == 0) {
 #pragma unroll
-      for (int q = 0; q < ST / 4; ++q) *(uint4 *)&o[4 * q] = ((const uint4 *)r)[q];
+      for (int q = 0; q < ST / 4; ++q) {
+        const uint4 v = ld_s128(r + 16 * q);
+        o[4 * q] = v.x;
+        o[4 * q + 1] = v.y;
+        o[4 * q + 2] = v.z;
+        o[4 * q + 3] = v.w;
+      }
     } else if constexpr (ST == 2) {
-      *(uint2 *)o = *(const uint2 *)r;
+      const uint2 v = ld_s64(r);
+      o[0] = v.x;
+      o[1] = v.y;
     } else {
-      o[0] = r[0];
+      o[0] = ld_s32(r);
     }
 #pragma unroll
-    for (int k = 0; k < NK; ++k) acc[k] += srow<R>(sm, lc + o[k]) * hv;
+    for (int k = 0; k < NK; ++k) acc[k] += ld_sr<R>(lcs + o[k]) * hv;
+  }
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    const int ob = outs[k];
+    const int b = ob & 0xffff;
+    if (partial) {
+      if (lact) atomicAdd((R *)(scr + (ob >> 16) * 128) + ln, acc[k]);
+    } else {
+      const R v = acc[k] * __ldg(scb + b);
+      if (act) Sb[(size_t)b * n + j] = v;
+      if (b == 0) gb += (double)v;
+    }
   }
 }
 
@@ -805,31 +876,32 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj7(Adj7Args a) {
       const int4 U0 = su[2 * u], U1 = su[2 * u + 1];
       const int nk = U0.z & 0xff;
       const bool partial = (U0.z >> 8) != 0;
-      R acc[16];
-#pragma unroll
-      for (int k = 0; k < 16; ++k) acc[k] = (R)0;
-      const uint32_t *rec = sr + U0.x;
-      const uint32_t *gl = sg + U1.x;
+      const uint32_t rec = smem_u32(sr + U0.x);
+      const uint32_t gl = smem_u32(sg + U1.x);
+      const uint32_t lcs = smem_u32(sm) + lc;
       switch (nk) {
-#define A7CASE(N) case N: adj7_unit<R, N>(sm, lc, rec, gl, U0.y, acc); break;
+#define A7CASE(N)                                                                        \
+  case N:                                                                                \
+    adj7_unit<R, N>(lcs, rec, gl, U0.y, partial, so + U0.w, sm + L.scr, sc + 2 * na, Sb, n, \
+                    j, ln, lact, act, gb);                                                \
+    break;
         A7CASE(1) A7CASE(2) A7CASE(3) A7CASE(4) A7CASE(5) A7CASE(6) A7CASE(7) A7CASE(8)
-        A7CASE(9) A7CASE(10) A7CASE(11) A7CASE(12) A7CASE(13) A7CASE(14) A7CASE(15) A7CASE(16)
 #undef A7CASE
-        default: break;
-      }
-#pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        if (k < nk) {
-          const int ob = so[U0.w + k];
-          const int b = ob & 0xffff;
-          if (partial) {
-            if (lact) atomicAdd((R *)(sm + L.scr + (ob >> 16) * 128) + ln, acc[k]);
-          } else {
-            const R v = acc[k] * __ldg(sc + 2 * na + b);
-            if (act) Sb[(size_t)b * n + j] = v;
-            if (b == 0) gb += (double)v;
+        default:
+          if constexpr (sizeof(R) == 4) {  // the FP32 plan holds up to 16 outputs
+            switch (nk) {
+#define A7CASE(N)                                                                        \
+  case N:                                                                                \
+    adj7_unit<R, N>(lcs, rec, gl, U0.y, partial, so + U0.w, sm + L.scr, sc + 2 * na, Sb, n, \
+                    j, ln, lact, act, gb);                                                \
+    break;
+              A7CASE(9) A7CASE(10) A7CASE(11) A7CASE(12) A7CASE(13) A7CASE(14) A7CASE(15)
+              A7CASE(16)
+#undef A7CASE
+              default: break;
+            }
           }
-        }
+          break;
       }
     }
     __syncthreads();
@@ -1083,18 +1155,18 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
       CKB(cudaGetLastError());
       return RC_OK;
     };
-    const Adj7Layout L7(t.na, bp.a7_nscratch, bp.a7_nunit, bp.a7_nout, bp.a7_nglist,
-                        bp.a7_nrec, bp.a7_nfin);
-    const bool v7_fits = bp.a7_ok && L7.total <= 227 * 1024;
+    const DevBellPlan::A7Dev &A7 = bp.a7[sizeof(R) == 8 ? 1 : 0];
+    const Adj7Layout L7(t.na, A7.nscratch, A7.nunit, A7.nout, A7.nglist, A7.nrec, A7.nfin);
+    const bool v7_fits = A7.ok && L7.total <= 227 * 1024;
     auto launch_all = [&](int v, bool last) -> int {
       if (v < 2) return launch(v, last);
       // variant 2: grouped correlation (v7)
       Adj7Args c;
       c.n = n; c.na = t.na; c.npts = npts; c.gstride = gstride; c.gy = b.gy;
-      c.nunit = bp.a7_nunit; c.nout = bp.a7_nout; c.nglist = bp.a7_nglist; c.nrec = bp.a7_nrec;
-      c.nfin = bp.a7_nfin; c.nscratch = bp.a7_nscratch;
-      c.list = bp.a7_list; c.unit = (const int4 *)bp.a7_unit; c.out = bp.a7_out;
-      c.glist = bp.a7_glist; c.rec = bp.a7_rec; c.fin = bp.a7_fin;
+      c.nunit = A7.nunit; c.nout = A7.nout; c.nglist = A7.nglist; c.nrec = A7.nrec;
+      c.nfin = A7.nfin; c.nscratch = A7.nscratch;
+      c.list = A7.list; c.unit = (const int4 *)A7.unit; c.out = A7.out;
+      c.glist = A7.glist; c.rec = A7.rec; c.fin = A7.fin;
       c.sc = b.sc; c.Tb = Tb; c.h = h; c.Sb = Sb; c.gbias = last ? gbias : nullptr;
       auto k = k_bell_adj7<R, NPB>;
       CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L7.total));

@@ -41,11 +41,13 @@ struct DevBellPlan {
   uint32_t *f5_rec = nullptr, *a5_pair = nullptr;
   uint32_t *f6_rec = nullptr;   // forward records as row indices
   int nrec32 = 0, norec = 0, npair5 = 0;
-  // v7 adjoint (grouped correlation)
-  int *a7_list = nullptr, *a7_unit = nullptr, *a7_out = nullptr, *a7_fin = nullptr;
-  uint32_t *a7_glist = nullptr, *a7_rec = nullptr;
-  int a7_nunit = 0, a7_nout = 0, a7_nglist = 0, a7_nrec = 0, a7_nfin = 0, a7_nscratch = 0;
-  bool a7_ok = false;
+  // v7 adjoint (grouped correlation): [0] FP32 plan, [1] FP64 plan
+  struct A7Dev {
+    int *list = nullptr, *unit = nullptr, *out = nullptr, *fin = nullptr;
+    uint32_t *glist = nullptr, *rec = nullptr;
+    int nunit = 0, nout = 0, nglist = 0, nrec = 0, nfin = 0, nscratch = 0;
+    bool ok = false;
+  } a7[2];
   double *sc64 = nullptr;  // [3][na]: a!, 1/a!, 1/a! (Tb, h, Sb scales)
   float *sc32 = nullptr;
   void release();

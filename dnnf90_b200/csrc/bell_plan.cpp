@@ -30,6 +30,118 @@ std::vector<std::vector<int>> balance(const std::vector<long> &cost, int workers
 
 int a7_stride(int nk) { return nk <= 2 ? nk : (nk + 3) / 4 * 4; }
 
+// the v7 adjoint plan with units of at most nkmax outputs
+static A7Plan build_a7(const TableSet &t, int aj_workers, int nkmax) {
+  A7Plan P;
+  const int na = t.na;
+    const int ROW = 128;
+    // g list of every output (output 0 pairs every a with itself, g = a)
+    std::map<std::vector<int>, std::vector<int>> groups;
+    {
+      std::vector<int> all(na);
+      std::iota(all.begin(), all.end(), 0);
+      groups[all].push_back(0);
+    }
+    for (int ib = 1; ib < na; ++ib) {
+      std::vector<int> gl;
+      for (int ip = t.pair_start[ib]; ip < t.pair_start[ib] + t.pair_num[ib]; ++ip)
+        gl.push_back(t.pair_id[ip]);
+      std::sort(gl.begin(), gl.end());
+      groups[gl].push_back(ib);
+    }
+    long total = 0;
+    for (auto &kv : groups) total += (long)kv.first.size() * kv.second.size();
+    const double target = std::max(8.0, (double)total / aj_workers * 0.5);
+    struct Unit {
+      const std::vector<int> *gl;  // the group's g list
+      int gstart, g0, ng;
+      std::vector<int> outs;
+      bool partial;
+      long cost;
+    };
+    std::vector<Unit> units;
+    std::vector<int> scratch_of(na, -1);
+    P.nscratch = 0;
+    for (auto &kv : groups) {
+      const std::vector<int> &gl = kv.first, &outs = kv.second;
+      const int G = (int)gl.size();
+      const int gstart = (int)P.glist.size();
+      for (int g : gl) P.glist.push_back((uint32_t)(na + g) * ROW);
+      // up to nkmax outputs per unit, evenly spread
+      const int nchunk = ((int)outs.size() + nkmax - 1) / nkmax;
+      for (int c = 0; c < nchunk; ++c) {
+        const size_t o0 = (size_t)c * outs.size() / nchunk, o1 = (size_t)(c + 1) * outs.size() / nchunk;
+        const int nk = (int)(o1 - o0);
+        // the g list split so that one unit holds about `target` products
+        const int nsplit = std::max(1, (int)std::lround((double)G * nk / target));
+        const int parts = std::min(nsplit, G);
+        for (int sp = 0; sp < parts; ++sp) {
+          Unit u;
+          u.gl = &gl;
+          u.gstart = gstart;
+          u.g0 = (int)((long)sp * G / parts);
+          u.ng = (int)((long)(sp + 1) * G / parts) - u.g0;
+          u.outs.assign(outs.begin() + o0, outs.begin() + o1);
+          u.partial = parts > 1;
+          u.cost = (long)u.ng * (2 * nk + 2) + 16;
+          units.push_back(u);
+        }
+        if (parts > 1)
+          for (size_t o = o0; o < o1; ++o) scratch_of[outs[o]] = P.nscratch++;
+      }
+    }
+    P.fin.clear();
+    for (int b = 0; b < na; ++b)
+      if (scratch_of[b] >= 0) {
+        P.fin.push_back(b);
+        P.fin.push_back(scratch_of[b]);
+      }
+    std::vector<long> cost;
+    for (auto &u : units) cost.push_back(u.cost);
+    auto asg = balance(cost, aj_workers);
+    P.list.assign((size_t)aj_workers * 2, 0);
+    for (int w = 0; w < aj_workers; ++w) {
+      P.list[w * 2] = (int)P.unit.size() / 8;
+      P.list[w * 2 + 1] = (int)asg[w].size();
+      for (int ui : asg[w]) {
+        const Unit &u = units[ui];
+        const int nk = (int)u.outs.size();
+        const int stride = a7_stride(nk);
+        while (P.rec.size() % 4) P.rec.push_back(0);
+        P.unit.push_back((int)P.rec.size());
+        P.unit.push_back(u.ng);
+        P.unit.push_back(nk | (u.partial ? 1 << 8 : 0));
+        P.unit.push_back((int)P.out.size());
+        P.unit.push_back(u.gstart + u.g0);
+        P.unit.push_back(0);
+        P.unit.push_back(0);
+        P.unit.push_back(0);
+        for (int b : u.outs) P.out.push_back(b | ((u.partial ? scratch_of[b] : 0) << 16));
+        for (int gi = u.g0; gi < u.g0 + u.ng; ++gi) {
+          const int g = (*u.gl)[gi];
+          for (int b : u.outs) {
+            int a = g;  // output 0: the partner of g is g
+            if (b != 0) {
+              std::vector<int> v(t.d0);
+              for (int i = 0; i < t.d0; ++i)
+                v[i] = t.alpha[(size_t)b * t.d0 + i] + t.alpha[(size_t)g * t.d0 + i];
+              a = t.find(v.data());
+            }
+            P.rec.push_back((uint32_t)a * ROW);
+          }
+          for (int e = nk; e < stride; ++e) P.rec.push_back(0);
+        }
+      }
+    }
+    for (int i = 0; i < 16; ++i) P.rec.push_back(0);
+    for (int i = 0; i < 4; ++i) P.glist.push_back(0);
+    P.ok = na < 65536 && P.nscratch < 65536;
+    for (size_t i = 0; i < P.rec.size(); ++i)
+      if (P.rec[i] >= (uint32_t)(2 * na) * ROW) P.ok = false;
+  
+  return P;
+}
+
 BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
   BellPlan P;
   P.workers = workers;
@@ -292,113 +404,8 @@ BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
         for (int v = 2; v <= t.alpha[(size_t)ia * t.d0 + i]; ++v) P.fact[ia] *= v;
   }
 
-  // ---- adjoint v7 (grouped correlation; see bell_plan.hpp)
-  {
-    const int ROW = 128;
-    // g list of every output (output 0 pairs every a with itself, g = a)
-    std::map<std::vector<int>, std::vector<int>> groups;
-    {
-      std::vector<int> all(na);
-      std::iota(all.begin(), all.end(), 0);
-      groups[all].push_back(0);
-    }
-    for (int ib = 1; ib < na; ++ib) {
-      std::vector<int> gl;
-      for (int ip = t.pair_start[ib]; ip < t.pair_start[ib] + t.pair_num[ib]; ++ip)
-        gl.push_back(t.pair_id[ip]);
-      std::sort(gl.begin(), gl.end());
-      groups[gl].push_back(ib);
-    }
-    long total = 0;
-    for (auto &kv : groups) total += (long)kv.first.size() * kv.second.size();
-    const double target = std::max(8.0, (double)total / aj_workers * 0.5);
-    struct Unit {
-      const std::vector<int> *gl;  // the group's g list
-      int gstart, g0, ng;
-      std::vector<int> outs;
-      bool partial;
-      long cost;
-    };
-    std::vector<Unit> units;
-    std::vector<int> scratch_of(na, -1);
-    P.a7_nscratch = 0;
-    for (auto &kv : groups) {
-      const std::vector<int> &gl = kv.first, &outs = kv.second;
-      const int G = (int)gl.size();
-      const int gstart = (int)P.a7_glist.size();
-      for (int g : gl) P.a7_glist.push_back((uint32_t)(na + g) * ROW);
-      // up to 16 outputs per unit, evenly spread
-      const int nchunk = ((int)outs.size() + 15) / 16;
-      for (int c = 0; c < nchunk; ++c) {
-        const size_t o0 = (size_t)c * outs.size() / nchunk, o1 = (size_t)(c + 1) * outs.size() / nchunk;
-        const int nk = (int)(o1 - o0);
-        // the g list split so that one unit holds about `target` products
-        const int nsplit = std::max(1, (int)std::lround((double)G * nk / target));
-        const int parts = std::min(nsplit, G);
-        for (int sp = 0; sp < parts; ++sp) {
-          Unit u;
-          u.gl = &gl;
-          u.gstart = gstart;
-          u.g0 = (int)((long)sp * G / parts);
-          u.ng = (int)((long)(sp + 1) * G / parts) - u.g0;
-          u.outs.assign(outs.begin() + o0, outs.begin() + o1);
-          u.partial = parts > 1;
-          u.cost = (long)u.ng * (2 * nk + 2) + 16;
-          units.push_back(u);
-        }
-        if (parts > 1)
-          for (size_t o = o0; o < o1; ++o) scratch_of[outs[o]] = P.a7_nscratch++;
-      }
-    }
-    P.a7_fin.clear();
-    for (int b = 0; b < na; ++b)
-      if (scratch_of[b] >= 0) {
-        P.a7_fin.push_back(b);
-        P.a7_fin.push_back(scratch_of[b]);
-      }
-    std::vector<long> cost;
-    for (auto &u : units) cost.push_back(u.cost);
-    auto asg = balance(cost, aj_workers);
-    P.a7_list.assign((size_t)aj_workers * 2, 0);
-    for (int w = 0; w < aj_workers; ++w) {
-      P.a7_list[w * 2] = (int)P.a7_unit.size() / 8;
-      P.a7_list[w * 2 + 1] = (int)asg[w].size();
-      for (int ui : asg[w]) {
-        const Unit &u = units[ui];
-        const int nk = (int)u.outs.size();
-        const int stride = a7_stride(nk);
-        while (P.a7_rec.size() % 4) P.a7_rec.push_back(0);
-        P.a7_unit.push_back((int)P.a7_rec.size());
-        P.a7_unit.push_back(u.ng);
-        P.a7_unit.push_back(nk | (u.partial ? 1 << 8 : 0));
-        P.a7_unit.push_back((int)P.a7_out.size());
-        P.a7_unit.push_back(u.gstart + u.g0);
-        P.a7_unit.push_back(0);
-        P.a7_unit.push_back(0);
-        P.a7_unit.push_back(0);
-        for (int b : u.outs) P.a7_out.push_back(b | ((u.partial ? scratch_of[b] : 0) << 16));
-        for (int gi = u.g0; gi < u.g0 + u.ng; ++gi) {
-          const int g = (*u.gl)[gi];
-          for (int b : u.outs) {
-            int a = g;  // output 0: the partner of g is g
-            if (b != 0) {
-              std::vector<int> v(t.d0);
-              for (int i = 0; i < t.d0; ++i)
-                v[i] = t.alpha[(size_t)b * t.d0 + i] + t.alpha[(size_t)g * t.d0 + i];
-              a = t.find(v.data());
-            }
-            P.a7_rec.push_back((uint32_t)a * ROW);
-          }
-          for (int e = nk; e < stride; ++e) P.a7_rec.push_back(0);
-        }
-      }
-    }
-    for (int i = 0; i < 16; ++i) P.a7_rec.push_back(0);
-    for (int i = 0; i < 4; ++i) P.a7_glist.push_back(0);
-    P.a7_ok = na < 65536 && P.a7_nscratch < 65536;
-    for (size_t i = 0; i < P.a7_rec.size(); ++i)
-      if (P.a7_rec[i] >= (uint32_t)(2 * na) * ROW) P.a7_ok = false;
-  }
+  P.a7f = build_a7(t, aj_workers, 16);
+  P.a7d = build_a7(t, aj_workers, 8);
 
   // adjoint outputs: Sb_0 (pairs (a, a) for every a) and every Sb_b, b >= 1
   std::vector<long> cost;

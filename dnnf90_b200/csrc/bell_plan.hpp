@@ -19,6 +19,24 @@
 
 namespace dnnf90 {
 
+// Adjoint v7, grouped correlation.  Outputs whose lists {g : b + g
+// carried} are equal (for a dense set: every b of one degree; output 0
+// pairs every a with itself) form units of up to nkmax outputs that share
+// each h_g load:  acc_k += (a! Tb)_{b_k + g} (h/g!)_g  over a range of the
+// group's g list.  A group whose list is long is split over several units;
+// their partial sums meet in a shared scratch row per output.
+struct A7Plan {
+  std::vector<int> list;        // [workers][2]: start, count into unit
+  std::vector<int> unit;        // [*][8]: record start (words, 4-aligned), ng,
+                                //   nk | partial << 8, out start, g-list start, 0, 0, 0
+  std::vector<int> out;         // output slot | scratch row << 16
+  std::vector<uint32_t> glist;  // byte offsets of the h rows, per group
+  std::vector<uint32_t> rec;    // per unit and g: a7_stride(nk) words of Tb row offsets
+  std::vector<int> fin;         // [*][2]: output slot, scratch row (split outputs)
+  int nscratch = 0;
+  bool ok = false;
+};
+
 struct BellPlan {
   int workers = 0, k = 0, na = 0, nslot = 0;
   // forward
@@ -66,21 +84,9 @@ struct BellPlan {
   std::vector<uint32_t> f5_rec;    // [*][2]
   std::vector<int> f5_cpdst;       // [na]: byte offset of the level-1 copy of S_a, or -1
   std::vector<uint32_t> f6_rec;    // the f5 records as rows: x row | z row << 16
-  // adjoint v7, grouped correlation.  Outputs whose lists {g : b + g
-  // carried} are equal (for a dense set: every b of one degree; output 0
-  // pairs every a with itself) form units of up to 16 outputs that share
-  // each h_g load:  acc_k += (a! Tb)_{b_k + g} (h/g!)_g  over a range of
-  // the group's g list.  A group whose list is long is split over several
-  // units; their partial sums meet in a shared scratch row per output.
-  std::vector<int> a7_list;        // [workers][2]: start, count into a7_unit
-  std::vector<int> a7_unit;        // [*][8]: record start (words, 4-aligned), ng,
-                                   //   nk | partial << 8, out start, g-list start, 0, 0, 0
-  std::vector<int> a7_out;         // output slot | scratch row << 16
-  std::vector<uint32_t> a7_glist;  // byte offsets of the h rows, per group
-  std::vector<uint32_t> a7_rec;    // per unit and g: a7_stride(nk) words of Tb row offsets
-  std::vector<int> a7_fin;         // [*][2]: output slot, scratch row (split outputs)
-  int a7_nscratch = 0;
-  bool a7_ok = false;
+  // adjoint v7, grouped correlation (A7Plan): FP32 units of up to 16
+  // outputs, FP64 units of up to 8 (one lane's accumulators in registers)
+  A7Plan a7f, a7d;
   // adjoint, v3: Sb_b b! = sum_{a >= b} (a! Tb_a) (h_{a-b} / (a-b)!), the
   // pair coefficient C(a,b) = a!/(b!(a-b)!) folded into per-row scales
   std::vector<int> a3_orec;   // [*][4]: ib, pstart, pcount, 0
