@@ -62,7 +62,7 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
         subprocess.run(cmd, check=True)
         changed = True
     if changed or not os.path.exists(LIB):
-        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcublas", "-lcuda"]
+        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcublas"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -746,6 +746,26 @@ static int check_flag(int *flag, cudaStream_t st, const char *what) {
   return RC_OK;
 }
 
+// cuTensorMapEncodeTiled from the driver the runtime has loaded, looked up
+// once: the library itself does not link libcuda, so it loads (and answers
+// its non-device calls) on hosts without a driver
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                         &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return (EncodeTiledFn)p;
+  }();
+  return fn;
+}
+
 // tensor map of the FWD/DT output C[M][N] (row stride ldc floats): boxes of
 // 32 rows x 32 columns in the 128-byte swizzle
 static int c_tensor_map(CUtensorMap *m, float *C, int M, int N, int ldc) {
@@ -753,7 +773,12 @@ static int c_tensor_map(CUtensorMap *m, float *C, int M, int N, int ldc) {
   const cuuint64_t strides[1] = {(cuuint64_t)ldc * sizeof(float)};
   const cuuint32_t box[2] = {32, 32};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = cuTensorMapEncodeTiled(
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is not available from the CUDA driver");
+    return RC_DEVICE;
+  }
+  const CUresult r = enc(
       m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, estr,
       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
