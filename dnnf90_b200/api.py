@@ -44,7 +44,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_twork_set_chunk", "dnnf90_last_error", "dnnf90_device_available",
     "dnnf90_launch_count", "dnnf90_profile_enable", "dnnf90_profile_read",
     "dnnf90_ngd_step_noalloc", "dnnf90_committee_step", "dnnf90_committee_info",
-    "dnnf90_tune_report",
+    "dnnf90_tune_report", "dnnf90_tune_force", "dnnf90_tabset_free",
 ]
 
 _lib = None
@@ -83,6 +83,7 @@ def lib():
         "dnnf90_net_create_ts": [i, i, pi],
         "dnnf90_net_load": [cs],
         "dnnf90_tabset_activation": [i, i],
+        "dnnf90_tabset_free": [i],
         "dnnf90_net_load_ts": [i, cs],
         "dnnf90_net_create": [i, pi],
         "dnnf90_net_set_layer": [i, i, pd],
@@ -125,6 +126,7 @@ def lib():
         "dnnf90_committee_step": [i, pi, pi, pi, pi, p, p, p, p],
         "dnnf90_committee_info": [pi, P(ctypes.c_float)],
         "dnnf90_tune_report": [ctypes.c_char_p, i],
+        "dnnf90_tune_force": [i, i],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -183,6 +185,12 @@ def tune_report() -> list:
     return out
 
 
+def tune_force(which: int, variant: int) -> None:
+    """Pin the Bell forward (which 0) or adjoint (which 1) kernel variant;
+    variant -1 hands the choice back to the autotuner."""
+    call("dnnf90_tune_force", which, variant)
+
+
 def profile_read() -> dict:
     """{kernel name: (launches, total device ms)} since the last read,
     from CUDA events recorded on each launch's own stream."""
@@ -215,6 +223,18 @@ class TableSet:
         for ia in range(self.na):
             call("dnnf90_alpha", ia + 1, _pi(a))
             self.alpha[ia] = a
+
+    def free(self) -> None:
+        """Release the handle (networks made on the set keep their copy)."""
+        if getattr(self, "tid", 0) > 0:
+            call("dnnf90_tabset_free", self.tid)
+            self.tid = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
     def slot(self, a) -> int:
         """1-based slot of multi-index a, 0 if it is not carried."""

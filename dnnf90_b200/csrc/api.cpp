@@ -96,6 +96,7 @@ template <typename T>
 int free_slot(T *reg) {
   for (int i = 1; i <= MAXH; ++i)
     if (!reg[i].used) return i;
+  set_error("every handle of this kind is in use (" + std::to_string(MAXH) + ")");
   return -1;
 }
 
@@ -631,6 +632,14 @@ int dnnf90_tabset_closure(int d0, int k, int nseed, const int *seeds) {
 int dnnf90_tabset_nderiv(int tid) {
   if (tid < 1 || tid > MAXH || !g_tab[tid].used) return RC_BAD_ARG;
   return g_tab[tid].ts.na;
+}
+
+int dnnf90_tabset_free(int tid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (tid < 1 || tid > MAXH || !g_tab[tid].used) return RC_BAD_ARG;
+  g_tab[tid].ts = TableSet();  // networks keep their own copy of the set
+  g_tab[tid].used = false;
+  return RC_OK;
 }
 
 int dnnf90_tabset_activation(int tid, int iact) {
@@ -1461,6 +1470,12 @@ int dnnf90_tune_report(char *buf, int len) {
     buf[len - 1] = 0;
   }
   return (int)pending.size();
+}
+
+int dnnf90_tune_force(int which, int variant) {
+  const int rc = tune_force(which, variant);
+  if (rc) set_error("dnnf90_tune_force: which must be 0 or 1, variant -1..7");
+  return rc;
 }
 
 int dnnf90_committee_info(int *policy, float *graph_ms) {

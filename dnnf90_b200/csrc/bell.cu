@@ -34,6 +34,11 @@ namespace dnnf90 {
   } while (0)
 
 void DevBellPlan::release() {
+  {
+    void *q[] = {f8.list, f8.hdr, f8.cpdst, f8.rec};
+    for (void *p : q)
+      if (p) cudaFree(p);
+  }
   for (auto &D : a7) {
     void *q[] = {D.list, D.unit, D.out, D.fin, D.glist, D.rec};
     for (void *p : q)
@@ -132,6 +137,22 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
     D.nfin = (int)Q.fin.size() / 2;
     D.nscratch = Q.nscratch;
     D.ok = Q.ok;
+  }
+  {
+    const F8Plan &F = P.f8;
+    if ((rc = put(&d.f8.list, F.list))) return rc;
+    if ((rc = put(&d.f8.hdr, F.hdr))) return rc;
+    if ((rc = put(&d.f8.cpdst, F.cpdst))) return rc;
+    if ((rc = put(&d.f8.rec, F.rec))) return rc;
+    d.f8.nrec = (int)F.rec.size();
+    d.f8.sbase1 = F.sbase1;
+    d.f8.bbase = F.bbase;
+    d.f8.uvbase = F.uvbase;
+    d.f8.dtbase = F.dtbase;
+    d.f8.recbase = F.recbase;
+    d.f8.zuv = F.zuv;
+    d.f8.smem = F.smem;
+    d.f8.ok = F.ok;
   }
   d.f5_ok = P.f5_ok;
   d.nrows5 = P.nrows5;
@@ -585,6 +606,226 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd5(Fwd5Args a) {
   cp_async_wait<0>();
 }
 
+// ---------------------------------------------------------------- v8
+struct Fwd8Args {
+  int n, na, npts, iact, gy, nrec;
+  uint32_t sbase1, bbase, uvbase, dtbase, recbase, zuv;
+  const double *tpc;
+  const int *list;     // [(K+1) * workers][2]
+  const int4 *hdr;     // [*][2]
+  const uint32_t *rec;
+  const int *cpdst;    // [na]
+  const void *sc;      // [0, na): a!, [na, 2na): 1/a!
+  const void *S;
+  void *T, *h;
+};
+
+// one band of records whose g has degree D: acc[q] += S~_b B~_{g,q-1},
+// q = 2..D+1 (B~_{g,1} = S~_g).  lx: this lane in the S buffer; lz: this
+// lane in the region of g's rows.
+template <typename R, int D, int NA>
+__device__ __forceinline__ void band8(unsigned char *sm, uint32_t lx, uint32_t lz,
+                                      const uint32_t *rp, int cnt, R (&acc)[NA]) {
+#pragma unroll 4
+  for (int e = 0; e < cnt; ++e) {
+    const uint32_t r = rp[e];
+    const R x = srow<R>(sm, lx + (r >> 16));
+    const uint32_t z = lz + (r & 0xffffu);
+#pragma unroll
+    for (int l = 0; l < D; ++l) acc[2 + l] += x * srow<R>(sm, z + l * 128);
+  }
+}
+
+// the bands of one target, D = DD down to 1
+template <typename R, int DD, int NA>
+struct Bands8 {
+  static __device__ __forceinline__ void run(unsigned char *sm, uint32_t lx, uint32_t lb,
+                                             const uint32_t *rp, uint64_t bands, R (&acc)[NA]) {
+    const int cnt = (int)((bands >> (8 * (DD - 1))) & 0xffu);
+    band8<R, DD, NA>(sm, lx, DD == 1 ? lx : lb, rp, cnt, acc);
+    Bands8<R, DD - 1, NA>::run(sm, lx, lb, rp + cnt, bands, acc);
+  }
+};
+template <typename R, int NA>
+struct Bands8<R, 0, NA> {
+  static __device__ __forceinline__ void run(unsigned char *, uint32_t, uint32_t,
+                                             const uint32_t *, uint64_t, R (&)[NA]) {}
+};
+
+// what the targets of one item share
+template <typename R, int KK>
+struct Item8 {
+  unsigned char *sm;
+  const uint32_t *rs;  // records in shared memory
+  uint32_t lo, lx;     // this lane's column; the same in the current S buffer
+  R *T, *H;            // this point's planes, offset by this lane's neuron
+  bool act;
+  R dt[KK + 2], uc[KK + 1], vc[KK + 1];
+};
+
+// the targets of degree P this warp owns
+template <typename R, int KK, int P, int NPB, bool TRAIN>
+__device__ __forceinline__ void fwd8_degree(const Fwd8Args &a, const Item8<R, KK> &c, int warp) {
+  const int ts = __ldg(a.list + (P * BELL_WORKERS + warp) * 2);
+  const int tn = __ldg(a.list + (P * BELL_WORKERS + warp) * 2 + 1);
+  const R *sc = (const R *)a.sc;
+  const bool wr = NPB == 32 || (threadIdx.x & 31) < NPB;  // lanes that own a column
+  for (int t = ts; t < ts + tn; ++t) {
+    const int4 h0 = __ldg(a.hdr + 2 * t), h1 = __ldg(a.hdr + 2 * t + 1);
+    const int ia = h0.x;
+    const R sa = srow<R>(c.sm, c.lx + ia * 128);
+    const R fa = __ldg(sc + ia);
+    R tt = c.dt[1] * sa, hh = c.dt[2] * sa;
+    if constexpr (P == KK) {
+      // T_a = a! (s' S~_a + sum_b S~_b U~_{a-b}), h_a likewise with s'', V~;
+      // four records per 16-byte load
+      const uint4 *rq = (const uint4 *)(c.rs + h0.y);
+      const uint32_t lz = a.uvbase + c.lo;
+      const int m = h0.z >> 2;
+      auto top = [&](uint32_t r) {
+        const R x = srow<R>(c.sm, c.lx + (r >> 16));
+        const uint32_t z = lz + (r & 0xffffu);
+        tt += x * srow<R>(c.sm, z);
+        hh += x * srow<R>(c.sm, z + 128);
+      };
+      for (int e = 0; e < m; ++e) {
+        const uint4 g4 = rq[e];
+        top(g4.x);
+        top(g4.y);
+        top(g4.z);
+        top(g4.w);
+      }
+    } else {
+      R uu = c.uc[1] * sa, vv = c.vc[1] * sa;
+      if constexpr (P >= 2) {
+        R acc[P + 1];
+#pragma unroll
+        for (int q = 0; q <= P; ++q) acc[q] = (R)0;
+        const uint64_t bands = (uint64_t)(uint32_t)h1.z << 32 | (uint32_t)h1.y;
+        Bands8<R, P - 1, P + 1>::run(c.sm, c.lx, a.bbase + c.lo, c.rs + h0.y, bands, acc);
+#pragma unroll
+        for (int q = 2; q <= P; ++q) {
+          const R b = acc[q] * (R)(1.0 / q);
+          if (P <= KK - 2 && wr) srow<R>(c.sm, a.bbase + c.lo + h0.w + (q - 1) * 128) = b;
+          tt += c.dt[q] * b;
+          hh += c.dt[q + 1] * b;
+          uu += c.uc[q] * b;
+          vv += c.vc[q] * b;
+        }
+      }
+      if (wr) {
+        srow<R>(c.sm, a.uvbase + c.lo + h1.x) = uu;
+        srow<R>(c.sm, a.uvbase + c.lo + h1.x + 128) = vv;
+      }
+    }
+    if (c.act) {
+      c.T[(size_t)ia * a.n] = fa * tt;
+      if (TRAIN) c.H[(size_t)ia * a.n] = fa * hh;
+    }
+  }
+}
+
+// Bell forward v8: the v5 recurrences (see k_bell_fwd5) over the F8Plan
+// layout.  Every degree is its own code path with its bands unrolled, the
+// records are read from shared memory as they are used, and the sigma
+// derivatives are formed while the other warps normalise S.
+template <typename R, int KK, int NPB, bool TRAIN>
+__global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd8(Fwd8Args a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char *sm = smem_raw;
+  {
+    uint4 *rs = (uint4 *)(sm + a.recbase);
+    for (int i = threadIdx.x; i < a.nrec / 4; i += blockDim.x) rs[i] = __ldg((const uint4 *)a.rec + i);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool lact = lane < NPB;
+  const int ln = lact ? lane : 0;
+  const int n = a.n, na = a.na;
+  const size_t plane = (size_t)na * n;
+  const R *sc = (const R *)a.sc;
+  // zero rows: row na of both S buffers and the zero U/V pair
+  if (threadIdx.x < 8) {
+    *(uint4 *)(sm + na * 128 + threadIdx.x * 16) = make_uint4(0, 0, 0, 0);
+    *(uint4 *)(sm + a.sbase1 + na * 128 + threadIdx.x * 16) = make_uint4(0, 0, 0, 0);
+  } else if (threadIdx.x < 24) {
+    *(uint4 *)(sm + a.uvbase + a.zuv + (threadIdx.x - 8) * 16) = make_uint4(0, 0, 0, 0);
+  }
+  Item8<R, KK> c;
+  c.sm = sm;
+  c.rs = (const uint32_t *)(sm + a.recbase);
+  c.lo = ln * sizeof(R);
+  const long nitem = (long)a.npts * a.gy;
+  const long it0 = (long)blockIdx.x * nitem / gridDim.x;
+  const long it1 = (long)(blockIdx.x + 1) * nitem / gridDim.x;
+  if (it0 < it1)
+    stage_rows<NPB, R>(sm, (const R *)a.S + (it0 % a.npts) * plane, na, n,
+                       (int)(it0 / a.npts) * NPB, BELL_WORKERS * 32);
+  cp_async_commit();
+  int buf = 0;
+  for (long it = it0; it < it1; ++it) {
+    const int pt = (int)(it % a.npts);
+    const int j = (int)(it / a.npts) * NPB + ln;
+    c.act = lact && j < n;
+    if (it + 1 < it1)
+      stage_rows<NPB, R>(sm + (buf ? 0 : a.sbase1), (const R *)a.S + ((it + 1) % a.npts) * plane,
+                         na, n, (int)((it + 1) / a.npts) * NPB, BELL_WORKERS * 32);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    c.lx = (buf ? a.sbase1 : 0) + c.lo;
+    c.T = (R *)a.T + pt * plane + j;
+    c.H = TRAIN ? (R *)a.h + pt * plane + j : nullptr;
+    if (warp == 0 && lact) {
+      // S_0 is its own scaled value (0! = 1): sigma^(q)(S_0) into the sigma rows
+      double d[KK + 2];
+      sigma_derivs(a.iact, a.tpc, KK, (double)srow<R>(sm, c.lx), d);
+#pragma unroll
+      for (int q = 0; q <= KK + 1; ++q) srow<R>(sm, a.dtbase + c.lo + q * 128) = (R)d[q];
+      if (c.act) {
+        c.T[0] = (R)d[0];
+        if (TRAIN) c.H[0] = (R)d[1];
+      }
+    }
+    // S_b -> S_b / b!, and the level-1 copy of each B run
+    for (int ia = warp; ia < na; ia += BELL_WORKERS) {
+      if (ia == 0) continue;
+      const int cd = __ldg(a.cpdst + ia);
+      if (lact) {
+        const R v = srow<R>(sm, c.lx + ia * 128) * __ldg(sc + na + ia);
+        srow<R>(sm, c.lx + ia * 128) = v;
+        if (cd >= 0) srow<R>(sm, a.bbase + c.lo + cd) = v;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q <= KK + 1; ++q) c.dt[q] = srow<R>(sm, a.dtbase + c.lo + q * 128);
+#pragma unroll
+    for (int q = 1; q < KK; ++q) {
+      c.uc[q] = c.dt[q + 1] * (R)(1.0 / (q + 1));
+      c.vc[q] = c.dt[q + 2] * (R)(1.0 / (q + 1));
+    }
+#pragma unroll
+    for (int p = 1; p <= 8; ++p) {
+      if (p <= KK) {
+        switch (p) {
+          case 1: fwd8_degree<R, KK, 1, NPB, TRAIN>(a, c, warp); break;
+          case 2: if constexpr (KK >= 2) fwd8_degree<R, KK, 2, NPB, TRAIN>(a, c, warp); break;
+          case 3: if constexpr (KK >= 3) fwd8_degree<R, KK, 3, NPB, TRAIN>(a, c, warp); break;
+          case 4: if constexpr (KK >= 4) fwd8_degree<R, KK, 4, NPB, TRAIN>(a, c, warp); break;
+          case 5: if constexpr (KK >= 5) fwd8_degree<R, KK, 5, NPB, TRAIN>(a, c, warp); break;
+          case 6: if constexpr (KK >= 6) fwd8_degree<R, KK, 6, NPB, TRAIN>(a, c, warp); break;
+          case 7: if constexpr (KK >= 7) fwd8_degree<R, KK, 7, NPB, TRAIN>(a, c, warp); break;
+          case 8: if constexpr (KK >= 8) fwd8_degree<R, KK, 8, NPB, TRAIN>(a, c, warp); break;
+          default: break;
+        }
+        __syncthreads();
+      }
+    }
+    buf ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
 struct Adj5Args {
   int n, na, npts, gstride, gy;
   int norec, npair;    // counts copied to shared memory (SREC)
@@ -989,9 +1230,22 @@ std::string tune_report() {
   return out;
 }
 
+// variants pinned by the caller: [0] forward, [1] adjoint; -1 = autotune
+static std::atomic<int> g_force[2] = {{-1}, {-1}};
+
+int tune_force(int which, int variant) {
+  if (which < 0 || which > 1 || variant < -1 || variant > 7) return RC_BAD_ARG;
+  g_force[which] = variant;
+  return RC_OK;
+}
+
 template <typename L>
 static int tuned_launch(const TuneKey &key, int nvar, int dflt, long items, cudaStream_t st,
                         L launch) {
+  {
+    const int f = g_force[key.which == 2 ? 1 : 0];
+    if (f >= 0) return launch(f < nvar ? f : dflt, true);
+  }
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
@@ -1052,9 +1306,25 @@ static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
   a.rec = (const uint2 *)bp.f5_rec; a.rec32 = bp.f6_rec; a.cpdst = bp.f5_cpdst;
   a.sc = sizeof(R) == 8 ? (const void *)bp.sc64 : (const void *)bp.sc32;
   a.S = S; a.T = T; a.h = h;
-  // variant 0: records in global memory; 1: records in shared memory
+  // variant 0: records in global memory; 1: records in shared memory;
+  // 2: v8 (lean per-degree loops over 16-bit offset records)
   const bool srec_fits = smem + (size_t)bp.nrec32 * 4 <= 227 * 1024;
+  const bool v8_ok = bp.f8.ok && bp.f8.smem <= 227 * 1024;
   auto launch = [&](int v, bool) -> int {
+    if (v == 2) {
+      Fwd8Args b;
+      b.n = n; b.na = t.na; b.npts = npts; b.iact = t.iact; b.gy = a.gy; b.nrec = bp.f8.nrec;
+      b.sbase1 = bp.f8.sbase1; b.bbase = bp.f8.bbase; b.uvbase = bp.f8.uvbase;
+      b.dtbase = bp.f8.dtbase; b.recbase = bp.f8.recbase; b.zuv = bp.f8.zuv;
+      b.tpc = t.tpc; b.list = bp.f8.list; b.hdr = (const int4 *)bp.f8.hdr; b.rec = bp.f8.rec;
+      b.cpdst = bp.f8.cpdst; b.sc = a.sc; b.S = S; b.T = T; b.h = h;
+      auto k = train ? k_bell_fwd8<R, KK, NPB, true> : k_bell_fwd8<R, KK, NPB, false>;
+      CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bp.f8.smem));
+      const int grid = persistent_grid((const void *)k, BELL_WORKERS * 32, bp.f8.smem, (long)npts * a.gy);
+      LAUNCH("k_bell_fwd", st, k<<<grid, BELL_WORKERS * 32, bp.f8.smem, st>>>(b));
+      CKB(cudaGetLastError());
+      return RC_OK;
+    }
     const bool srec = v == 1;
     const size_t sm = smem + (srec ? (size_t)bp.nrec32 * 4 : 0);
     auto k = srec ? (train ? k_bell_fwd5<R, KK, NPB, true, true> : k_bell_fwd5<R, KK, NPB, false, true>)
@@ -1065,8 +1335,12 @@ static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
     CKB(cudaGetLastError());
     return RC_OK;
   };
-  return tuned_launch(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)}, srec_fits ? 2 : 1,
-                      srec_fits ? 1 : 0, (long)npts * a.gy, st, launch);
+  if (v8_ok && !srec_fits)  // variants 0 and 2 only: v8 takes the place of 1
+    return tuned_launch(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)}, 2, 1,
+                        (long)npts * a.gy, st, [&](int v, bool last) { return launch(v ? 2 : 0, last); });
+  return tuned_launch(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)},
+                      v8_ok ? 3 : srec_fits ? 2 : 1, v8_ok ? 2 : srec_fits ? 1 : 0,
+                      (long)npts * a.gy, st, launch);
 }
 
 template <typename R, int KK>

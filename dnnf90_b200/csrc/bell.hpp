@@ -48,6 +48,14 @@ struct DevBellPlan {
     int nunit = 0, nout = 0, nglist = 0, nrec = 0, nfin = 0, nscratch = 0;
     bool ok = false;
   } a7[2];
+  // v8 forward (F8Plan)
+  struct F8Dev {
+    int *list = nullptr, *hdr = nullptr, *cpdst = nullptr;
+    uint32_t *rec = nullptr;
+    int nrec = 0, sbase1 = 0, bbase = 0, uvbase = 0, dtbase = 0, recbase = 0, zuv = 0;
+    int smem = 0;
+    bool ok = false;
+  } f8;
   double *sc64 = nullptr;  // [3][na]: a!, 1/a!, 1/a! (Tb, h, Sb scales)
   float *sc32 = nullptr;
   void release();
@@ -57,6 +65,9 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d);
 
 // the autotuner's choices: "kernel width precision variant ms..." lines
 std::string tune_report();
+// pin the variant of the Bell forward (which 0) or adjoint (which 1) kernels;
+// variant -1 returns them to the autotuner
+int tune_force(int which, int variant);
 
 // RC_UNSUPPORTED when the set does not fit (K > 8 or the per-point state
 // exceeds shared memory): the caller then uses the generic kernels.

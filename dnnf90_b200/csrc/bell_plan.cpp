@@ -142,6 +142,100 @@ static A7Plan build_a7(const TableSet &t, int aj_workers, int nkmax) {
   return P;
 }
 
+// the v8 forward plan (see F8Plan)
+static F8Plan build_f8(const TableSet &t, int workers) {
+  F8Plan P;
+  const int na = t.na, k = t.k, ROW = 128;
+  P.srows = na + 1;
+  std::vector<int> b1(na, -1), uv(na, -1);
+  int brow = 0, uvrow = 0;
+  for (int ia = 1; ia < na; ++ia)
+    if (t.deg[ia] >= 2 && t.deg[ia] <= k - 2) {
+      b1[ia] = brow * ROW;
+      brow += t.deg[ia];
+    }
+  for (int ia = 1; ia < na; ++ia)
+    if (t.deg[ia] <= k - 1) {
+      uv[ia] = uvrow * ROW;
+      uvrow += 2;
+    }
+  P.zuv = uvrow * ROW;
+  uvrow += 2;
+  P.sbase1 = P.srows * ROW;
+  P.bbase = 2 * P.srows * ROW;
+  P.uvbase = P.bbase + brow * ROW;
+  P.dtbase = P.uvbase + uvrow * ROW;
+  P.recbase = P.dtbase + (k + 2) * ROW;
+  P.cpdst = b1;
+  // every record field is a 16-bit byte offset inside its region
+  bool ok = k <= 8 && (long)P.srows * ROW <= 65536 && (long)brow * ROW <= 65536 &&
+            (long)uvrow * ROW <= 65536;
+  const uint32_t zrec = ((uint32_t)(na * ROW) << 16) | (uint32_t)P.zuv;
+  P.list.assign((size_t)(k + 1) * workers * 2, 0);
+  for (int p = 1; p <= k && ok; ++p) {
+    std::vector<int> items;
+    std::vector<long> cost;
+    for (int ia = 1; ia < na; ++ia)
+      if (t.deg[ia] == p) {
+        items.push_back(ia);
+        long c = 24;
+        const int st = p >= 2 ? t.fq_at(ia, 2) : 0, nn = p >= 2 ? t.fq_len(ia, 2) : 0;
+        for (int i = st; i < st + nn; ++i) c += p == k ? 9 : 6 + 2 * t.deg[t.fq_id[i]];
+        cost.push_back(c);
+      }
+    auto asg = balance(cost, workers);
+    for (int w = 0; w < workers; ++w) {
+      P.list[((size_t)p * workers + w) * 2] = (int)P.hdr.size() / 8;
+      P.list[((size_t)p * workers + w) * 2 + 1] = (int)asg[w].size();
+      for (int it : asg[w]) {
+        const int ia = items[it];
+        if (p == k)
+          while (P.rec.size() % 4) P.rec.push_back(zrec);
+        const int rstart = (int)P.rec.size();
+        int cnt[9] = {0};
+        if (p >= 2) {
+          const int st = t.fq_at(ia, 2), nn = t.fq_len(ia, 2);
+          std::vector<int> idx;
+          for (int i = st; i < st + nn; ++i) idx.push_back(i);
+          if (p < k)  // bands of |g| = D, longest first, slot order inside
+            std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+              return t.deg[t.fq_id[a]] > t.deg[t.fq_id[b]];
+            });
+          for (int i : idx) {
+            const int ib = t.fq_ib[i], g = t.fq_id[i];
+            const int z = p == k ? uv[g] : (t.deg[g] >= 2 ? b1[g] : g * ROW);
+            P.rec.push_back(((uint32_t)(ib * ROW) << 16) | (uint32_t)z);
+            if (p < k) cnt[t.deg[g]]++;
+          }
+        }
+        if (p == k)
+          while ((P.rec.size() - rstart) % 4) P.rec.push_back(zrec);
+        uint32_t blo = 0, bhi = 0;
+        for (int d = 1; d <= 8; ++d) {
+          if (cnt[d] > 255) ok = false;
+          if (d <= 4)
+            blo |= (uint32_t)(cnt[d] & 0xff) << (8 * (d - 1));
+          else
+            bhi |= (uint32_t)(cnt[d] & 0xff) << (8 * (d - 5));
+        }
+        P.hdr.push_back(ia);
+        P.hdr.push_back(rstart);
+        P.hdr.push_back((int)P.rec.size() - rstart);
+        P.hdr.push_back(p <= k - 2 ? b1[ia] : -1);
+        P.hdr.push_back(p <= k - 1 ? uv[ia] : -1);
+        P.hdr.push_back((int)blo);
+        P.hdr.push_back((int)bhi);
+        P.hdr.push_back(0);
+      }
+    }
+  }
+  for (int i = 0; i < 4; ++i) P.rec.push_back(0);
+  while (P.rec.size() % 4) P.rec.push_back(0);  // whole 16-byte pieces
+  P.smem = P.recbase + (int)P.rec.size() * 4;
+  P.ok = ok && P.smem <= 227 * 1024;
+  return P;
+}
+
 BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
   BellPlan P;
   P.workers = workers;
@@ -406,6 +500,7 @@ BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
 
   P.a7f = build_a7(t, aj_workers, 16);
   P.a7d = build_a7(t, aj_workers, 8);
+  P.f8 = build_f8(t, workers);
 
   // adjoint outputs: Sb_0 (pairs (a, a) for every a) and every Sb_b, b >= 1
   std::vector<long> cost;

@@ -37,8 +37,30 @@ struct A7Plan {
   bool ok = false;
 };
 
+// Forward v8: the v5 recurrences with one 32-bit record per (b, g) pair,
+//   x << 16 | z,
+// x the byte offset of the S_b/b! row inside the current S buffer and z the
+// byte offset of g's first row inside its region: the S buffer for |g| = 1,
+// the B region for 2 <= |g| <= K-2 (levels 1..|g| of B_{g,q}/g!, level 1 a
+// copy of S_g/g!), the U/V region on the top degree (U_g/g!, then V_g/g!).
+// Shared memory: two S buffers of na + 1 rows (row na stays zero), the B
+// region, the U/V region (with a zero pair), K+2 sigma rows, the records.
+struct F8Plan {
+  std::vector<int> list;       // [(k+1) * workers][2]: first target, count
+  std::vector<int> hdr;        // [*][8]: ia, rstart, nrec, B run of a (or -1),
+                               //   U/V pair of a (or -1), bands D=1..4, D=5..8, 0
+  std::vector<uint32_t> rec;   // records; top-degree lists 4-aligned, padded
+                               //   with (zero S row, zero U/V pair)
+  std::vector<int> cpdst;      // [na]: B-region offset of the level-1 copy, or -1
+  int srows = 0, sbase1 = 0, bbase = 0, uvbase = 0, dtbase = 0, recbase = 0;
+  int zuv = 0;                 // U/V-region offset of the zero pair
+  int smem = 0;                // bytes of shared memory
+  bool ok = false;
+};
+
 struct BellPlan {
   int workers = 0, k = 0, na = 0, nslot = 0;
+  F8Plan f8;
   // forward
   std::vector<int> fw_list;   // [(k+1) * workers][2]: start, count into fw_arec
   std::vector<int> fw_arec;   // [*][4]: ia | p << 16, gstart, gcount, bbase

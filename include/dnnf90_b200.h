@@ -24,6 +24,10 @@ extern "C" {
  * products with FP32 accumulation on the tensor cores, FP64 gradient
  * reductions.  New; the reference is FP64 only. */
 int dnnf90_net_set_precision(int nid, int prec);
+/* release a table-set handle (the reference keeps every set until exit;
+ * there are 64 handles).  Networks created on the set keep working: each
+ * holds its own copy.  new */
+int dnnf90_tabset_free(int tid);
 /* number of weights of a network (flat layout); new */
 int dnnf90_nweights(int nid);
 /* read layer l back in the dnnf90_net_set_layer row layout; new */
@@ -116,6 +120,13 @@ int dnnf90_committee_step(int nnet, const int *nids, const int *tids, const int 
  * width precision chosen-variant ms-of-each-variant"; returns the length
  * (buf may be NULL); new */
 int dnnf90_tune_report(char *buf, int len);
+/* pin the variant of the Bell forward (which 0: 0 records in global memory,
+ * 1 records in shared memory, 2 per-degree loops over 16-bit offset records)
+ * or adjoint (which 1: 0 pairs in global memory, 1 in shared memory,
+ * 2 grouped correlation) kernels for every later launch; variant -1 hands
+ * the choice back to the autotuner, and a variant a launch shape cannot use
+ * runs its default.  For reproducible timing and for tests; new */
+int dnnf90_tune_force(int which, int variant);
 /* policy (0 work, 1 square root, 2 none) and timed replay ms of the graph
  * the last committee step used; new */
 int dnnf90_committee_info(int *policy, float *graph_ms);

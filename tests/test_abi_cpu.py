@@ -158,3 +158,17 @@ def test_no_device_fails_loudly():
         g.point(np.zeros(2), np.zeros(ts.na))
     g.free()
     net.free()
+
+
+def test_tabset_free_releases_the_handle():
+    L = api.lib()
+    ids = [L.dnnf90_tabset_dense(2, 2) for _ in range(3)]
+    assert all(i > 0 for i in ids)
+    assert L.dnnf90_tabset_free(ids[1]) == 0
+    assert L.dnnf90_tabset_free(ids[1]) == -1       # already released
+    assert L.dnnf90_tabset_nderiv(ids[1]) == -1
+    again = L.dnnf90_tabset_dense(2, 2)
+    assert 0 < again <= ids[1]                        # handles are reused lowest first
+    for i in (ids[0], ids[2], again):
+        assert L.dnnf90_tabset_free(i) == 0
+    assert L.dnnf90_tabset_free(0) == -1 and L.dnnf90_tabset_free(65) == -1
