@@ -333,15 +333,18 @@ def main():
         red = ReducedStep(net.nw, dev)  # dL/dw and the loss, summed over ranks
 
         def local(g, loss):
+            # the current stream: the bench stream, or the capture stream of a graph
             api.call("dnnf90_grad_rule_dev", net.nid, net.tid, npts, X.data_ptr(), rule.rid,
-                     g.data_ptr(), loss.data_ptr(), None, st)
+                     g.data_ptr(), loss.data_ptr(), None,
+                     torch.cuda.current_stream(dev).cuda_stream)
 
         return net, red, local
 
     def step(net, red, local):
         red.step(local)
 
-    def timed(net, g, loss, nsteps, clocks=False, profile=False, warmup=None, settle=True):
+    def timed(net, g, loss, nsteps, clocks=False, profile=False, warmup=None, settle=True,
+              use_graph=True):
         # the clock sampler starts before the warm-up and has produced a
         # sample before the timed region, so its start-up stays outside it
         ck = Clocks(local)
@@ -377,6 +380,20 @@ def main():
             ck.wait_first()
         if ws > 1:
             dist.barrier()
+        # one GPU: the step is captured once into a CUDA graph and replayed,
+        # so that the device never waits on the host between steps (the
+        # library's entries wait for their stream and read the GEMM time-out
+        # flag only outside a capture; the flag is sticky, and the profiled
+        # pass below, made of plain calls, reads it).  Several GPUs: plain
+        # calls, the all-reduce between them.
+        gph, per_graph = None, 0
+        if use_graph and ws == 1:
+            gph = torch.cuda.CUDAGraph()
+            c0 = api.launch_count()
+            with torch.cuda.graph(gph):
+                step(net, g, loss)
+            per_graph = api.launch_count() - c0  # the library's kernels in one replay
+            torch.cuda.synchronize(dev)
         n0 = api.launch_count()
         if profile:
             api.profile_read()
@@ -386,9 +403,14 @@ def main():
             ck.mark()
         ev[0].record(stream)
         for i in range(nsteps):
-            step(net, g, loss)
+            if gph is not None:
+                gph.replay()
+            else:
+                step(net, g, loss)
             ev[i + 1].record(stream)
         torch.cuda.synchronize(dev)
+        gph_used = gph is not None
+        del gph
         e0, e1 = ev[0], ev[-1]
         each = [round(ev[i].elapsed_time(ev[i + 1]), 3) for i in range(nsteps)]
         if clocks:
@@ -400,7 +422,7 @@ def main():
             api.profile_enable(False)
             prof = api.profile_read()
         ms = e0.elapsed_time(e1) / nsteps
-        launches = api.launch_count() - n0
+        launches = api.launch_count() - n0 + (per_graph * nsteps if gph_used else 0)
         if ws > 1:
             t = torch.tensor([ms], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -416,7 +438,8 @@ def main():
     value = ws * npts / (ms / 1000.0)
     # per-kernel device times from a separate pass: every launch bracketed
     # by CUDA events on its own stream (kept out of the timed region above)
-    _, _, prof, _, _ = timed(net, g, loss, args.prof_steps, profile=True, warmup=0, settle=False)
+    _, _, prof, _, _ = timed(net, g, loss, args.prof_steps, profile=True, warmup=0, settle=False,
+                             use_graph=False)
 
     # ---- dominant kernel and its roofline
     hbm, tc, peak_kind = peaks()
@@ -464,7 +487,7 @@ def main():
     net64, g64, loss64 = make(api.PREC_F64)
     ms64, _, _, _, each64 = timed(net64, g64, loss64, args.f64_steps, warmup=1)
     _, _, prof64, _, _ = timed(net64, g64, loss64, args.prof_steps, profile=True, warmup=0,
-                               settle=False)
+                               settle=False, use_graph=False)
     value64 = ws * npts / (ms64 / 1000.0)
     net64.free()
 
@@ -530,7 +553,9 @@ def main():
                        "parallelism": f"dp{ws}: points sharded, dL/dw all-reduced (NCCL)",
                        "l2": "inputs larger than L2 (126 MB): a work chunk's planes are ~48 GB, so no flush",
                        "hbm_free_gib_at_start": round(hbm_free0, 1),
-                       "launches_per_step": launches / max(args.steps, 1)},
+                       "launches_per_step": launches / max(args.steps, 1),
+                       "timing": ("one step captured as a CUDA graph, replayed per timed step"
+                                  if ws == 1 else "plain calls per step")},
             "f64": {"value": value64, "unit": "pts/s", "ms_per_step": ms64,
                     "step_ms_each": each64[0], "settle_steps": each64[1], "steps": args.f64_steps, "split_speedup": value / value64,
                     "kernel_ms_per_step": per_step_ms(prof64)},

@@ -620,6 +620,35 @@ struct Fwd8Args {
   void *T, *h;
 };
 
+// the (U, V) pair of one lane: two adjacent values of a 256-byte row
+template <typename R>
+struct Pair;
+template <>
+struct Pair<float> {
+  using T = float2;
+};
+template <>
+struct Pair<double> {
+  using T = double2;
+};
+
+// (t, h) += x * (u, v) as one packed FP32 multiply-add; the register pairs
+// are formed inside the asm so that no value is moved through integer ops
+__device__ __forceinline__ void fma_pair(float2 &th, float x, float2 uv) {
+  asm("{\n\t.reg .b64 acc, xx, u;\n\t"
+      "mov.b64 acc, {%0, %1};\n\t"
+      "mov.b64 xx, {%2, %2};\n\t"
+      "mov.b64 u, {%3, %4};\n\t"
+      "fma.rn.f32x2 acc, xx, u, acc;\n\t"
+      "mov.b64 {%0, %1}, acc;\n\t}"
+      : "+f"(th.x), "+f"(th.y)
+      : "f"(x), "f"(uv.x), "f"(uv.y));
+}
+__device__ __forceinline__ void fma_pair(double2 &th, double x, double2 uv) {
+  th.x += x * uv.x;
+  th.y += x * uv.y;
+}
+
 // one band of records whose g has degree D: acc[q] += S~_b B~_{g,q-1},
 // q = 2..D+1 (B~_{g,1} = S~_g).  lx: this lane in the S buffer; lz: this
 // lane in the region of g's rows.
@@ -630,7 +659,7 @@ __device__ __forceinline__ void band8(unsigned char *sm, uint32_t lx, uint32_t l
   for (int e = 0; e < cnt; ++e) {
     const uint32_t r = rp[e];
     const R x = srow<R>(sm, lx + (r >> 16));
-    const uint32_t z = lz + (r & 0xffffu);
+    const uint32_t z = lz + (r & 0xffffu) * 4;
 #pragma unroll
     for (int l = 0; l < D; ++l) acc[2 + l] += x * srow<R>(sm, z + l * 128);
   }
@@ -659,6 +688,7 @@ struct Item8 {
   const uint32_t *rs;  // records in shared memory
   uint32_t lo, lx;     // this lane's column; the same in the current S buffer
   R *T, *H;            // this point's planes, offset by this lane's neuron
+  uint32_t lp;         // this lane's (U, V) pair inside a 256-byte pair row
   bool act;
   R dt[KK + 2], uc[KK + 1], vc[KK + 1];
 };
@@ -678,15 +708,17 @@ __device__ __forceinline__ void fwd8_degree(const Fwd8Args &a, const Item8<R, KK
     R tt = c.dt[1] * sa, hh = c.dt[2] * sa;
     if constexpr (P == KK) {
       // T_a = a! (s' S~_a + sum_b S~_b U~_{a-b}), h_a likewise with s'', V~;
-      // four records per 16-byte load
+      // four records per 16-byte load, one load per (U, V) pair
+      using PR = typename Pair<R>::T;
       const uint4 *rq = (const uint4 *)(c.rs + h0.y);
-      const uint32_t lz = a.uvbase + c.lo;
+      const uint32_t lz = a.uvbase + c.lp;
       const int m = h0.z >> 2;
+      PR th;
+      th.x = tt;
+      th.y = hh;
       auto top = [&](uint32_t r) {
         const R x = srow<R>(c.sm, c.lx + (r >> 16));
-        const uint32_t z = lz + (r & 0xffffu);
-        tt += x * srow<R>(c.sm, z);
-        hh += x * srow<R>(c.sm, z + 128);
+        fma_pair(th, x, srow<PR>(c.sm, lz + (r & 0xffffu) * 4));
       };
       for (int e = 0; e < m; ++e) {
         const uint4 g4 = rq[e];
@@ -695,6 +727,8 @@ __device__ __forceinline__ void fwd8_degree(const Fwd8Args &a, const Item8<R, KK
         top(g4.z);
         top(g4.w);
       }
+      tt = th.x;
+      hh = th.y;
     } else {
       R uu = c.uc[1] * sa, vv = c.vc[1] * sa;
       if constexpr (P >= 2) {
@@ -714,8 +748,10 @@ __device__ __forceinline__ void fwd8_degree(const Fwd8Args &a, const Item8<R, KK
         }
       }
       if (wr) {
-        srow<R>(c.sm, a.uvbase + c.lo + h1.x) = uu;
-        srow<R>(c.sm, a.uvbase + c.lo + h1.x + 128) = vv;
+        typename Pair<R>::T p;
+        p.x = uu;
+        p.y = vv;
+        srow<typename Pair<R>::T>(c.sm, a.uvbase + c.lp + h1.x) = p;
       }
     }
     if (c.act) {
@@ -754,6 +790,7 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd8(Fwd8Args a) {
   c.sm = sm;
   c.rs = (const uint32_t *)(sm + a.recbase);
   c.lo = ln * sizeof(R);
+  c.lp = ln * 2 * sizeof(R);
   const long nitem = (long)a.npts * a.gy;
   const long it0 = (long)blockIdx.x * nitem / gridDim.x;
   const long it1 = (long)(blockIdx.x + 1) * nitem / gridDim.x;
@@ -1475,6 +1512,163 @@ int bell_adj2(const DevBellPlan &bp, const DevTables &t, int n, int npts, const 
   if (!bp.ready) return RC_UNSUPPORTED;
   return prec == PREC_F64 ? adj2_t<double>(bp, t, n, npts, Tb, h, Sb, gbias, gstride, st)
                           : adj2_t<float>(bp, t, n, npts, Tb, h, Sb, gbias, gstride, st);
+}
+
+// ------------------------------------------------- first-layer adjoint, staged
+struct AdjL2sArgs {
+  int n, na, npts, gy;
+  const int *up;           // [na][D0]: slot of g + e_i | (g_i + 1) << 16, or -1
+  const void *Tb, *h;      // [P][na][n]
+  const double *X;         // [P][D0]
+  double *g;               // dW_2 [n][D0 + 1], accumulated (null in row mode)
+  double *rows;            // [P][nw] (row mode)
+  size_t nw, woff;
+};
+
+// The first hidden layer's Bell adjoint fused with dW_2 (the k_adj_l2v sums)
+//   Sb^0 = sum_g Tb^g h^g,  Sb^{e_i} = sum_g (g_i + 1) Tb^{g + e_i} h^g,
+//   dW_2[j][0] += Sb^0,  dW_2[j][1 + i] += Sb^0 x_i + Sb^{e_i},
+// one (point, NPB-neuron tile) at a time per block: the item's Tb and h rows
+// are staged in shared memory (the next item's copy in flight meanwhile) and
+// the 32 warps split the slots g.  dW_2 is linear in each slot's share, so
+// every warp keeps its own FP64 partial of the tile's dW_2 rows and adds it
+// in once per tile; only the per-point rows (Jacobian mode) are summed over
+// the warps per item.  Every Tb row is read from HBM once instead of D0 + 1
+// times through the caches.
+template <typename R, int D0, int NPB>
+__global__ void __launch_bounds__(1024) k_adj_l2s(AdjL2sArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char *sm = smem_raw;
+  const int na = a.na, n = a.n;
+  const uint32_t bsz = 2u * na * 128;  // one buffer: Tb rows, then h rows
+  const uint32_t upoff = 2 * bsz, redoff = upoff + ((uint32_t)na * D0 * 4 + 127) / 128 * 128;
+  uint32_t *up = (uint32_t *)(sm + upoff);
+  for (int e = threadIdx.x; e < na * D0; e += blockDim.x) up[e] = (uint32_t)__ldg(a.up + e);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool lact = lane < NPB;
+  const int ln = lact ? lane : 0;
+  const uint32_t lo = ln * sizeof(R);
+  const size_t plane = (size_t)na * n;
+  const long nitem = (long)a.npts * a.gy;
+  const long it0 = (long)blockIdx.x * nitem / gridDim.x;
+  const long it1 = (long)(blockIdx.x + 1) * nitem / gridDim.x;
+  auto stage = [&](long it, uint32_t dst) {
+    const size_t pofs = (size_t)(it % a.npts) * plane;
+    const int j0 = (int)(it / a.npts) * NPB;
+    stage_rows<NPB, R>(sm + dst, (const R *)a.Tb + pofs, na, n, j0, 1024);
+    stage_rows<NPB, R>(sm + dst + na * 128, (const R *)a.h + pofs, na, n, j0, 1024);
+  };
+  if (it0 < it1) stage(it0, 0);
+  cp_async_commit();
+  double acc[D0 + 1];
+#pragma unroll
+  for (int o = 0; o <= D0; ++o) acc[o] = 0.0;
+  int tile = it0 < it1 ? (int)(it0 / a.npts) : 0;
+  // this warp's partial of the tile's dW_2 rows
+  auto flush = [&](int tl) {
+    const int j = tl * NPB + ln;
+    if (a.g && lact && j < n) {
+      double *gr = a.g + (size_t)j * (D0 + 1);
+#pragma unroll
+      for (int o = 0; o <= D0; ++o)
+        if (acc[o] != 0.0) atomicAdd(gr + o, acc[o]);
+    }
+#pragma unroll
+    for (int o = 0; o <= D0; ++o) acc[o] = 0.0;
+  };
+  for (long it = it0; it < it1; ++it) {
+    const uint32_t buf = (uint32_t)((it - it0) & 1) * bsz;
+    cp_async_wait<0>();
+    __syncthreads();  // this item's rows are in; every warp is done with the last item
+    if (it + 1 < it1) stage(it + 1, buf ? 0 : bsz);
+    cp_async_commit();
+    const int pt = (int)(it % a.npts), tl = (int)(it / a.npts);
+    if (tl != tile) {
+      flush(tile);
+      tile = tl;
+    }
+    const uint32_t tb = buf + lo, hb = tb + na * 128;
+    R s[D0 + 1];
+#pragma unroll
+    for (int o = 0; o <= D0; ++o) s[o] = (R)0;
+    for (int g = warp; g < na; g += 32) {
+      const R hg = srow<R>(sm, hb + g * 128);
+      s[0] += srow<R>(sm, tb + g * 128) * hg;
+#pragma unroll
+      for (int i = 0; i < D0; ++i) {
+        const uint32_t u = up[g * D0 + i];
+        if ((int)u >= 0) s[1 + i] += (R)(u >> 16) * srow<R>(sm, tb + (u & 0xffffu) * 128) * hg;
+      }
+    }
+    const double *x = a.X + (size_t)pt * D0;
+    if (!a.rows) {
+      acc[0] += (double)s[0];
+#pragma unroll
+      for (int i = 0; i < D0; ++i) acc[1 + i] += (double)s[0] * __ldg(x + i) + (double)s[1 + i];
+      continue;
+    }
+    // Jacobian rows: the point's sums over the warps, in a fixed order
+    if (lact)
+#pragma unroll
+      for (int o = 0; o <= D0; ++o) srow<R>(sm, redoff + (warp * (D0 + 1) + o) * 128 + lo) = s[o];
+    __syncthreads();
+    const int j = tl * NPB + ln;
+    if (warp == 0 && lact && j < n) {
+      R v[D0 + 1];
+#pragma unroll
+      for (int o = 0; o <= D0; ++o) {
+        v[o] = (R)0;
+        for (int w = 0; w < 32; ++w) v[o] += srow<R>(sm, redoff + (w * (D0 + 1) + o) * 128 + lo);
+      }
+      double *row = a.rows + (size_t)pt * a.nw + a.woff + (size_t)j * (D0 + 1);
+      row[0] = (double)v[0];
+#pragma unroll
+      for (int i = 0; i < D0; ++i) row[1 + i] = (double)v[0] * x[i] + (double)v[1 + i];
+    }
+  }
+  cp_async_wait<0>();
+  if (it0 < it1) flush(tile);
+}
+
+template <typename R, int D0>
+static int adj_l2s_k(const AdjL2sArgs &a, cudaStream_t st) {
+  constexpr int NPB = sizeof(R) == 8 ? 16 : 32;
+  const size_t smem = 4 * (size_t)a.na * 128 + ((size_t)a.na * D0 * 4 + 127) / 128 * 128 +
+                      (size_t)32 * (D0 + 1) * 128;
+  if (smem > 227 * 1024 || a.na > 65535 || a.n % (16 / (int)sizeof(R))) return RC_UNSUPPORTED;
+  AdjL2sArgs b = a;
+  b.gy = (a.n + NPB - 1) / NPB;
+  auto k = k_adj_l2s<R, D0, NPB>;
+  CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = persistent_grid((const void *)k, 1024, smem, (long)a.npts * b.gy);
+  LAUNCH("k_bell_adj_l2", st, k<<<grid, 1024, smem, st>>>(b));
+  CKB(cudaGetLastError());
+  return RC_OK;
+}
+
+template <typename R>
+static int adj_l2s_t(int d0, const AdjL2sArgs &a, cudaStream_t st) {
+  switch (d0) {
+    case 1: return adj_l2s_k<R, 1>(a, st);
+    case 2: return adj_l2s_k<R, 2>(a, st);
+    case 3: return adj_l2s_k<R, 3>(a, st);
+    case 4: return adj_l2s_k<R, 4>(a, st);
+    case 5: return adj_l2s_k<R, 5>(a, st);
+    case 6: return adj_l2s_k<R, 6>(a, st);
+    case 7: return adj_l2s_k<R, 7>(a, st);
+    case 8: return adj_l2s_k<R, 8>(a, st);
+    default: return RC_UNSUPPORTED;
+  }
+}
+
+int bell_adj_l2s(int d0, int n, int na, int npts, const int *up, const void *Tb, const void *h,
+                 const double *X, double *g, double *rows, size_t nw, size_t woff, int prec,
+                 cudaStream_t st) {
+  if (npts <= 0) return RC_OK;
+  AdjL2sArgs a;
+  a.n = n; a.na = na; a.npts = npts; a.gy = 0; a.up = up; a.Tb = Tb; a.h = h; a.X = X;
+  a.g = g; a.rows = rows; a.nw = nw; a.woff = woff;
+  return prec == PREC_F64 ? adj_l2s_t<double>(d0, a, st) : adj_l2s_t<float>(d0, a, st);
 }
 
 }  // namespace dnnf90

@@ -76,5 +76,10 @@ int bell_fwd2(const DevBellPlan &bp, const DevTables &t, int n, int npts, const 
 int bell_adj2(const DevBellPlan &bp, const DevTables &t, int n, int npts, const void *Tb,
               const void *h, void *Sb, double *gbias, int gstride, int prec,
               cudaStream_t st);
+// the first hidden layer's adjoint fused with dW_2, staged through shared
+// memory (RC_UNSUPPORTED when an item's rows do not fit)
+int bell_adj_l2s(int d0, int n, int na, int npts, const int *up, const void *Tb, const void *h,
+                 const double *X, double *g, double *rows, size_t nw, size_t woff, int prec,
+                 cudaStream_t st);
 
 }  // namespace dnnf90

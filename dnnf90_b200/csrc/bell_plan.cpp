@@ -154,6 +154,7 @@ static F8Plan build_f8(const TableSet &t, int workers) {
       b1[ia] = brow * ROW;
       brow += t.deg[ia];
     }
+  // U/V pairs interleaved per lane: one 256-byte row per pair
   for (int ia = 1; ia < na; ++ia)
     if (t.deg[ia] <= k - 1) {
       uv[ia] = uvrow * ROW;
@@ -167,10 +168,11 @@ static F8Plan build_f8(const TableSet &t, int workers) {
   P.dtbase = P.uvbase + uvrow * ROW;
   P.recbase = P.dtbase + (k + 2) * ROW;
   P.cpdst = b1;
-  // every record field is a 16-bit byte offset inside its region
-  bool ok = k <= 8 && (long)P.srows * ROW <= 65536 && (long)brow * ROW <= 65536 &&
-            (long)uvrow * ROW <= 65536;
-  const uint32_t zrec = ((uint32_t)(na * ROW) << 16) | (uint32_t)P.zuv;
+  // x: a 16-bit byte offset in the S buffer; z: a 16-bit offset in 4-byte
+  // units inside its region
+  bool ok = k <= 8 && (long)P.srows * ROW <= 65536 && (long)brow * ROW <= 4 * 65536 &&
+            (long)uvrow * ROW <= 4 * 65536;
+  const uint32_t zrec = ((uint32_t)(na * ROW) << 16) | (uint32_t)(P.zuv / 4);
   P.list.assign((size_t)(k + 1) * workers * 2, 0);
   for (int p = 1; p <= k && ok; ++p) {
     std::vector<int> items;
@@ -204,7 +206,7 @@ static F8Plan build_f8(const TableSet &t, int workers) {
           for (int i : idx) {
             const int ib = t.fq_ib[i], g = t.fq_id[i];
             const int z = p == k ? uv[g] : (t.deg[g] >= 2 ? b1[g] : g * ROW);
-            P.rec.push_back(((uint32_t)(ib * ROW) << 16) | (uint32_t)z);
+            P.rec.push_back(((uint32_t)(ib * ROW) << 16) | (uint32_t)(z / 4));
             if (p < k) cnt[t.deg[g]]++;
           }
         }

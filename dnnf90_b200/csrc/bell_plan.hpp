@@ -38,11 +38,12 @@ struct A7Plan {
 };
 
 // Forward v8: the v5 recurrences with one 32-bit record per (b, g) pair,
-//   x << 16 | z,
+//   x << 16 | z / 4,
 // x the byte offset of the S_b/b! row inside the current S buffer and z the
 // byte offset of g's first row inside its region: the S buffer for |g| = 1,
 // the B region for 2 <= |g| <= K-2 (levels 1..|g| of B_{g,q}/g!, level 1 a
-// copy of S_g/g!), the U/V region on the top degree (U_g/g!, then V_g/g!).
+// copy of S_g/g!), the U/V region on the top degree.  A U/V pair is one
+// 256-byte row holding (U_g/g!, V_g/g!) side by side for each lane.
 // Shared memory: two S buffers of na + 1 rows (row na stays zero), the B
 // region, the U/V region (with a zero pair), K+2 sigma rows, the records.
 struct F8Plan {

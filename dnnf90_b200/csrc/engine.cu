@@ -1569,6 +1569,9 @@ static int adj_chunk(Chunk<R> &c, const double *X, const double *seed,
   a2.Tb = p.Tb; a2.h = p.h[1]; a2.X = X;
   a2.g = rows || !grad ? nullptr : grad + net.woff[1];
   a2.rows = rows; a2.nw = net.nw; a2.woff = net.woff[1];
+  rc = bell_adj_l2s(t.d0, a2.n, na, np, t.l2up, p.Tb, p.h[1], X, a2.g, rows, net.nw,
+                    net.woff[1], split ? PREC_SPLIT : PREC_F64, c.st);
+  if (rc != RC_UNSUPPORTED) return rc;
   {
     AdjL2vArgs v;
     v.n = a2.n; v.na = na; v.npts = np; v.up = t.l2up; v.Tb = p.Tb; v.h = p.h[1]; v.X = X;
