@@ -1541,9 +1541,15 @@ __global__ void __launch_bounds__(1024) k_adj_l2s(AdjL2sArgs a) {
   unsigned char *sm = smem_raw;
   const int na = a.na, n = a.n;
   const uint32_t bsz = 2u * na * 128;  // one buffer: Tb rows, then h rows
-  const uint32_t upoff = 2 * bsz, redoff = upoff + ((uint32_t)na * D0 * 4 + 127) / 128 * 128;
-  uint32_t *up = (uint32_t *)(sm + upoff);
-  for (int e = threadIdx.x; e < na * D0; e += blockDim.x) up[e] = (uint32_t)__ldg(a.up + e);
+  const uint32_t upoff = 2 * bsz, redoff = upoff + ((uint32_t)na * D0 * 8 + 127) / 128 * 128;
+  // (byte offset of the Tb row of g + e_i, multiplier g_i + 1) per (g, i);
+  // a missing child reads row 0 with multiplier 0
+  uint2 *up = (uint2 *)(sm + upoff);
+  for (int e = threadIdx.x; e < na * D0; e += blockDim.x) {
+    const int u = __ldg(a.up + e);
+    up[e] = u >= 0 ? make_uint2((uint32_t)(u & 0xffff) * 128, __float_as_uint((float)(u >> 16)))
+                   : make_uint2(0u, 0u);
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool lact = lane < NPB;
   const int ln = lact ? lane : 0;
@@ -1596,8 +1602,8 @@ __global__ void __launch_bounds__(1024) k_adj_l2s(AdjL2sArgs a) {
       s[0] += srow<R>(sm, tb + g * 128) * hg;
 #pragma unroll
       for (int i = 0; i < D0; ++i) {
-        const uint32_t u = up[g * D0 + i];
-        if ((int)u >= 0) s[1 + i] += (R)(u >> 16) * srow<R>(sm, tb + (u & 0xffffu) * 128) * hg;
+        const uint2 u = up[g * D0 + i];
+        s[1 + i] += (R)__uint_as_float(u.y) * srow<R>(sm, tb + u.x) * hg;
       }
     }
     const double *x = a.X + (size_t)pt * D0;
@@ -1633,7 +1639,7 @@ __global__ void __launch_bounds__(1024) k_adj_l2s(AdjL2sArgs a) {
 template <typename R, int D0>
 static int adj_l2s_k(const AdjL2sArgs &a, cudaStream_t st) {
   constexpr int NPB = sizeof(R) == 8 ? 16 : 32;
-  const size_t smem = 4 * (size_t)a.na * 128 + ((size_t)a.na * D0 * 4 + 127) / 128 * 128 +
+  const size_t smem = 4 * (size_t)a.na * 128 + ((size_t)a.na * D0 * 8 + 127) / 128 * 128 +
                       (size_t)32 * (D0 + 1) * 128;
   if (smem > 227 * 1024 || a.na > 65535 || a.n % (16 / (int)sizeof(R))) return RC_UNSUPPORTED;
   AdjL2sArgs b = a;

@@ -25,6 +25,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "engine.hpp"
 #include "gemm_tc.hpp"
@@ -800,9 +801,32 @@ __global__ void __launch_bounds__(256) k_adj_l2v(AdjL2vArgs a) {
     for (int i = 0; i <= D0; ++i) atomicAdd(a.g + (size_t)j * (D0 + 1) + i, acc[i]);
 }
 
+// Sum of 16 values over the 32 lanes of a warp with 16 shuffles (not 80):
+// each level hands half of the still-open rows to the partner lane.  On
+// return, lanes 2r and 2r + 1 hold the total of row r.
+__device__ __forceinline__ double warp_sum16(double (&p)[16]) {
+  const int lane = threadIdx.x & 31;
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+  double q[8], r[4], u[2];
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    q[k] = (b4 ? p[k + 8] : p[k]) + __shfl_xor_sync(0xffffffffu, b4 ? p[k] : p[k + 8], 16);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    r[k] = (b3 ? q[k + 4] : q[k]) + __shfl_xor_sync(0xffffffffu, b3 ? q[k] : q[k + 4], 8);
+#pragma unroll
+  for (int k = 0; k < 2; ++k)
+    u[k] = (b2 ? r[k + 2] : r[k]) + __shfl_xor_sync(0xffffffffu, b2 ? r[k] : r[k + 2], 4);
+  double v = (b1 ? u[1] : u[0]) + __shfl_xor_sync(0xffffffffu, b1 ? u[0] : u[1], 2);
+  return v + __shfl_xor_sync(0xffffffffu, v, 1);
+}
+
 // Output layer and seed, one warp per point (see k_output_fwd for the
 // formulas).  Shared memory per warp: tl[nout][na], sd[nout][na] (double).
-template <typename R>
+// VEC (rows a whole number of 16-byte pieces): 16 rows per pass, each lane
+// reading 16-byte pieces of every row, so that 16 loads per lane are in
+// flight, and one 16-row reduction (warp_sum16) per pass.
+template <typename R, bool VEC>
 __global__ void __launch_bounds__(256) k_output_fwdv(OutArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -813,6 +837,43 @@ __global__ void __launch_bounds__(256) k_output_fwdv(OutArgs a) {
   double lsum = 0.0;
   for (long pt = (long)blockIdx.x * nw + warp; pt < a.npts; pt += (long)gridDim.x * nw) {
     const R *Tm = (const R *)a.Tm + pt * plane;
+    if constexpr (VEC) {
+      constexpr int V = 16 / sizeof(R);  // values per 16-byte piece
+      using VT = typename std::conditional<sizeof(R) == 4, float4, double2>::type;
+      for (int o = 0; o < nout; ++o) {
+        const double *w = a.W + (size_t)o * (m + 1) + 1;
+        for (int ia0 = 0; ia0 < na; ia0 += 16) {
+          double p[16];
+#pragma unroll
+          for (int r = 0; r < 16; ++r) p[r] = 0.0;
+          for (int c0 = lane * V; c0 < m; c0 += 32 * V) {
+            double wv[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) wv[v] = __ldg(w + c0 + v);
+            VT t[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+              if (ia0 + r < na) t[r] = __ldg((const VT *)(Tm + (size_t)(ia0 + r) * m + c0));
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+              if (ia0 + r < na) {
+                if constexpr (V == 4)
+                  p[r] += wv[0] * (double)t[r].x + wv[1] * (double)t[r].y +
+                          wv[2] * (double)t[r].z + wv[3] * (double)t[r].w;
+                else
+                  p[r] += wv[0] * (double)t[r].x + wv[1] * (double)t[r].y;
+              }
+          }
+          const double tot = warp_sum16(p);
+          const int ia = ia0 + (lane >> 1);
+          if (!(lane & 1) && ia < na) {
+            const double v = (ia == 0 ? a.W[(size_t)o * (m + 1)] : 0.0) + tot;
+            tl[o * na + ia] = v;
+            if (a.out) a.out[(pt * (size_t)na + ia) * nout + o] = v;
+          }
+        }
+      }
+    } else
     for (int o = 0; o < nout; ++o) {
       const double *w = a.W + (size_t)o * (m + 1) + 1;
       // four multi-indices per step, independent loads and reductions
@@ -1386,10 +1447,14 @@ static int launch_output_fwdv(const OutArgs &o, cudaStream_t st) {
   const int wpb = (int)std::min<size_t>(8, (200 * 1024) / std::max<size_t>(per_warp, 1));
   if (wpb < 1) return RC_UNSUPPORTED;
   const size_t smem = per_warp * wpb;
-  const void *k = (const void *)k_output_fwdv<R>;
+  const bool vec = o.m % (16 / (int)sizeof(R)) == 0;
+  const void *k = vec ? (const void *)k_output_fwdv<R, true> : (const void *)k_output_fwdv<R, false>;
   CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = std::max(1, std::min((o.npts + wpb - 1) / wpb, occ_grid(k, 32 * wpb, smem)));
-  LAUNCH("k_output_fwd", st, (k_output_fwdv<R><<<grid, 32 * wpb, smem, st>>>(o)));
+  if (vec)
+    LAUNCH("k_output_fwd", st, (k_output_fwdv<R, true><<<grid, 32 * wpb, smem, st>>>(o)));
+  else
+    LAUNCH("k_output_fwd", st, (k_output_fwdv<R, false><<<grid, 32 * wpb, smem, st>>>(o)));
   CK(cudaGetLastError());
   return RC_OK;
 }
