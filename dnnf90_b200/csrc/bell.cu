@@ -803,12 +803,26 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd8(Fwd8Args a) {
     const int pt = (int)(it % a.npts);
     const int j = (int)(it / a.npts) * NPB + ln;
     c.act = lact && j < n;
-    if (it + 1 < it1)
+    // FP32: the next item's rows are copied after the barrier, into the
+    // buffer the last item used, so no barrier ends the top degree; FP64
+    // (measured faster so) copies before it and keeps that barrier
+    constexpr bool LATE = sizeof(R) == 4;
+    if (!LATE && it + 1 < it1)
       stage_rows<NPB, R>(sm + (buf ? 0 : a.sbase1), (const R *)a.S + ((it + 1) % a.npts) * plane,
                          na, n, (int)((it + 1) / a.npts) * NPB, BELL_WORKERS * 32);
-    cp_async_commit();
-    cp_async_wait<1>();
-    __syncthreads();
+    if (!LATE) {
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();  // this item's S rows are in; every warp is done with the last item
+    if (LATE) {
+      if (it + 1 < it1)
+        stage_rows<NPB, R>(sm + (buf ? 0 : a.sbase1), (const R *)a.S + ((it + 1) % a.npts) * plane,
+                           na, n, (int)((it + 1) / a.npts) * NPB, BELL_WORKERS * 32);
+      cp_async_commit();
+    }
     c.lx = (buf ? a.sbase1 : 0) + c.lo;
     c.T = (R *)a.T + pt * plane + j;
     c.H = TRAIN ? (R *)a.h + pt * plane + j : nullptr;
@@ -855,7 +869,7 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd8(Fwd8Args a) {
           case 8: if constexpr (KK >= 8) fwd8_degree<R, KK, 8, NPB, TRAIN>(a, c, warp); break;
           default: break;
         }
-        __syncthreads();
+        if (p < KK || !LATE) __syncthreads();  // FP32: the top degree ends at the next item's barrier
       }
     }
     buf ^= 1;
@@ -1193,7 +1207,9 @@ __global__ void __launch_bounds__(ADJ_WORKERS * 32) k_bell_adj7(Adj7Args a) {
       if (act) Sb[(size_t)b * n + j] = v;
       if (b == 0) gb += (double)v;
     }
-    __syncthreads();
+    // no barrier here: the next item's copy goes to the buffer that every
+    // warp left at the barrier after the units, and the scratch rows are
+    // added to only after the next item's first barrier
     buf ^= 1;
   }
   cp_async_wait<0>();

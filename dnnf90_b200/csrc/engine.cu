@@ -801,33 +801,32 @@ __global__ void __launch_bounds__(256) k_adj_l2v(AdjL2vArgs a) {
     for (int i = 0; i <= D0; ++i) atomicAdd(a.g + (size_t)j * (D0 + 1) + i, acc[i]);
 }
 
-// Sum of 16 values over the 32 lanes of a warp with 16 shuffles (not 80):
+// Sum of 8 values over the 32 lanes of a warp with 9 shuffles (not 40):
 // each level hands half of the still-open rows to the partner lane.  On
-// return, lanes 2r and 2r + 1 hold the total of row r.
-__device__ __forceinline__ double warp_sum16(double (&p)[16]) {
+// return, lanes 4r .. 4r + 3 hold the total of row r.
+__device__ __forceinline__ double warp_sum8(double (&p)[8]) {
   const int lane = threadIdx.x & 31;
-  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
-  double q[8], r[4], u[2];
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-    q[k] = (b4 ? p[k + 8] : p[k]) + __shfl_xor_sync(0xffffffffu, b4 ? p[k] : p[k + 8], 16);
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  double q[4], r[2];
 #pragma unroll
   for (int k = 0; k < 4; ++k)
-    r[k] = (b3 ? q[k + 4] : q[k]) + __shfl_xor_sync(0xffffffffu, b3 ? q[k] : q[k + 4], 8);
+    q[k] = (b4 ? p[k + 4] : p[k]) + __shfl_xor_sync(0xffffffffu, b4 ? p[k] : p[k + 4], 16);
 #pragma unroll
   for (int k = 0; k < 2; ++k)
-    u[k] = (b2 ? r[k + 2] : r[k]) + __shfl_xor_sync(0xffffffffu, b2 ? r[k] : r[k + 2], 4);
-  double v = (b1 ? u[1] : u[0]) + __shfl_xor_sync(0xffffffffu, b1 ? u[0] : u[1], 2);
+    r[k] = (b3 ? q[k + 2] : q[k]) + __shfl_xor_sync(0xffffffffu, b3 ? q[k] : q[k + 2], 8);
+  double v = (b2 ? r[1] : r[0]) + __shfl_xor_sync(0xffffffffu, b2 ? r[0] : r[1], 4);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
   return v + __shfl_xor_sync(0xffffffffu, v, 1);
 }
 
 // Output layer and seed, one warp per point (see k_output_fwd for the
 // formulas).  Shared memory per warp: tl[nout][na], sd[nout][na] (double).
-// VEC (rows a whole number of 16-byte pieces): 16 rows per pass, each lane
-// reading 16-byte pieces of every row, so that 16 loads per lane are in
-// flight, and one 16-row reduction (warp_sum16) per pass.
+// VEC (rows a whole number of 16-byte pieces): 8 rows per pass, each lane
+// reading 16-byte pieces of every row, so that 8 loads per lane are in
+// flight, one 8-row reduction (warp_sum8) per pass, and few enough
+// registers for three blocks per SM.
 template <typename R, bool VEC>
-__global__ void __launch_bounds__(256) k_output_fwdv(OutArgs a) {
+__global__ void __launch_bounds__(256, VEC ? 3 : 1) k_output_fwdv(OutArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int m = a.m, na = a.na, nout = a.nout;
@@ -842,20 +841,20 @@ __global__ void __launch_bounds__(256) k_output_fwdv(OutArgs a) {
       using VT = typename std::conditional<sizeof(R) == 4, float4, double2>::type;
       for (int o = 0; o < nout; ++o) {
         const double *w = a.W + (size_t)o * (m + 1) + 1;
-        for (int ia0 = 0; ia0 < na; ia0 += 16) {
-          double p[16];
+        for (int ia0 = 0; ia0 < na; ia0 += 8) {
+          double p[8];
 #pragma unroll
-          for (int r = 0; r < 16; ++r) p[r] = 0.0;
+          for (int r = 0; r < 8; ++r) p[r] = 0.0;
           for (int c0 = lane * V; c0 < m; c0 += 32 * V) {
             double wv[V];
 #pragma unroll
             for (int v = 0; v < V; ++v) wv[v] = __ldg(w + c0 + v);
-            VT t[16];
+            VT t[8];
 #pragma unroll
-            for (int r = 0; r < 16; ++r)
+            for (int r = 0; r < 8; ++r)
               if (ia0 + r < na) t[r] = __ldg((const VT *)(Tm + (size_t)(ia0 + r) * m + c0));
 #pragma unroll
-            for (int r = 0; r < 16; ++r)
+            for (int r = 0; r < 8; ++r)
               if (ia0 + r < na) {
                 if constexpr (V == 4)
                   p[r] += wv[0] * (double)t[r].x + wv[1] * (double)t[r].y +
@@ -864,9 +863,9 @@ __global__ void __launch_bounds__(256) k_output_fwdv(OutArgs a) {
                   p[r] += wv[0] * (double)t[r].x + wv[1] * (double)t[r].y;
               }
           }
-          const double tot = warp_sum16(p);
-          const int ia = ia0 + (lane >> 1);
-          if (!(lane & 1) && ia < na) {
+          const double tot = warp_sum8(p);
+          const int ia = ia0 + (lane >> 2);
+          if (!(lane & 3) && ia < na) {
             const double v = (ia == 0 ? a.W[(size_t)o * (m + 1)] : 0.0) + tot;
             tl[o * na + ia] = v;
             if (a.out) a.out[(pt * (size_t)na + ia) * nout + o] = v;
