@@ -674,12 +674,20 @@ void gemm_tc_release_weights(DevNet *net) {
   net->tc = nullptr;
 }
 
-static bool tc_shape_ok(int N, int K) {
-  if (N % 16 || K % 16 || N < 16 || K < 16) return false;
-  if (N > 128 && N % 128) return false;
-  const int BN = std::min(N, 128), nkb = (K + 63) / 64;
-  const size_t smem = (size_t)3 * nkb * BN * 128 + 2 * 3 * 128 * 128 + 2048 + tc::STG_BYTES;
-  return smem <= 227 * 1024;
+// N tile of a FWD/DT product with N outputs and depth K: the widest of
+// min(N, 128), 64, 32, 16 that divides N and leaves the pre-split weights
+// (3 terms x K x BN bf16) resident in shared memory beside the stages; 0
+// when none does.  (K = 256 takes BN = 64.)
+static int tc_bn(int N, int K) {
+  if (N % 16 || K % 16 || N < 16 || K < 16) return 0;
+  const int nkb = (K + 63) / 64;
+  const int cand[4] = {std::min(N, 128), 64, 32, 16};
+  for (int BN : cand) {
+    if (BN > N || N % BN) continue;
+    const size_t smem = (size_t)3 * nkb * BN * 128 + 2 * 3 * 128 * 128 + 2048 + tc::STG_BYTES;
+    if (smem <= 227 * 1024) return BN;
+  }
+  return 0;
 }
 
 // Pre-split weights of a network.  The buffers are allocated on the first
@@ -704,8 +712,7 @@ int gemm_tc_prepare(DevNet *net, const double *hw, cudaStream_t st) {
   for (int l = 3; l < L; ++l) {  // hidden layers with a GEMM
     const int n = net->dims[l - 1], m = net->dims[l - 2];
     const double *Wl = hw + net->woff[l - 1];
-    if (tc_shape_ok(n, m)) {
-      const int BN = std::min(n, 128);
+    if (const int BN = tc_bn(n, m)) {
       auto b = tc::prep_b(n, m, BN, [&](int j, int k) { return (float)Wl[(size_t)j * (m + 1) + 1 + k]; });
       if (!w->fwd[l - 1]) CKT(cudaMalloc(&w->fwd[l - 1], b.size()));
       CKT(cudaMemcpyAsync(w->fwd[l - 1], b.data(), b.size(), cudaMemcpyHostToDevice, st));
@@ -716,8 +723,7 @@ int gemm_tc_prepare(DevNet *net, const double *hw, cudaStream_t st) {
       w->bn_fwd[l - 1] = BN;
       CKT(cudaStreamSynchronize(st));  // b and bias leave scope
     }
-    if (tc_shape_ok(m, n)) {
-      const int BN = std::min(m, 128);
+    if (const int BN = tc_bn(m, n)) {
       auto b = tc::prep_b(m, n, BN, [&](int i, int j) { return (float)Wl[(size_t)j * (m + 1) + 1 + i]; });
       if (!w->dt[l - 1]) CKT(cudaMalloc(&w->dt[l - 1], b.size()));
       CKT(cudaMemcpyAsync(w->dt[l - 1], b.data(), b.size(), cudaMemcpyHostToDevice, st));

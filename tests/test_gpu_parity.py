@@ -78,6 +78,7 @@ def _rule_terms(ts, name):
     (2, 3, [[0, 1], [1, 0], [3, 0]], [2, 64, 64, 64, 1], "kdv", 300),
     (4, 7, None, [4, 64, 64, 64, 1], "zk7", 6),
     (4, 5, None, [4, 24, 20, 3], "halfsq", 40),
+    (2, 3, None, [2, 256, 256, 256, 1], "halfsq", 64),   # K = 256 layer GEMMs (N tile 64)
 ])
 @pytest.mark.parametrize("prec", [api.PREC_F64, api.PREC_SPLIT])
 def test_grad_rule_batch(d0, k, seeds, dims, rule, npts, prec):
