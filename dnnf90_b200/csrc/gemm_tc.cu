@@ -853,11 +853,12 @@ int gemm_tc_dt(const DevNet *net, int l, int M, int n, int m, const void *Sb, vo
 int gemm_tc_dw(const DevNet *net, int l, int M, int n, int m, const void *Sb, const void *Tm,
                double *G, cudaStream_t st) {
   TcWeights *w = (TcWeights *)net->tc;
-  if (!w || n > 128 || n % 16 || m % 16) return RC_UNSUPPORTED;
+  if (!w || n % 16 || m % 16) return RC_UNSUPPORTED;
   const int BN = 64;
-  const int ntn = (m + BN - 1) / BN;
+  const int ntn = (m + BN - 1) / BN, ntm = (n + tc::BM - 1) / tc::BM;  // output tiles
+  if (ntm > 65535) return RC_UNSUPPORTED;
   const int nkb_all = (M + tc::BK - 1) / tc::BK;
-  const int ctas_k = std::max(1, std::min(nkb_all, grid_sms() / ntn));
+  const int ctas_k = std::max(1, std::min(nkb_all, grid_sms() / (ntn * ntm)));
   tc::Args a;
   std::memset(&a, 0, sizeof a);
   a.mode = tc::MODE_DW; a.M = n; a.N = m; a.K = M; a.na = 1;
@@ -867,7 +868,7 @@ int gemm_tc_dw(const DevNet *net, int l, int M, int n, int m, const void *Sb, co
   a.flag = w->flag;
   const size_t stage = 3 * (8 * 2 * 1024) + 3 * (8 * 1 * 1024);
   const size_t smem = 1024 + 3 * stage + 1024;
-  dim3 grid((nkb_all + a.kblocks_per_cta - 1) / a.kblocks_per_cta, ntn);
+  dim3 grid((nkb_all + a.kblocks_per_cta - 1) / a.kblocks_per_cta, ntn, ntm);
   return launch(a, tc::MODE_DW, grid, smem, st);
 }
 
