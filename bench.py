@@ -303,6 +303,10 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--committee-steps", type=int, default=3,
                     help="timed steps of the 64-network committee (0 skips it)")
+    ap.add_argument("--pin-variants", default=None, metavar="FWD,ADJ",
+                    help="pin the Bell forward and adjoint kernel variants (dnnf90_tune_force) "
+                         "instead of autotuning them; for profiler runs, whose serialised "
+                         "launches upset the autotuner's timings")
     ap.add_argument("--prof-steps", type=int, default=1,
                     help="steps of the per-kernel event-profiled pass (untimed)")
     args = ap.parse_args()
@@ -315,6 +319,10 @@ def main():
     from dnnf90_b200 import api
     from dnnf90_b200.dp import ReducedStep
 
+    if args.pin_variants:
+        fv, av = (int(v) for v in args.pin_variants.split(","))
+        api.tune_force(0, fv)
+        api.tune_force(1, av)
     ws, rank, local = dist_init()
     dev = torch.device("cuda", local)
     hbm_free0 = torch.cuda.mem_get_info(dev)[0] / 2**30
