@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libdnnf90_b200.so")
 
 PREC_F64 = 0
 PREC_SPLIT = 1
-SEED_HALFSQ, SEED_PINN, SEED_JROW = 1, 2, 3
+SEED_HALFSQ, SEED_PINN, SEED_JROW, SEED_SYS = 1, 2, 3, 4
 
 # the symbols the headers declare (include/dnnf90.h, include/dnnf90_b200.h)
 REFERENCE_SYMBOLS = [
@@ -45,6 +45,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_launch_count", "dnnf90_profile_enable", "dnnf90_profile_read",
     "dnnf90_ngd_step_noalloc", "dnnf90_committee_step", "dnnf90_committee_info",
     "dnnf90_tune_report", "dnnf90_tune_force", "dnnf90_tabset_free",
+    "dnnf90_seed_rule_sys", "dnnf90_grad_sys_batch",
 ]
 
 _lib = None
@@ -127,6 +128,8 @@ def lib():
         "dnnf90_committee_info": [pi, P(ctypes.c_float)],
         "dnnf90_tune_report": [ctypes.c_char_p, i],
         "dnnf90_tune_force": [i, i],
+        "dnnf90_seed_rule_sys": [i, i, pi, pd, pi, pi, pi, pd, d],
+        "dnnf90_grad_sys_batch": [i, i, i, pd, pd, i, i, pd, pd],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -336,6 +339,18 @@ class Grad:
              rule.rid, self.gid, _pd(loss), _pd(t))
         return (float(loss[0]), t) if want_t else float(loss[0])
 
+    def sys_batch(self, X, rule: "SeedRule", src=None, want_t=False):
+        """Forward, system seed (sources src[npts][nres], None = zero) and
+        adjoint over a batch, added to this accumulator.  Returns the loss,
+        and T[npts][nout][na] if want_t."""
+        X = _f64(X)
+        loss = np.zeros(1)
+        tm = np.zeros((X.shape[0], self.net.nout, self.net.na)) if want_t else None
+        sv = _f64(src) if src is not None else None
+        call("dnnf90_grad_sys_batch", self.net.nid, self.net.tid, X.shape[0], _pd(X), _pd(sv),
+             rule.rid, self.gid, _pd(loss), _pd(tm))
+        return (float(loss[0]), tm) if want_t else float(loss[0])
+
     def read(self):
         g = np.zeros(self.net.nw)
         call("dnnf90_grad_read", self.gid, _pd(g))
@@ -364,6 +379,22 @@ class SeedRule:
         n = np.array([int(t[2]) for t in terms] or [0], np.int32)
         self.rid = call("dnnf90_seed_rule_create", int(kind), len(terms), _pd(c), _pi(s),
                         _pi(n), float(fac))
+
+    @classmethod
+    def system(cls, nres, terms, wres=None, fac: float = 1.0) -> "SeedRule":
+        """A system rule (dnnf90_seed_rule_sys).  terms: (residual, coeff,
+        [(component, slot), ...]) with 1-based residual, component and slot."""
+        self = cls.__new__(cls)
+        self.kind = SEED_SYS
+        res = np.array([t[0] for t in terms], np.int32)
+        coeff = np.array([t[1] for t in terms], np.float64)
+        nfac = np.array([len(t[2]) for t in terms], np.int32)
+        comp = np.array([f[0] for t in terms for f in t[2]], np.int32)
+        slot = np.array([f[1] for t in terms for f in t[2]], np.int32)
+        wr = _f64(np.asarray(wres, np.float64)) if wres is not None else None
+        self.rid = call("dnnf90_seed_rule_sys", int(nres), len(terms), _pi(res), _pd(coeff),
+                        _pi(nfac), _pi(comp), _pi(slot), _pd(wr), float(fac))
+        return self
 
     def free(self):
         if self.rid > 0:

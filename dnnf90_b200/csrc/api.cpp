@@ -224,10 +224,16 @@ int grad_alloc(GradH &g) {
   return ck(cudaMemset(g.d, 0, sizeof(double) * std::max(1, g.nw)), "cudaMemset");
 }
 
-int rule_device(RuleH &r, const TableSet &ts) {
+int rule_device(RuleH &r, const NetH &n) {
+  const TableSet &ts = n.ts;
   for (int s : r.r.ind)
     if (s < 0 || s >= ts.na) {
       set_error("seed rule names a slot the table set does not carry");
+      return RC_BAD_ARG;
+    }
+  for (size_t f = 0; f + 1 < r.r.sfac.size(); f += 2)
+    if (r.r.sfac[f] >= n.dims[n.nlayer - 1] || r.r.sfac[f + 1] >= ts.na) {
+      set_error("system seed rule names an output component or slot the network does not carry");
       return RC_BAD_ARG;
     }
   if (!r.up) {
@@ -473,14 +479,15 @@ void relayout(const double *src, double *dst, int npts, int na, int nout,
 // jrow_batch).  kind SEED_GIVEN uses seed[npts][na] (output 1).
 int host_train(int nid, int tid, int npts, const double *x, int kind,
                RuleH *rule, const double *seed, double *grad_dev, double *rows,
-               double *loss, double *t, double *resid) {
+               double *loss, double *t, double *resid, const double *src = nullptr,
+               double *tmall = nullptr) {
   NetH &n = g_net[nid];
   WorkH &w = g_twk[tid];
   int rc;
   if ((rc = flush_queue(tid))) return rc;
   if ((rc = work_stream(w))) return rc;
   if ((rc = net_device(n, w.st))) return rc;
-  if (rule && (rc = rule_device(*rule, n.ts))) return rc;
+  if (rule && (rc = rule_device(*rule, n))) return rc;
   if ((rc = work_planes(w, n, npts, false))) return rc;
   const int na = n.ts.na, d0 = n.ts.d0, nout = n.dims[n.nlayer - 1];
   const int cap = w.p.cap_pts;
@@ -500,6 +507,15 @@ int host_train(int nid, int tid, int npts, const double *x, int kind,
     if (drows) cudaFree(drows);
     return rc;
   }
+  const int nres = rule ? rule->r.nres : 0;
+  double *dsrc = nullptr;
+  if (src && nres > 0 &&
+      (rc = ck(cudaMalloc(&dsrc, sizeof(double) * (size_t)cap * nres), "cudaMalloc"))) {
+    if (dseed) cudaFree(dseed);
+    if (drows) cudaFree(drows);
+    cudaFree(dloss);
+    return rc;
+  }
   cudaMemsetAsync(dloss, 0, sizeof(double), w.st);
   std::vector<double> sm, tbuf;
   for (int c0 = 0; c0 < npts && !rc; c0 += cap) {
@@ -517,8 +533,14 @@ int host_train(int nid, int tid, int npts, const double *x, int kind,
                               cudaMemcpyHostToDevice, w.st), "H2D");
       if (rc) break;
     }
+    if (dsrc) {
+      rc = ck(cudaMemcpyAsync(dsrc, src + (size_t)c0 * nres, sizeof(double) * (size_t)np * nres,
+                              cudaMemcpyHostToDevice, w.st), "H2D");
+      if (rc) break;
+    }
     BatchArgs a;
-    a.npts = np; a.X = w.p.X; a.out = (t || resid) ? w.p.out : nullptr;
+    a.npts = np; a.X = w.p.X; a.out = (t || resid || tmall) ? w.p.out : nullptr;
+    a.src = dsrc;
     a.seeds = dseed; a.grad = rows ? nullptr : grad_dev; a.rows = drows;
     a.loss = dloss; a.train = true; a.prec = n.prec;
     rc = run_batch(n.dt, n.dn, rule ? rule->d : given, w.p, a, w.st);
@@ -528,12 +550,13 @@ int host_train(int nid, int tid, int npts, const double *x, int kind,
                               cudaMemcpyDeviceToHost, w.st), "D2H");
       if (rc) break;
     }
-    if (t || resid) {
+    if (t || resid || tmall) {
       tbuf.resize((size_t)np * na * nout);
       rc = ck(cudaMemcpyAsync(tbuf.data(), w.p.out, sizeof(double) * tbuf.size(),
                               cudaMemcpyDeviceToHost, w.st), "D2H");
       if (!rc) rc = ck(cudaStreamSynchronize(w.st), "sync");
       if (rc) break;
+      if (tmall) relayout(tbuf.data(), tmall + (size_t)c0 * nout * na, np, na, nout, false);
       std::vector<double> t1((size_t)np * na);
       relayout(tbuf.data(), t1.data(), np, na, nout, true);
       if (t) std::memcpy(t + (size_t)c0 * na, t1.data(), sizeof(double) * t1.size());
@@ -556,6 +579,7 @@ int host_train(int nid, int tid, int npts, const double *x, int kind,
   if (loss) *loss = lv;
   if (dseed) cudaFree(dseed);
   if (drows) cudaFree(drows);
+  if (dsrc) cudaFree(dsrc);
   cudaFree(dloss);
   return rc;
 }
@@ -984,6 +1008,48 @@ int dnnf90_seed_rule_create(int kind, int nterm, const double *coeff, const int 
   return id;
 }
 
+int dnnf90_seed_rule_sys(int nres, int nterm, const int *res, const double *coeff,
+                         const int *nfac, const int *comp, const int *slot, const double *wres,
+                         double fac) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (nres < 1 || nres > SYS_MAXRES || nterm < 1 || !res || !coeff || !nfac || !comp || !slot) {
+    set_error("dnnf90_seed_rule_sys: 1 <= nres <= " + std::to_string(SYS_MAXRES) +
+              ", nterm >= 1 and every term array are required");
+    return RC_BAD_ARG;
+  }
+  RuleH r;
+  r.used = true;
+  r.r.kind = SEED_SYS;
+  r.r.fac = fac;
+  r.r.nres = nres;
+  int f = 0;
+  for (int k = 0; k < nterm; ++k) {
+    if (res[k] < 1 || res[k] > nres || nfac[k] < 1 || nfac[k] > SYS_MAXFAC) {
+      set_error("dnnf90_seed_rule_sys: term " + std::to_string(k + 1) +
+                ": residual outside 1..nres or factor count outside 1.." +
+                std::to_string(SYS_MAXFAC));
+      return RC_BAD_ARG;
+    }
+    r.r.sys.push_back(res[k] - 1);
+    r.r.sys.push_back(nfac[k]);
+    r.r.sys.push_back(f);
+    r.r.coeff.push_back(coeff[k]);
+    for (int m = 0; m < nfac[k]; ++m, ++f) {
+      if (comp[f] < 1 || slot[f] < 1) {
+        set_error("dnnf90_seed_rule_sys: components and slots are 1-based");
+        return RC_BAD_ARG;
+      }
+      r.r.sfac.push_back(comp[f] - 1);
+      r.r.sfac.push_back(slot[f] - 1);
+    }
+  }
+  for (int i = 0; i < nres; ++i) r.r.wres.push_back(wres ? wres[i] : 1.0);
+  int id = free_slot(g_rule);
+  if (id < 0) return RC_BAD_ARG;
+  g_rule[id] = std::move(r);
+  return id;
+}
+
 int dnnf90_seed_rule_free(int rid) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (rid < 1 || rid > MAXH || !g_rule[rid].used) return RC_BAD_ARG;
@@ -1006,6 +1072,20 @@ int dnnf90_grad_rule_batch(int nid, int tid, int npts, const double *x, int rid,
   if ((rc = device_ready()) || (rc = grad_alloc(g_grd[gid]))) return rc;
   return host_train(nid, tid, npts, x, g_rule[rid].r.kind, &g_rule[rid], nullptr,
                     g_grd[gid].d, nullptr, loss, t, nullptr);
+}
+
+int dnnf90_grad_sys_batch(int nid, int tid, int npts, const double *x, const double *src,
+                          int rid, int gid, double *loss, double *tm) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, gid, true);
+  if (rc) return rc;
+  if (bad_rule(rid) || g_rule[rid].r.kind != SEED_SYS) return RC_BAD_ARG;
+  if (npts < 0 || (npts > 0 && !x)) return RC_BAD_ARG;
+  if (loss) *loss = 0.0;
+  if (npts == 0) return RC_OK;
+  if ((rc = device_ready()) || (rc = grad_alloc(g_grd[gid]))) return rc;
+  return host_train(nid, tid, npts, x, SEED_SYS, &g_rule[rid], nullptr, g_grd[gid].d, nullptr,
+                    loss, nullptr, nullptr, src, tm);
 }
 
 int dnnf90_jrow_batch(int nid, int tid, int npts, const double *x, int rid, double *rows,
@@ -1154,7 +1234,7 @@ int dnnf90_grad_rule_dev(int nid, int tid, int npts, const double *x_dev, int ri
   WorkH &w = g_twk[tid];
   cudaStream_t st = (cudaStream_t)stream;
   if ((rc = net_device(n, st))) return rc;
-  if ((rc = rule_device(g_rule[rid], n.ts))) return rc;
+  if ((rc = rule_device(g_rule[rid], n))) return rc;
   if ((rc = work_planes(w, n, npts, false))) return rc;
   w.kept = false;
   BatchArgs a;
@@ -1175,7 +1255,7 @@ int dnnf90_jrow_dev(int nid, int tid, int npts, const double *x_dev, int rid,
   WorkH &w = g_twk[tid];
   cudaStream_t st = (cudaStream_t)stream;
   if ((rc = net_device(n, st))) return rc;
-  if ((rc = rule_device(g_rule[rid], n.ts))) return rc;
+  if ((rc = rule_device(g_rule[rid], n))) return rc;
   if ((rc = work_planes(w, n, npts, false))) return rc;
   w.kept = false;
   BatchArgs a;
@@ -1417,7 +1497,7 @@ int dnnf90_committee_step(int nnet, const int *nids, const int *tids, const int 
     NetH &n = g_net[nids[i]];
     flush_for_net(nids[i]);
     if ((rc = net_device(n, caller))) return rc;
-    if ((rc = rule_device(g_rule[rids[i]], n.ts))) return rc;
+    if ((rc = rule_device(g_rule[rids[i]], n))) return rc;
   }
   Committee *C = nullptr;
   for (auto &c : g_comm)

@@ -283,12 +283,14 @@ void DevNet::release() {
 }
 
 void DevRule::release() {
-  if (coeff) cudaFree(coeff);
-  if (ind) cudaFree(ind);
-  if (nonlin) cudaFree(nonlin);
+  void *ps[] = {coeff, ind, nonlin, sys, sfac, wres};
+  for (void *p : ps)
+    if (p) cudaFree(p);
   coeff = nullptr;
   ind = nullptr;
   nonlin = nullptr;
+  sys = sfac = nullptr;
+  wres = nullptr;
 }
 
 int upload_rule(const SeedRuleHost &r, DevRule &d) {
@@ -301,6 +303,12 @@ int upload_rule(const SeedRuleHost &r, DevRule &d) {
   if ((rc = dput(&d.coeff, r.coeff.data(), r.coeff.size()))) return rc;
   if ((rc = dput(&d.ind, r.ind.data(), r.ind.size()))) return rc;
   if ((rc = dput(&d.nonlin, r.nonlin.data(), r.nonlin.size()))) return rc;
+  d.nres = r.nres;
+  if (r.kind == SEED_SYS) {
+    if ((rc = dput(&d.sys, r.sys.data(), r.sys.size()))) return rc;
+    if ((rc = dput(&d.sfac, r.sfac.data(), r.sfac.size()))) return rc;
+    if ((rc = dput(&d.wres, r.wres.data(), r.wres.size()))) return rc;
+  }
   return RC_OK;
 }
 
@@ -539,7 +547,42 @@ struct OutArgs {
   const int *ind, *nonlin;
   double fac;
   double *loss;
+  int nres;              // SEED_SYS
+  const int *sys, *sfac;
+  const double *wres;
+  const double *src;     // [P][nres] sources (may be null)
 };
+
+// Residuals of a system rule at one point and the seed they imply
+// (calc_sys_residual / set_sys_seed, app/pinn_module.f90:86-162), in the
+// reference's order of operations; tl[nout][na] the point's outputs, sd
+// (zeroed) receives the seed.  Returns the point's loss fac/2 sum_r w_r R_r^2.
+__device__ double sys_seed(const OutArgs &a, const double *tl, double *sd, long pt) {
+  const int na = a.na;
+  double R[SYS_MAXRES];
+  for (int r = 0; r < a.nres; ++r) R[r] = a.src ? -a.src[pt * a.nres + r] : 0.0;
+  for (int k = 0; k < a.nterm; ++k) {
+    const int r = a.sys[3 * k], nf = a.sys[3 * k + 1], f0 = a.sys[3 * k + 2];
+    double prod = a.coeff[k];
+    for (int m = 0; m < nf; ++m) prod = prod * tl[a.sfac[2 * (f0 + m)] * na + a.sfac[2 * (f0 + m) + 1]];
+    R[r] = R[r] + prod;
+  }
+  double l = 0.0;
+  for (int r = 0; r < a.nres; ++r) l += a.wres[r] * R[r] * R[r];
+  for (int k = 0; k < a.nterm; ++k) {
+    const int r = a.sys[3 * k], nf = a.sys[3 * k + 1], f0 = a.sys[3 * k + 2];
+    for (int m = 0; m < nf; ++m) {
+      double other = a.fac * a.wres[r] * R[r] * a.coeff[k];
+      for (int mm = 0; mm < nf; ++mm) {
+        if (mm == m) continue;
+        other = other * tl[a.sfac[2 * (f0 + mm)] * na + a.sfac[2 * (f0 + mm) + 1]];
+      }
+      const int at = a.sfac[2 * (f0 + m)] * na + a.sfac[2 * (f0 + m) + 1];
+      sd[at] = sd[at] + other;
+    }
+  }
+  return 0.5 * a.fac * l;
+}
 
 // Output layer (identity read-out, lib/train_module.f90:326-328) and the
 // seed of the loss at every point (app/pinn_module.f90:32-65).  One block
@@ -574,6 +617,8 @@ __global__ void __launch_bounds__(256) k_output_fwd(OutArgs a) {
         double l = 0.0;
         for (int ia = 0; ia < na; ++ia) { sd[ia] = tl[ia]; l += tl[ia] * tl[ia]; }
         lsum += 0.5 * l;
+      } else if (a.kind == SEED_SYS) {
+        lsum += sys_seed(a, tl, sd, pt);
       } else {
         double R0 = 0.0;
         for (int t = 0; t < a.nterm; ++t) {
@@ -904,6 +949,8 @@ __global__ void __launch_bounds__(256, VEC ? 3 : 1) k_output_fwdv(OutArgs a) {
           double l = 0.0;
           for (int ia = 0; ia < na; ++ia) { sd[ia] = tl[ia]; l += tl[ia] * tl[ia]; }
           lsum += 0.5 * l;
+        } else if (a.kind == SEED_SYS) {
+          lsum += sys_seed(a, tl, sd, pt);
         } else {
           double R0 = 0.0;
           for (int t = 0; t < a.nterm; ++t) {
@@ -1504,7 +1551,8 @@ struct Chunk {
 // rule's seed and loss.  train keeps the h planes for the adjoint.
 template <typename R>
 static int fwd_chunk(Chunk<R> &c, const DevRule *rule, const double *X,
-                     double *out, double *seed, double *loss, bool train) {
+                     double *out, double *seed, double *loss, bool train,
+                     const double *src = nullptr) {
   const DevTables &t = c.t;
   const DevNet &net = c.net;
   Planes &p = c.p;
@@ -1548,6 +1596,11 @@ static int fwd_chunk(Chunk<R> &c, const DevRule *rule, const double *X,
   o.nonlin = rule ? rule->nonlin : nullptr;
   o.fac = rule ? rule->fac : 1.0;
   o.loss = loss;
+  o.nres = rule ? rule->nres : 0;
+  o.sys = rule ? rule->sys : nullptr;
+  o.sfac = rule ? rule->sfac : nullptr;
+  o.wres = rule ? rule->wres : nullptr;
+  o.src = src;
   size_t smem = (size_t)2 * o.nout * na * sizeof(double);
   if (smem > 200 * 1024) { set_error("output layer too wide"); return RC_UNSUPPORTED; }
   rc = launch_output_fwdv<R>(o, c.st);
@@ -1660,7 +1713,7 @@ static int run_all(const DevTables &t, const DevNet &net, const DevRule &rule,
     const bool given = rule.kind == SEED_GIVEN;
     double *seed = (a.train && !given) ? (double *)p.seed : nullptr;
     int rc = fwd_chunk<R>(c, a.train && !given ? &rule : nullptr, X, out, seed, a.loss,
-                          a.train);
+                          a.train, a.src ? a.src + (size_t)c0 * rule.nres : nullptr);
     if (rc) return rc;
     if (!a.train) continue;
     const double *sd = given ? a.seeds + (size_t)c0 * nout * na : seed;

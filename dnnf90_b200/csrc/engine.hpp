@@ -46,7 +46,9 @@ enum SeedKind : int {
   SEED_GIVEN = 0,   // caller supplied dL/dT per point
   SEED_HALFSQ = 1,  // L = sum_a T_a^2 / 2, seed = T
   SEED_PINN = 2,    // L = fac R^2 / 2 with R a linear / u*T_a term list
-  SEED_JROW = 3     // seed = dR/dT, per-point gradient rows
+  SEED_JROW = 3,    // seed = dR/dT, per-point gradient rows
+  SEED_SYS = 4      // system: R_r from products of several outputs' slots,
+                    // L = fac/2 sum_r w_r R_r^2 (app/pinn_module.f90:86-162)
 };
 
 struct SeedRuleHost {
@@ -55,7 +57,15 @@ struct SeedRuleHost {
   std::vector<int> ind;     // 0-based slots
   std::vector<int> nonlin;  // 1: term is coeff * T_0 * T_ind
   double fac = 1.0;
+  // SEED_SYS: term k adds coeff[k] * prod of its factors to residual
+  // sys[3k]; its sys[3k + 1] factors start at sys[3k + 2] in sfac, pairs
+  // (component, slot), 0-based; wres[nres] the residual weights
+  int nres = 0;
+  std::vector<int> sys, sfac;
+  std::vector<double> wres;
 };
+constexpr int SYS_MAXRES = 8;   // residuals of a system rule
+constexpr int SYS_MAXFAC = 4;   // factors of one term
 
 // device copy of one table set
 struct DevTables {
@@ -128,6 +138,7 @@ struct Stream {
 struct BatchArgs {
   int npts = 0;
   const double *X = nullptr;
+  const double *src = nullptr;  // SEED_SYS sources [npts][nres] (may be null)
   double *out = nullptr;
   const double *seeds = nullptr;
   double *grad = nullptr;
@@ -145,6 +156,9 @@ struct DevRule {
   double *coeff = nullptr;
   int *ind = nullptr;
   int *nonlin = nullptr;
+  int nres = 0;              // SEED_SYS (see SeedRuleHost)
+  int *sys = nullptr, *sfac = nullptr;
+  double *wres = nullptr;
   void release();
 };
 int upload_rule(const SeedRuleHost &r, DevRule &d);

@@ -55,10 +55,31 @@ int dnnf90_grad_batch(int nid, int tid, int npts, const double *x,
 int dnnf90_seed_rule_create(int kind, int nterm, const double *coeff,
                             const int *slot, const int *nonlin, double fac);
 int dnnf90_seed_rule_free(int rid);
+/* A system seed rule (calc_sys_residual / set_sys_seed, app/pinn_module.f90:
+ * 86-162): several residuals over several output components.  Term k adds
+ *   coeff[k] * T(comp, slot) * ...   (nfac[k] factors, 1 <= nfac[k] <= 4)
+ * to residual res[k]; its factors follow those of terms < k in comp[] and
+ * slot[].  R_r = -src_r + (sum of its terms), L = fac/2 sum_r wres[r] R_r^2,
+ * seed = fac sum_r wres[r] R_r dR_r/dT, each factor of a term seeded with
+ * the product of the term's other factors.  res, comp and slot are 1-based;
+ * 1 <= nres <= 8; wres may be NULL (all 1).  Usable with
+ * dnnf90_grad_rule_batch / _dev (sources zero) and dnnf90_grad_sys_batch;
+ * the Jacobian-row entries refuse it.  Returns a rule handle. */
+int dnnf90_seed_rule_sys(int nres, int nterm, const int *res, const double *coeff,
+                         const int *nfac, const int *comp, const int *slot,
+                         const double *wres, double fac);
 /* forward -> device seed -> adjoint over a batch, added to gid; loss (sum
  * over points) and t (output 1) may be NULL */
 int dnnf90_grad_rule_batch(int nid, int tid, int npts, const double *x,
                            int rid, int gid, double *loss, double *t);
+/* forward -> system seed with sources src[npts][nres] (NULL: zero) ->
+ * adjoint over a batch, added to gid; loss (sum over points) and
+ * tm[npts][nout][na] (every output component) may be NULL.  The batched
+ * form of the reference's per-point calc_sys_residual / set_sys_seed /
+ * net_backward_point_multi loop (app/pinn_module.f90:86-162,
+ * lib/train_module.f90:459-475); new */
+int dnnf90_grad_sys_batch(int nid, int tid, int npts, const double *x, const double *src,
+                          int rid, int gid, double *loss, double *tm);
 /* Jacobian rows of a rule's residual, rows[npts][nweights]; resid[npts]
  * (the residual R per point) and t may be NULL */
 int dnnf90_jrow_batch(int nid, int tid, int npts, const double *x, int rid,

@@ -710,6 +710,110 @@ int orc_grad_batch(const orc_tables *t, int nlayer, const int *dims,
   return 0;
 }
 
+void orc_sys_residual(const orc_sys_rule *r, const double *tm, int na, const double *src,
+                      double *R) {
+  for (int ir = 0; ir < r->nres; ++ir) R[ir] = src ? -src[ir] : 0.0;
+  int f = 0;
+  for (int k = 0; k < r->nterm; ++k) {
+    double prod = r->coeff[k];
+    for (int m = 0; m < r->nfac[k]; ++m)
+      prod = prod * tm[(size_t)(r->comp[f + m] - 1) * na + r->slot[f + m] - 1];
+    R[r->res[k] - 1] = R[r->res[k] - 1] + prod;
+    f += r->nfac[k];
+  }
+}
+
+void orc_sys_seed(const orc_sys_rule *r, const double *tm, int na, int nout, const double *R,
+                  double *seedm) {
+  for (int i = 0; i < nout * na; ++i) seedm[i] = 0.0;
+  int f = 0;
+  for (int k = 0; k < r->nterm; ++k) {
+    const int ir = r->res[k] - 1;
+    const double wr = r->wres ? r->wres[ir] : 1.0;
+    for (int m = 0; m < r->nfac[k]; ++m) {
+      double other = r->fac * wr * R[ir] * r->coeff[k];
+      for (int mm = 0; mm < r->nfac[k]; ++mm) {
+        if (mm == m) continue;
+        other = other * tm[(size_t)(r->comp[f + mm] - 1) * na + r->slot[f + mm] - 1];
+      }
+      const size_t at = (size_t)(r->comp[f + m] - 1) * na + r->slot[f + m] - 1;
+      seedm[at] = seedm[at] + other;
+    }
+    f += r->nfac[k];
+  }
+}
+
+int orc_grad_sys_batch(const orc_tables *t, int nlayer, const int *dims, const double *w,
+                       int npts, const double *X, const orc_sys_rule *rule,
+                       const double *src, double *grad, double *tout, double *loss,
+                       int nthreads) {
+  if (nlayer < 2 || dims[0] != t->d0 || !rule || rule->nres < 1 || rule->nterm < 1) return -1;
+  const int na = t->na, d0 = t->d0, nout = dims[nlayer - 1], nres = rule->nres;
+  {
+    int f = 0;
+    for (int k = 0; k < rule->nterm; ++k) {
+      if (rule->res[k] < 1 || rule->res[k] > nres || rule->nfac[k] < 1) return -1;
+      for (int m = 0; m < rule->nfac[k]; ++m, ++f)
+        if (rule->comp[f] < 1 || rule->comp[f] > nout || rule->slot[f] < 1 || rule->slot[f] > na)
+          return -1;
+    }
+  }
+  const int nw = orc_weight_count(nlayer, dims);
+  if (grad) memset(grad, 0, sizeof(double) * nw);
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+  nthreads = 1;
+#endif
+  const int nthr = nthreads;
+  double *gthr = (double *)calloc((size_t)nthr * nw, sizeof(double));
+  double *lthr = (double *)calloc(nthr, sizeof(double));
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nthr)
+#endif
+  {
+#ifdef _OPENMP
+    int tid = omp_get_thread_num();
+#else
+    int tid = 0;
+#endif
+    work wk;
+    work_init(&wk, t, nlayer, dims);
+    double *tm = (double *)malloc(sizeof(double) * (size_t)nout * na);
+    double *sd = (double *)malloc(sizeof(double) * (size_t)nout * na);
+    double *R = (double *)malloc(sizeof(double) * nres);
+    double *g = gthr + (size_t)tid * nw;
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+    for (int n = 0; n < npts; ++n) {
+      forward_core(t, &wk, dims, w, X + (size_t)n * d0, 1);
+      for (int o = 0; o < nout; ++o)
+        for (int ia = 0; ia < na; ++ia) tm[(size_t)o * na + ia] = TT(&wk, o + 1, ia, nlayer - 1);
+      if (tout) memcpy(tout + (size_t)n * nout * na, tm, sizeof(double) * (size_t)nout * na);
+      orc_sys_residual(rule, tm, na, src ? src + (size_t)n * nres : NULL, R);
+      double l = 0.0;
+      for (int ir = 0; ir < nres; ++ir) l += (rule->wres ? rule->wres[ir] : 1.0) * R[ir] * R[ir];
+      lthr[tid] += 0.5 * rule->fac * l;
+      orc_sys_seed(rule, tm, na, nout, R, sd);
+      backward_core(t, &wk, dims, w, sd, g);
+    }
+    free(tm);
+    free(sd);
+    free(R);
+    work_free(&wk);
+  }
+  if (grad)
+    for (int th = 0; th < nthr; ++th)
+      for (int i = 0; i < nw; ++i) grad[i] += gthr[(size_t)th * nw + i];
+  double total = 0.0;
+  for (int th = 0; th < nthr; ++th) total += lthr[th];
+  if (loss) *loss = total;
+  free(gthr);
+  free(lthr);
+  return 0;
+}
+
 int orc_eval_batch(const orc_tables *t, int nlayer, const int *dims,
                    const double *w, int npts, const double *X, double *tout,
                    int nthreads) {

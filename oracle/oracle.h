@@ -112,6 +112,42 @@ int orc_grad_batch(const orc_tables *t, int nlayer, const int *dims,
                    double *grad, double *rows, double *tout, double *loss,
                    int nthreads);
 
+/* System seed rule (calc_sys_residual / set_sys_seed, app/pinn_module.f90:
+ * 86-162): residual r of a point is
+ *   R_r = -src_r + sum over the terms k of residual r of
+ *         coeff_k * prod_{m < nfac_k} T(comp_{k,m}, slot_{k,m}),
+ * the loss L = fac/2 sum_r w_r R_r^2 and the seed
+ *   dL/dT(c, a) = fac sum_r w_r R_r dR_r/dT(c, a),
+ * each factor of a term seeded with the product of the term's other
+ * factors (accumulated, so a repeated factor counts twice).  res, comp,
+ * slot are 1-based; the factors of term k follow those of terms < k in
+ * comp/slot; wres may be NULL (all 1). */
+typedef struct {
+  int nres, nterm;
+  const int *res;       /* [nterm] */
+  const double *coeff;  /* [nterm] */
+  const int *nfac;      /* [nterm] */
+  const int *comp;      /* [sum nfac] */
+  const int *slot;      /* [sum nfac] */
+  const double *wres;   /* [nres] or NULL */
+  double fac;
+} orc_sys_rule;
+
+/* tm[nout][na] of one point; src[nres] may be NULL (zero) */
+void orc_sys_residual(const orc_sys_rule *r, const double *tm, int na, const double *src,
+                      double *R);
+/* seedm[nout][na], overwritten */
+void orc_sys_seed(const orc_sys_rule *r, const double *tm, int na, int nout, const double *R,
+                  double *seedm);
+/* Batched driver for a system rule: per point forward (all outputs), seed,
+ * adjoint; grad (zeroed first) summed over points, loss summed over points
+ * (may be NULL), tout[npts][nout][na] (may be NULL), src[npts][nres] (may
+ * be NULL).  Returns -1 on bad arguments. */
+int orc_grad_sys_batch(const orc_tables *t, int nlayer, const int *dims, const double *w,
+                       int npts, const double *X, const orc_sys_rule *rule,
+                       const double *src, double *grad, double *tout, double *loss,
+                       int nthreads);
+
 /* Forward only over a batch (net_eval_hod per point). */
 int orc_eval_batch(const orc_tables *t, int nlayer, const int *dims,
                    const double *w, int npts, const double *X, double *tout,

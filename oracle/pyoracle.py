@@ -8,7 +8,7 @@ The oracle restates the reference's table construction
 (lib/multi_index_bell_module.f90:128-429), its forward pass
 (lib/train_module.f90:241-335, lib/net_module.f90:295-375), its adjoint
 (lib/train_module.f90:360-450), the residual seeds of app/pinn_module.f90:
-32-65, the Adam step (lib/train_module.f90:656-683) and the primal natural
+32-65 and of its systems (:86-162), the Adam step (lib/train_module.f90:656-683) and the primal natural
 gradient step (app/optimizer_module.f90:221-522).
 """
 from __future__ import annotations
@@ -58,6 +58,7 @@ def lib():
         L.orc_grad_batch.argtypes = [vp, ci, P(ci), vp, ci, vp, vp, vp, vp, vp,
                                      vp, vp, ci]
         L.orc_eval_batch.argtypes = [vp, ci, P(ci), vp, ci, vp, vp, ci]
+        L.orc_grad_sys_batch.argtypes = [vp, ci, P(ci), vp, ci, vp, vp, vp, vp, vp, vp, ci]
         L.orc_adam_step.argtypes = [ci, vp, vp, vp, vp, cd, cd, cd, cd, ci, ci]
         L.orc_ngd_step.argtypes = [ci, ci, vp, vp, ci, cd, vp]
         _lib = L
@@ -72,6 +73,14 @@ class _SeedRule(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("nterm", ctypes.c_int),
                 ("coeff", ctypes.c_void_p), ("ind", ctypes.c_void_p),
                 ("nonlin", ctypes.c_void_p), ("fac", ctypes.c_double)]
+
+
+class _SysRule(ctypes.Structure):
+    _fields_ = [("nres", ctypes.c_int), ("nterm", ctypes.c_int),
+                ("res", ctypes.c_void_p), ("coeff", ctypes.c_void_p),
+                ("nfac", ctypes.c_void_p), ("comp", ctypes.c_void_p),
+                ("slot", ctypes.c_void_p), ("wres", ctypes.c_void_p),
+                ("fac", ctypes.c_double)]
 
 
 class Tables:
@@ -210,6 +219,36 @@ def grad_batch(tab: Tables, dims, w, X, kind=SEED_HALFSQ, terms=(), fac=1.0,
     if rc != 0:
         raise ValueError("oracle grad_batch: bad arguments")
     return g, T, loss.value, rows
+
+
+def grad_sys_batch(tab: Tables, dims, w, X, nres, terms, wres=None, fac=1.0, src=None,
+                   nthreads=0, want_t=True):
+    """Forward + system seed + adjoint (calc_sys_residual / set_sys_seed).
+
+    terms: (residual, coeff, [(component, slot), ...]) with 1-based residual,
+    component and slot.  src[npts][nres] may be None.  Returns (grad,
+    T[npts][nout][na] or None, loss)."""
+    X = np.ascontiguousarray(X, np.float64)
+    npts, nout = X.shape[0], dims[-1]
+    res = np.array([t[0] for t in terms], np.int32)
+    coeff = np.array([t[1] for t in terms], np.float64)
+    nfac = np.array([len(t[2]) for t in terms], np.int32)
+    comp = np.array([f[0] for t in terms for f in t[2]], np.int32)
+    slot = np.array([f[1] for t in terms for f in t[2]], np.int32)
+    wr = np.ascontiguousarray(wres, np.float64) if wres is not None else None
+    r = _SysRule(nres, len(terms), _p(res), _p(coeff), _p(nfac), _p(comp), _p(slot), _p(wr),
+                 float(fac))
+    sv = np.ascontiguousarray(src, np.float64) if src is not None else None
+    g = np.zeros(weight_count(dims))
+    T = np.zeros((npts, nout, tab.na)) if want_t else None
+    loss = ctypes.c_double(0.0)
+    w = np.ascontiguousarray(w, np.float64)
+    rc = lib().orc_grad_sys_batch(tab._h, len(dims), _dims(dims), _p(w), npts, _p(X),
+                                  ctypes.byref(r), _p(sv), _p(g), _p(T), ctypes.byref(loss),
+                                  nthreads)
+    if rc != 0:
+        raise ValueError("oracle grad_sys_batch: bad arguments")
+    return g, T, loss.value
 
 
 def eval_batch(tab: Tables, dims, w, X, nthreads=0):
