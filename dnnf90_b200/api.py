@@ -45,7 +45,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_launch_count", "dnnf90_profile_enable", "dnnf90_profile_read",
     "dnnf90_ngd_step_noalloc", "dnnf90_committee_step", "dnnf90_committee_info",
     "dnnf90_tune_report", "dnnf90_tune_force", "dnnf90_tabset_free",
-    "dnnf90_seed_rule_sys", "dnnf90_grad_sys_batch",
+    "dnnf90_seed_rule_sys", "dnnf90_grad_sys_batch", "dnnf90_grad_value_batch",
 ]
 
 _lib = None
@@ -130,6 +130,7 @@ def lib():
         "dnnf90_tune_force": [i, i],
         "dnnf90_seed_rule_sys": [i, i, pi, pd, pi, pi, pi, pd, d],
         "dnnf90_grad_sys_batch": [i, i, i, pd, pd, i, i, pd, pd],
+        "dnnf90_grad_value_batch": [i, i, i, pd, pd, d, i, pd],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -350,6 +351,15 @@ class Grad:
         call("dnnf90_grad_sys_batch", self.net.nid, self.net.tid, X.shape[0], _pd(X), _pd(sv),
              rule.rid, self.gid, _pd(loss), _pd(tm))
         return (float(loss[0]), tm) if want_t else float(loss[0])
+
+    def value_batch(self, X, y, coef=1.0):
+        """Value-only fit L = coef/2 sum (N(x) - y)^2 over a batch, added to
+        this accumulator (net_grad_batch).  Returns the loss."""
+        X, y = _f64(X), _f64(np.asarray(y, np.float64).reshape(-1))
+        loss = np.zeros(1)
+        call("dnnf90_grad_value_batch", self.net.nid, self.net.tid, X.shape[0], _pd(X), _pd(y),
+             float(coef), self.gid, _pd(loss))
+        return float(loss[0])
 
     def read(self):
         g = np.zeros(self.net.nw)

@@ -1088,6 +1088,35 @@ int dnnf90_grad_sys_batch(int nid, int tid, int npts, const double *x, const dou
                     loss, nullptr, nullptr, src, tm);
 }
 
+int dnnf90_grad_value_batch(int nid, int tid, int npts, const double *x, const double *y,
+                            double coef, int gid, double *loss) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, gid, true);
+  if (rc) return rc;
+  if (npts < 0 || (npts > 0 && (!x || !y))) return RC_BAD_ARG;
+  if (g_net[nid].dims[g_net[nid].nlayer - 1] != 1) {
+    set_error("dnnf90_grad_value_batch: the value fit is for a single output");
+    return RC_BAD_ARG;
+  }
+  if (loss) *loss = 0.0;
+  if (npts == 0) return RC_OK;
+  if ((rc = device_ready()) || (rc = grad_alloc(g_grd[gid]))) return rc;
+  // R = N(x) - y as a one-term system rule with source y: L = coef/2 R^2
+  RuleH r;
+  r.used = true;
+  r.r.kind = SEED_SYS;
+  r.r.fac = coef;
+  r.r.nres = 1;
+  r.r.sys = {0, 1, 0};
+  r.r.sfac = {0, 0};
+  r.r.coeff = {1.0};
+  r.r.wres = {1.0};
+  rc = host_train(nid, tid, npts, x, SEED_SYS, &r, nullptr, g_grd[gid].d, nullptr, loss, nullptr,
+                  nullptr, y, nullptr);
+  r.d.release();
+  return rc;
+}
+
 int dnnf90_jrow_batch(int nid, int tid, int npts, const double *x, int rid, double *rows,
                       double *resid, double *t) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);

@@ -80,6 +80,13 @@ int dnnf90_grad_rule_batch(int nid, int tid, int npts, const double *x,
  * lib/train_module.f90:459-475); new */
 int dnnf90_grad_sys_batch(int nid, int tid, int npts, const double *x, const double *src,
                           int rid, int gid, double *loss, double *tm);
+/* the value-only fit of net_grad_batch (lib/train_module.f90:525-631) over
+ * a batch: L = coef/2 sum_n (N(x_n) - y_n)^2 for a single-output network,
+ * dL/dw added to gid, loss (may be NULL) = L.  Only the value slot enters;
+ * a network on the table set that carries the value alone (the closure of
+ * {0}) evaluates no derivative. */
+int dnnf90_grad_value_batch(int nid, int tid, int npts, const double *x, const double *y,
+                            double coef, int gid, double *loss);
 /* Jacobian rows of a rule's residual, rows[npts][nweights]; resid[npts]
  * (the residual R per point) and t may be NULL */
 int dnnf90_jrow_batch(int nid, int tid, int npts, const double *x, int rid,

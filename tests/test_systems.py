@@ -6,7 +6,9 @@ differences of its own loss, and against the scalar PINN rule, which is the
 one-component special case.  On the GPU the device rule (forward -> seed on
 the device -> adjoint) is checked against the oracle on a steady 2-D
 Navier-Stokes system with outputs (u, v, p): two momentum residuals with
-products of one component and another's derivative, and continuity.
+products of one component and another's derivative, and continuity.  The
+value-only batched fit (net_grad_batch) is checked against a numpy
+restatement of the reference's batched backpropagation.
 """
 import numpy as np
 import pytest
@@ -143,3 +145,59 @@ def test_system_rule_argument_checks():
     with pytest.raises(api.Dnnf90Error):
         api.jacobian_rows(net, np.zeros((4, 2)), jr)
     rule.free(); jr.free(); g.free(); net.free(); ts.free()
+
+
+# ------------------------------------------------------ value-only fit
+
+
+def _value_fit_reference(dims, w, X, y, coef):
+    """net_grad_batch (lib/train_module.f90:525-631) restated in numpy, FP64:
+    forward with the bias channel, output deltas coef (N - y), deltas
+    back through W_{l+1}^T times tanh', gradient blocks D_l [1, Z_{l-1}]^T.
+    Weights in the flat layer layout (bias first)."""
+    Ws, off = [], 0
+    for l in range(1, len(dims)):
+        n, m = dims[l], dims[l - 1]
+        Ws.append(w[off:off + n * (m + 1)].reshape(n, m + 1))
+        off += n * (m + 1)
+    Z = [X]
+    for l, W in enumerate(Ws):
+        a = Z[-1] @ W[:, 1:].T + W[:, 0]
+        Z.append(np.tanh(a) if l < len(Ws) - 1 else a)
+    D = coef * (Z[-1] - y[:, None])
+    loss = 0.5 * coef * float(((Z[-1][:, 0] - y) ** 2).sum())
+    grads = [None] * len(Ws)
+    for l in range(len(Ws) - 1, -1, -1):
+        grads[l] = D.T @ np.hstack([np.ones((X.shape[0], 1)), Z[l]])
+        if l > 0:
+            D = (D @ Ws[l][:, 1:]) * (1.0 - Z[l] ** 2)
+    return np.concatenate([g.reshape(-1) for g in grads]), loss
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [0, 1])
+def test_value_fit_matches_the_batched_reference(prec):
+    from dnnf90_b200 import api
+    dims = [3, 64, 64, 1]
+    w = xavier_weights(dims, 12)
+    w[np.arange(len(w)) % 7 == 0] += 0.05
+    rng = np.random.default_rng(13)
+    X = rng.uniform(-1, 1, (5000, 3))
+    y = np.sin(X.sum(axis=1))
+    gref, lref = _value_fit_reference(dims, w, X, y, 0.8)
+    tol = 1e-12 if prec == 0 else 1e-5
+    # the value alone (closure of {0}), then a full K = 2 set: only the value slot enters
+    for seeds, k in (([[0, 0, 0]], 1), (None, 2)):
+        ts = api.TableSet(3, k, seeds)
+        net = api.Net(ts, dims, weights=w, precision=prec)
+        g = net.grad()
+        for rep in range(2):            # two calls add up
+            loss = g.value_batch(X, y, 0.8)
+            assert abs(loss - lref) <= tol * lref
+        assert rel_err(g.read(), 2 * gref) < tol, rel_err(g.read(), 2 * gref)
+        g.free(); net.free(); ts.free()
+    with pytest.raises(api.Dnnf90Error):               # a single output only
+        ts = api.TableSet(3, 1, [[0, 0, 0]])
+        net2 = api.Net(ts, [3, 8, 2], weights=xavier_weights([3, 8, 2], 1))
+        g2 = net2.grad()
+        g2.value_batch(X[:4], y[:4])
