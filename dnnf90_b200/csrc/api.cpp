@@ -142,10 +142,6 @@ size_t layer_off(const NetH &n, int l) {  // 1-based l in 2..nlayer
 int net_device(NetH &n, cudaStream_t st) {
   int rc = device_ready();
   if (rc) return rc;
-  if (n.ts.iact > 2) {
-    set_error("the Bessel activations are not on the device path");
-    return RC_UNSUPPORTED;
-  }
   if (!n.dt_ok) {
     if ((rc = upload_tables(n.ts, n.dt))) return rc;
     n.dt_ok = true;

@@ -17,7 +17,7 @@
 
 struct orc_tables {
   int d0, k, na;
-  int iact;  /* activation: 0 tanh, 1 sin, 2 erf (the tabset's iact) */
+  int iact;  /* activation: 0 tanh, 1 sin, 2 erf, 3 J0, 4 J1 (the tabset's iact) */
   int *alpha;   /* [na][d0] */
   int *deg;     /* [na] */
   int *ind_e1;  /* [d0], 1-based slot or 0 */
@@ -376,15 +376,84 @@ static void erf_derivs(double a, int nq, double *d) {
   for (int q = 1; q <= nq; ++q) d[q] = c2spi * ((q - 1) % 2 ? -1.0 : 1.0) * psi[q - 1];
 }
 
+/* J_0(x) .. J_n(x) (n <= 62): for |x| < 1e-5 two terms of the power
+ * series, otherwise Miller's backward recurrence
+ *   J_{k-1}(x) = (2k / x) J_k(x) - J_{k+1}(x)
+ * started at an even index well above max(n, |x|) and normalised by
+ *   J_0(x) + 2 sum_{k >= 1} J_{2k}(x) = 1
+ * (Abramowitz & Stegun 9.1.27, 9.1.46; the method of 9.12), with a
+ * rescale whenever the unnormalised values grow past 1e200.  Negative
+ * arguments by J_n(-x) = (-1)^n J_n(x), as the reference's besj_series
+ * wrapper does (lib/bessel_module.f90:50-72).  The reference computes the
+ * values with Zhang and Jin's jyna; this is an independent method, pinned
+ * against scipy in the tests. */
+void orc_besj_all(int n, double x, double *bj) {
+  const double ax = fabs(x);
+  if (ax < 1e-5) {
+    // two terms of the power series, (x/2)^k / k! (1 - (x/2)^2 / (k + 1));
+    // the next term is below 1e-21 of the first
+    const double h = 0.5 * x;
+    double p = 1.0;
+    for (int k = 0; k <= n; ++k) {
+      bj[k] = p * (1.0 - h * h / (double)(k + 1));
+      p = p * h / (double)(k + 1);
+    }
+    return;
+  }
+  const double top = ax > n ? ax : (double)n;
+  int m = (int)top + 30 + (int)(3.0 * sqrt(top));
+  m += m & 1;
+  double jp1 = 0.0, j = 1.0, sum = 0.0;
+  for (int k = m; k >= 1; --k) {
+    const double jm1 = (2.0 * k / ax) * j - jp1;
+    jp1 = j;
+    j = jm1; /* J_{k-1} */
+    if (k - 1 <= n) bj[k - 1] = j;
+    if (k - 1 >= 2 && !((k - 1) & 1)) sum += 2.0 * j;
+    if (fabs(j) > 1e200) {
+      j *= 1e-200;
+      jp1 *= 1e-200;
+      sum *= 1e-200;
+      for (int i = k - 1; i <= n; ++i) bj[i] *= 1e-200;
+    }
+  }
+  sum += j;
+  for (int i = 0; i <= n; ++i) bj[i] /= sum;
+  if (x < 0.0)
+    for (int i = 1; i <= n; i += 2) bj[i] = -bj[i];
+}
+
+/* besj0_derivs / besj1_derivs (lib/multi_index_bell_module.f90:757-826):
+ *   J_0^(q) = ((-1)^q / 2^q) sum_k (-1)^k C(q,k) J_{q-2k},
+ *   J_1^(q) = ((-1)^q / 2^q) sum_k (-1)^k C(q,k) J_{1+q-2k},
+ * J_{-n} = (-1)^n J_n, the binomials built as C(q,k+1) = C(q,k)(q-k)/(k+1) */
+static void besj_derivs(int shift, double a, int nq, double *d) {
+  double bj[64];
+  orc_besj_all(nq + shift, a, bj);
+  for (int q = 0; q <= nq; ++q) {
+    double term = 0.0, c = 1.0;
+    for (int k = 0; k <= q; ++k) {
+      const int m = shift + q - 2 * k;
+      const double sk = (k & 1) ? -1.0 : 1.0;
+      if (m >= 0) term = term + sk * c * bj[m];
+      else term = term + sk * c * ((-m) & 1 ? -1.0 : 1.0) * bj[-m];
+      c = c * (double)(q - k) / (double)(k + 1);
+    }
+    d[q] = (q & 1 ? -1.0 : 1.0) * term / ldexp(1.0, q);
+  }
+}
+
 /* act_derivs_ts (:723-741): the activation contract, sigma^(q), q = 0..nq */
 void orc_act_derivs(const orc_tables *t, double a, int nq, double *d) {
   if (t->iact == 1) sin_derivs(a, nq, d);
   else if (t->iact == 2) erf_derivs(a, nq, d);
+  else if (t->iact == 3) besj_derivs(0, a, nq, d);
+  else if (t->iact == 4) besj_derivs(1, a, nq, d);
   else orc_tanh_derivs(t, a, nq, d);
 }
 
 int orc_tables_set_activation(orc_tables *t, int iact) {
-  if (iact < 0 || iact > 2) return -1;
+  if (iact < 0 || iact > 4) return -1;
   t->iact = iact;
   return 0;
 }

@@ -49,11 +49,13 @@ void orc_tables_copy(const orc_tables *t, int *alpha, int *deg, int *ind_e1,
  * lib/multi_index_bell_module.f90:852-867) */
 void orc_tanh_derivs(const orc_tables *t, double a, int nq, double *d);
 /* sigma^(q)(a) for the table set's activation (act_derivs_ts, :723-741):
- * 0 tanh, 1 sin (:745-755), 2 erf (:831-850) */
+ * 0 tanh, 1 sin (:745-755), 2 erf (:831-850), 3 J0 and 4 J1 (:757-826) */
 void orc_act_derivs(const orc_tables *t, double a, int nq, double *d);
 /* select the activation of a table set (dnnf90_tabset_activation); 0 on
- * success, -1 for codes outside 0..2 (the Bessel functions are not restated) */
+ * success, -1 for codes outside 0..4 */
 int orc_tables_set_activation(orc_tables *t, int iact);
+/* J_0(x) .. J_n(x), n <= 62, into bj[0..n] (Miller's backward recurrence) */
+void orc_besj_all(int n, double x, double *bj);
 
 /* Network weights: layers l = 2..nlayer concatenated, each a row-major
  * [dims[l-1]][dims[l-2]+1] block whose row j is the bias followed by the

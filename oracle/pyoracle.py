@@ -51,6 +51,7 @@ def lib():
         L.orc_tables_copy.argtypes = [vp] + [vp] * 14
         L.orc_tanh_derivs.argtypes = [vp, cd, ci, vp]
         L.orc_act_derivs.argtypes = [vp, cd, ci, vp]
+        L.orc_besj_all.argtypes = [ci, cd, vp]
         L.orc_tables_set_activation.argtypes = [vp, ci]
         L.orc_weight_count.argtypes = [ci, P(ci)]
         L.orc_eval_point.argtypes = [vp, ci, P(ci), vp, vp, vp, vp]
@@ -249,6 +250,13 @@ def grad_sys_batch(tab: Tables, dims, w, X, nres, terms, wres=None, fac=1.0, src
     if rc != 0:
         raise ValueError("oracle grad_sys_batch: bad arguments")
     return g, T, loss.value
+
+
+def besj_all(n: int, x: float) -> np.ndarray:
+    """J_0(x) .. J_n(x) (the oracle's Miller recurrence)."""
+    bj = np.zeros(n + 1)
+    lib().orc_besj_all(int(n), float(x), _p(bj))
+    return bj
 
 
 def eval_batch(tab: Tables, dims, w, X, nthreads=0):

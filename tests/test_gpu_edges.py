@@ -1,5 +1,5 @@
 """Edge cases of the device path against the oracle, through the C ABI:
-the sin and erf activations, first-order tables (K = 1), a single input
+the sin, erf and Bessel J0 / J1 activations, first-order tables (K = 1), a single input
 (D0 = 1), one point, several outputs, and a closure set whose top degree
 is below K."""
 import numpy as np
@@ -62,10 +62,9 @@ def test_closure_below_k():
     _check(2, 4, [[2, 0], [0, 1]], [2, 32, 32, 1], 33, api.PREC_F64, seed=6)
 
 
-def test_bessel_activation_is_refused():
-    ts = api.TableSet(2, 2, activation=3)
-    net = api.Net(ts, [2, 8, 1], weights=xavier_weights([2, 8, 1], 1))
-    with pytest.raises(api.Dnnf90Error) as e:
-        net.eval(np.zeros((2, 2)))
-    assert e.value.rc == -5
-    net.free()
+@pytest.mark.parametrize("prec", [api.PREC_F64, api.PREC_SPLIT])
+@pytest.mark.parametrize("activation", [3, 4])
+def test_bessel_activations(activation, prec):
+    # J0 / J1 with their derivatives from J_0 .. J_{K+2}, K = 7 (nine orders)
+    _check(2, 7, None, [2, 32, 32, 1], 48, prec, activation, seed=activation)
+    _check(3, 4, None, [3, 32, 32, 1], 64, prec, activation, seed=10 + activation)

@@ -131,3 +131,19 @@ def test_oracle_sin_and_erf_derivatives():
         ref = [math.erf(a), g, -2 * a * g, (4 * a * a - 2) * g, (12 * a - 8 * a ** 3) * g,
                (16 * a ** 4 - 48 * a * a + 12) * g]
         assert np.allclose(d, ref, rtol=1e-13, atol=1e-15), (a, d, ref)
+
+
+def test_bessel_values_and_derivatives_against_scipy():
+    """The oracle's J_n (Miller's backward recurrence) and the J0 / J1
+    derivative combinations of besj0_derivs / besj1_derivs
+    (lib/multi_index_bell_module.f90:757-826) against scipy."""
+    import scipy.special as sp
+    xs = np.concatenate([np.linspace(-40, 40, 801), [0.0, 1e-300, 1e-30, 1e-10, -1e-6, 1e-3]])
+    for x in xs:
+        assert np.max(np.abs(po.besj_all(12, x) - sp.jv(np.arange(13), x))) < 2e-15, x
+    for act, order in ((3, 0), (4, 1)):
+        tab = po.Tables(2, 7, activation=act)
+        for a in (-7.3, -1.2, 0.0, 0.4, 3.3, 15.0):
+            d = tab.act_derivs(a, 9)
+            ref = [sp.jvp(order, a, q) for q in range(10)]
+            assert np.max(np.abs(d - ref)) < 1e-14, (act, a)
