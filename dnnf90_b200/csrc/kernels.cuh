@@ -51,6 +51,27 @@ static __device__ __noinline__ void besj_all(int n, double x, double *bj) {
     for (int i = 1; i <= n; i += 2) bj[i] = -bj[i];
 }
 
+// J0 (shift 0) or J1 (shift 1) and its derivatives to order nq: the
+// binomial combinations of besj0_derivs / besj1_derivs
+// (lib/multi_index_bell_module.f90:757-826),
+//   J_s^(q) = ((-1)^q / 2^q) sum_k (-1)^k C(q,k) J_{s+q-2k},  J_{-n} = (-1)^n J_n.
+// Not inlined, so that its locals stay out of the kernels that never use it.
+static __device__ __noinline__ void besj_derivs(int shift, double a, int nq, double *d) {
+  double bj[KMAX + 4];
+  besj_all(nq + shift, a, bj);
+  for (int q = 0; q <= nq; ++q) {
+    double term = 0.0, c = 1.0;
+    for (int kk = 0; kk <= q; ++kk) {
+      const int m = shift + q - 2 * kk;
+      const double sk = (kk & 1) ? -1.0 : 1.0;
+      if (m >= 0) term = term + sk * c * bj[m];
+      else term = term + sk * c * ((-m) & 1 ? -1.0 : 1.0) * bj[-m];
+      c = c * (double)(q - kk) / (double)(kk + 1);
+    }
+    d[q] = (q & 1 ? -1.0 : 1.0) * term / ldexp(1.0, q);
+  }
+}
+
 // sigma^(q)(a), q = 0..k+1, in FP64.  tanh: Horner on the integer
 // polynomials P_q(t), t = tanh(a) (tanh_derivs_ts,
 // lib/multi_index_bell_module.f90:852-867); sin: sin(a + q pi/2)
@@ -61,20 +82,11 @@ __device__ __forceinline__ void sigma_derivs(int iact, const double *__restrict_
                                              int k, double a, double *d) {
   const int nq = k + 1;
   if (iact == 3 || iact == 4) {
-    const int shift = iact - 3;
-    double bj[KMAX + 4];
-    besj_all(nq + shift, a, bj);
-    for (int q = 0; q <= nq; ++q) {
-      double term = 0.0, c = 1.0;
-      for (int kk = 0; kk <= q; ++kk) {
-        const int m = shift + q - 2 * kk;
-        const double sk = (kk & 1) ? -1.0 : 1.0;
-        if (m >= 0) term = term + sk * c * bj[m];
-        else term = term + sk * c * ((-m) & 1 ? -1.0 : 1.0) * bj[-m];
-        c = c * (double)(q - kk) / (double)(kk + 1);
-      }
-      d[q] = (q & 1 ? -1.0 : 1.0) * term / ldexp(1.0, q);
-    }
+    // the callee fills its own array, so d itself is never passed by
+    // address and stays in registers wherever k is a compile-time constant
+    double tmp[KMAX + 2];
+    besj_derivs(iact - 3, a, nq, tmp);
+    for (int q = 0; q <= nq; ++q) d[q] = tmp[q];
     return;
   }
   if (iact == 1) {
