@@ -46,6 +46,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_ngd_step_noalloc", "dnnf90_committee_step", "dnnf90_committee_info",
     "dnnf90_tune_report", "dnnf90_tune_force", "dnnf90_tabset_free",
     "dnnf90_seed_rule_sys", "dnnf90_grad_sys_batch", "dnnf90_grad_value_batch",
+    "dnnf90_ngd_step_dual",
 ]
 
 _lib = None
@@ -112,6 +113,7 @@ def lib():
         "dnnf90_jrow_batch": [i, i, i, pd, i, pd, pd, pd],
         "dnnf90_grad_read": [i, pd],
         "dnnf90_ngd_step": [i, i, pd, pd, i, d, i, pd],
+        "dnnf90_ngd_step_dual": [i, i, pd, pd, i, d, i, pd],
         "dnnf90_set_weights_dev": [i, p, p],
         "dnnf90_forward_dev": [i, i, i, p, p, i, p],
         "dnnf90_backward_dev": [i, i, i, p, p, p, p],
@@ -422,11 +424,13 @@ def jacobian_rows(net: Net, X, rule: SeedRule):
     return rows, resid, t
 
 
-def ngd_step(net: Net, rows, b, nb: int, mu: float, prec: int = PREC_F64):
+def ngd_step(net: Net, rows, b, nb: int, mu: float, prec: int = PREC_F64, dual: bool = False):
+    """Damped Gauss-Newton step u = (J^T J / nb + mu I)^{-1} (b / nb); dual
+    takes the Gram-space route (dnnf90_ngd_step_dual), for nrow < nw."""
     rows, b = _f64(rows), _f64(b)
     u = np.zeros(net.nw)
-    call("dnnf90_ngd_step", net.nid, rows.shape[0], _pd(rows), _pd(b), int(nb), float(mu),
-         int(prec), _pd(u))
+    call("dnnf90_ngd_step_dual" if dual else "dnnf90_ngd_step", net.nid, rows.shape[0],
+         _pd(rows), _pd(b), int(nb), float(mu), int(prec), _pd(u))
     return u
 
 

@@ -1139,8 +1139,8 @@ int dnnf90_grad_read(int gid, double *g) {
   return ck(cudaMemcpy(g, gr.d, sizeof(double) * gr.nw, cudaMemcpyDeviceToHost), "D2H");
 }
 
-int dnnf90_ngd_step(int nid, int nrow, const double *rows, const double *b, int nb,
-                    double mu, int prec, double *u) {
+static int ngd_host(int nid, int nrow, const double *rows, const double *b, int nb, double mu,
+                    int prec, double *u, bool dual) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (bad_net(nid) || nrow < 1 || nb < 1 || !rows || !b || !u) return RC_BAD_ARG;
   if (prec != PREC_F64 && prec != PREC_SPLIT) return RC_BAD_ARG;
@@ -1156,11 +1156,23 @@ int dnnf90_ngd_step(int nid, int nrow, const double *rows, const double *b, int 
   du = db + nw;
   rc = ck(cudaMemcpy(dr, rows, sizeof(double) * (size_t)nrow * nw, cudaMemcpyHostToDevice), "H2D");
   if (!rc) rc = ck(cudaMemcpy(db, b, sizeof(double) * nw, cudaMemcpyHostToDevice), "H2D");
-  if (!rc) rc = ngd_device(dr, nrow, nw, db, nb, mu, du, prec, nullptr);
+  if (!rc)
+    rc = dual ? ngd_device_dual(dr, nrow, nw, db, nb, mu, du, prec, nullptr)
+              : ngd_device(dr, nrow, nw, db, nb, mu, du, prec, nullptr);
   if (!rc) rc = ck(cudaMemcpy(u, du, sizeof(double) * nw, cudaMemcpyDeviceToHost), "D2H");
   cudaFree(dr);
   cudaFree(db);
   return rc;
+}
+
+int dnnf90_ngd_step(int nid, int nrow, const double *rows, const double *b, int nb,
+                    double mu, int prec, double *u) {
+  return ngd_host(nid, nrow, rows, b, nb, mu, prec, u, false);
+}
+
+int dnnf90_ngd_step_dual(int nid, int nrow, const double *rows, const double *b, int nb,
+                         double mu, int prec, double *u) {
+  return ngd_host(nid, nrow, rows, b, nb, mu, prec, u, true);
 }
 
 // ------------------------------------------------------------- device pointers

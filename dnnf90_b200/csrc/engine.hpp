@@ -189,6 +189,9 @@ int adam_device(double *w, const double *g, double *m, double *v, int nw,
 // (prec), then Cholesky-factored and solved in FP64.
 int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
                double mu, double *u, int prec, cudaStream_t st);
+// the same step by the dual (Gram-space) route, app/optimizer_module.f90:408-446
+int ngd_device_dual(const double *rows, int nrow, int nw, const double *b, int nb, double mu,
+                    double *u, int prec, cudaStream_t st);
 
 // The same step on caller device buffers with the metric in a fixed
 // scratch area of the library (no device allocation); nw <= ngd_noalloc_maxw().

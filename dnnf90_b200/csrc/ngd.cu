@@ -229,67 +229,183 @@ __global__ void k_rows_f32(const double *rows, int nrow, int nw, float *J, int l
   }
 }
 
-int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
-               double mu, double *u, int prec, cudaStream_t st) {
-  double *G = nullptr;
-  int *info = nullptr;
-  CKN(cudaMalloc(&G, sizeof(double) * (size_t)nw * nw));
-  CKN(cudaMalloc(&info, sizeof(int)));
-  CKN(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)nw * nw, st));
-  CKN(cudaMemsetAsync(info, 0, sizeof(int), st));
-  const int tiles = (nw + 63) / 64;
+// G[nc][nc] (lower triangle, zeroed here) = A^T A for A[nr][nc]: on the
+// tensor cores in the split precision (split-BF16 products of an FP32 copy,
+// FP32 accumulation per 512 rows, FP64 across them), else FP64 tiles
+static int gram(const double *A, int nr, int nc, double *G, int prec, cudaStream_t st) {
+  CKN(cudaMemsetAsync(G, 0, sizeof(double) * (size_t)nc * nc, st));
   int rc = RC_UNSUPPORTED;
   if (prec == PREC_SPLIT && gemm_tc_available()) {
-    // the metric on the tensor cores: split-BF16 products of the FP32 rows
-    // with FP32 accumulation per 512 rows, FP64 across them
-    const int ldj = (nw + 3) / 4 * 4;
+    const int ldj = (nc + 3) / 4 * 4;
     float *J = nullptr;
-    if (cudaMalloc(&J, sizeof(float) * (size_t)nrow * ldj) == cudaSuccess) {
-      LAUNCH("k_rows_f32", st, k_rows_f32<<<1024, 256, 0, st>>>(rows, nrow, nw, J, ldj));
-      rc = gemm_tc_syrk(J, nrow, nw, ldj, G, st);
+    if (cudaMalloc(&J, sizeof(float) * (size_t)nr * ldj) == cudaSuccess) {
+      LAUNCH("k_rows_f32", st, k_rows_f32<<<1024, 256, 0, st>>>(A, nr, nc, J, ldj));
+      rc = gemm_tc_syrk(J, nr, nc, ldj, G, st);
       cudaFree(J);
     }
   }
-  if (rc == RC_UNSUPPORTED) {
-    rc = RC_OK;
-    int rchunk = std::max(64, (nrow + 7) / 8);
-    rchunk = (rchunk + 15) / 16 * 16;
-    dim3 grid(tiles, tiles, (nrow + rchunk - 1) / rchunk);
-    LAUNCH("k_syrk_f64", st, k_syrk_f64<<<grid, 256, 0, st>>>(rows, nrow, nw, G, rchunk));
-    CKN(cudaGetLastError());
-  }
-  if (rc) {
-    cudaFree(G);
-    cudaFree(info);
-    return rc;
-  }
-  LAUNCH("k_scale_damp", st, k_scale_damp<<<1024, 256, 0, st>>>(G, nw, 1.0 / (double)nb, mu, b, u));
+  if (rc != RC_UNSUPPORTED) return rc;
+  const int tiles = (nc + 63) / 64;
+  int rchunk = std::max(64, (nr + 7) / 8);
+  rchunk = (rchunk + 15) / 16 * 16;
+  dim3 grid(tiles, tiles, (nr + rchunk - 1) / rchunk);
+  LAUNCH("k_syrk_f64", st, k_syrk_f64<<<grid, 256, 0, st>>>(A, nr, nc, G, rchunk));
   CKN(cudaGetLastError());
-  for (int k0 = 0; k0 < nw; k0 += NB) {
-    const int nbk = std::min(NB, nw - k0);
-    LAUNCH("k_potrf_diag", st, k_potrf_diag<<<1, 256, 0, st>>>(G, nw, k0, nbk, info));
+  return RC_OK;
+}
+
+// Cholesky factorization of the damped G[n][n] (lower triangle) and the
+// solve G x = x; -1 with the first non-positive pivot in the error text
+static int chol_solve(double *G, int n, double *x, int *info, cudaStream_t st) {
+  CKN(cudaMemsetAsync(info, 0, sizeof(int), st));
+  for (int k0 = 0; k0 < n; k0 += NB) {
+    const int nbk = std::min(NB, n - k0);
+    LAUNCH("k_potrf_diag", st, k_potrf_diag<<<1, 256, 0, st>>>(G, n, k0, nbk, info));
     CKN(cudaGetLastError());
-    if (k0 + nbk < nw) {
-      const int rem = nw - k0 - nbk;
-      LAUNCH("k_trsm_panel", st, k_trsm_panel<<<std::max(1, std::min(256, (rem + 127) / 128)), 128, 0, st>>>(G, nw, k0, nbk));
+    if (k0 + nbk < n) {
+      const int rem = n - k0 - nbk;
+      LAUNCH("k_trsm_panel", st, k_trsm_panel<<<std::max(1, std::min(256, (rem + 127) / 128)), 128, 0, st>>>(G, n, k0, nbk));
       CKN(cudaGetLastError());
       const int tt = (rem + 63) / 64;
-      LAUNCH("k_syrk_trail", st, k_syrk_trail<<<dim3(tt, tt), 256, 0, st>>>(G, nw, k0, nbk));
+      LAUNCH("k_syrk_trail", st, k_syrk_trail<<<dim3(tt, tt), 256, 0, st>>>(G, n, k0, nbk));
       CKN(cudaGetLastError());
     }
   }
-  LAUNCH("k_chol_solve", st, k_chol_solve<<<1, 1024, 0, st>>>(G, nw, u));
+  LAUNCH("k_chol_solve", st, k_chol_solve<<<1, 1024, 0, st>>>(G, n, x));
   CKN(cudaGetLastError());
   int hinfo = 0;
   CKN(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
   CKN(cudaStreamSynchronize(st));
-  cudaFree(G);
-  cudaFree(info);
   if (hinfo) {
     set_error("the damped metric is not positive definite at column " + std::to_string(hinfo));
     return RC_BAD_ARG;
   }
   return RC_OK;
+}
+
+int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
+               double mu, double *u, int prec, cudaStream_t st) {
+  double *G = nullptr;
+  int *info = nullptr;
+  CKN(cudaMalloc(&G, sizeof(double) * (size_t)nw * nw));
+  if (cudaMalloc(&info, sizeof(int)) != cudaSuccess) {
+    cudaFree(G);
+    set_error("cudaMalloc failed for the metric pivot flag");
+    return RC_NOMEM;
+  }
+  int rc = gram(rows, nrow, nw, G, prec, st);
+  if (!rc) {
+    LAUNCH("k_scale_damp", st, k_scale_damp<<<1024, 256, 0, st>>>(G, nw, 1.0 / (double)nb, mu, b, u));
+    rc = cudaGetLastError() == cudaSuccess ? RC_OK : RC_DEVICE;
+  }
+  if (!rc) rc = chol_solve(G, nw, u, info, st);
+  cudaFree(G);
+  cudaFree(info);
+  return rc;
+}
+
+// ------------------------------------------------- dual (Gram-space) route
+// The dual route of app/optimizer_module.f90:408-446: with G = J^T J / nb
+// and the damping mu, the push-through identity gives
+//   (G + mu I)^{-1} b' = (1 / mu) (b' - J^T K^{-1} (J b') / nb),
+//   K = mu I + J J^T / nb  (nrow x nrow),  b' = b / nb,
+// so the nw x nw metric is never formed: an nrow x nrow solve and two
+// passes over the rows.  The step is the primal one to roundoff.
+
+// T[nc][nr] = A^T for A[nr][nc], 32 x 32 tiles through shared memory
+__global__ void k_transpose(const double *A, int nr, int nc, double *T) {
+  __shared__ double tile[32][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int r = r0 + i, c = c0 + threadIdx.x;
+    tile[i][threadIdx.x] = (r < nr && c < nc) ? A[(size_t)r * nc + c] : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int c = c0 + i, r = r0 + threadIdx.x;
+    if (c < nc && r < nr) T[(size_t)c * nr + r] = tile[threadIdx.x][i];
+  }
+}
+
+// K = K / nb + mu I on the lower triangle
+__global__ void k_damp(double *K, int n, double inv_nb, double mu) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)n * n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e / n), j = (int)(e - (size_t)i * n);
+    if (j > i) continue;
+    K[e] = K[e] * inv_nb + (i == j ? mu : 0.0);
+  }
+}
+
+// y[r] = alpha sum_i J[r][i] x[i], one warp per row
+__global__ void k_rows_dot(const double *J, int nrow, int nw, const double *x, double alpha,
+                           double *y) {
+  const int lane = threadIdx.x & 31;
+  for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nrow;
+       r += gridDim.x * (blockDim.x >> 5)) {
+    double s = 0.0;
+    for (int i = lane; i < nw; i += 32) s += J[(size_t)r * nw + i] * x[i];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[r] = alpha * s;
+  }
+}
+
+// u[i] = (b[i] / nb - (1 / nb) sum_r J[r][i] y[r]) / mu
+__global__ void k_dual_step(const double *J, int nrow, int nw, const double *b, const double *y,
+                            double inv_nb, double inv_mu, double *u) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int r = 0; r < nrow; ++r) s += J[(size_t)r * nw + i] * y[r];
+    u[i] = (b[i] * inv_nb - s * inv_nb) * inv_mu;
+  }
+}
+
+int ngd_device_dual(const double *rows, int nrow, int nw, const double *b, int nb, double mu,
+                    double *u, int prec, cudaStream_t st) {
+  if (!(mu > 0.0)) {
+    set_error("the dual natural-gradient step needs a positive damping mu");
+    return RC_BAD_ARG;
+  }
+  double *K = nullptr, *JT = nullptr, *y = nullptr;
+  int *info = nullptr;
+  auto cleanup = [&]() {
+    if (K) cudaFree(K);
+    if (JT) cudaFree(JT);
+    if (y) cudaFree(y);
+    if (info) cudaFree(info);
+  };
+  if (cudaMalloc(&K, sizeof(double) * (size_t)nrow * nrow) != cudaSuccess ||
+      cudaMalloc(&JT, sizeof(double) * (size_t)nrow * nw) != cudaSuccess ||
+      cudaMalloc(&y, sizeof(double) * (size_t)nrow) != cudaSuccess ||
+      cudaMalloc(&info, sizeof(int)) != cudaSuccess) {
+    cleanup();
+    set_error("cudaMalloc failed for the dual natural-gradient step");
+    return RC_NOMEM;
+  }
+  // K = J J^T: the Gram product of the transposed rows, always in FP64.
+  // The step ends with (b' - J^T y / nb) / mu, a cancellation divided by a
+  // small damping, which magnifies the rounding of split-BF16 products in K
+  // far past what the primal solve sees (measured backward error 6e-3
+  // against 1e-7); K is only nrow x nrow, so FP64 costs little here.
+  (void)prec;
+  LAUNCH("k_transpose", st, k_transpose<<<dim3((nw + 31) / 32, (nrow + 31) / 32), dim3(32, 8), 0, st>>>(rows, nrow, nw, JT));
+  int rc = cudaGetLastError() == cudaSuccess ? RC_OK : RC_DEVICE;
+  if (!rc) rc = gram(JT, nw, nrow, K, PREC_F64, st);
+  if (!rc) {
+    const double inv_nb = 1.0 / (double)nb;
+    LAUNCH("k_damp", st, k_damp<<<1024, 256, 0, st>>>(K, nrow, inv_nb, mu));
+    LAUNCH("k_rows_dot", st, k_rows_dot<<<std::max(1, std::min(4096, (nrow + 7) / 8)), 256, 0, st>>>(rows, nrow, nw, b, inv_nb, y));
+    rc = cudaGetLastError() == cudaSuccess ? RC_OK : RC_DEVICE;
+    if (!rc) rc = chol_solve(K, nrow, y, info, st);
+    if (!rc) {
+      LAUNCH("k_dual_step", st, k_dual_step<<<std::max(1, (nw + 255) / 256), 256, 0, st>>>(rows, nrow, nw, b, y, inv_nb, 1.0 / mu, u));
+      rc = cudaGetLastError() == cudaSuccess ? RC_OK : RC_DEVICE;
+      if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = RC_DEVICE;
+    }
+  }
+  if (rc == RC_DEVICE) set_error("the dual natural-gradient step failed on the device");
+  cleanup();
+  return rc;
 }
 
 // ------------------------------------------------- no-allocation variant

@@ -99,6 +99,15 @@ int dnnf90_grad_read(int gid, double *g);
  * in FP64; the solve is an FP64 Cholesky factorization. */
 int dnnf90_ngd_step(int nid, int nrow, const double *rows, const double *b,
                     int nb, double mu, int prec, double *u);
+/* the same step by the dual (Gram-space) route of app/optimizer_module.f90:
+ * 408-446: K = mu I + J J^T / nb (nrow x nrow), y = K^{-1} J (b / nb),
+ * u = (b / nb - J^T y / nb) / mu.  The nw x nw metric is never formed, so
+ * it is the route for nrow < nw; the step equals the primal one to
+ * roundoff.  K is formed in FP64 whatever prec says: the final division
+ * by mu after a cancellation would magnify split-product rounding.
+ * mu > 0. */
+int dnnf90_ngd_step_dual(int nid, int nrow, const double *rows, const double *b,
+                         int nb, double mu, int prec, double *u);
 
 /* ---- device-pointer entry points (pointers to device memory; stream is
  * a cudaStream_t, NULL for the legacy default stream).  On the split path

@@ -228,3 +228,41 @@ def test_ngd_step_at_heat_scale():
         berr = np.linalg.norm(G @ u - bn) / (g2 * np.linalg.norm(u) + np.linalg.norm(bn))
         assert berr < bound, (prec, berr)
     r.free(); net.free()
+
+
+def test_ngd_dual_route_equals_the_primal_step():
+    """The Gram-space route (app/optimizer_module.f90:408-446) on fewer rows
+    than weights: 512 heat-residual rows, 4481 weights.  The step must be the
+    primal one to roundoff, and both must meet the primal backward-error
+    bound on the FP64 system."""
+    dims = [3, 64, 64, 1]
+    seeds = [[1, 0, 0], [0, 2, 0], [0, 0, 2]]
+    ts = api.TableSet(3, 2, seeds)
+    terms = [(1.0, ts.slot((1, 0, 0)), 0), (-1.0, ts.slot((0, 2, 0)), 0),
+             (-1.0, ts.slot((0, 0, 2)), 0)]
+    w = xavier_weights(dims, 6)
+    X = np.random.default_rng(9).uniform(0, 1, (512, 3))
+    net = _net(ts, dims, w, api.PREC_F64)
+    r = api.SeedRule(api.SEED_JROW, terms)
+    rows, resid, _ = api.jacobian_rows(net, X, r)
+    nb, mu = len(X), 1e-3
+    b = (resid[:, None] * rows).sum(axis=0)
+    G = rows.T @ rows / nb + mu * np.eye(rows.shape[1])
+    bn = b / nb
+    g2 = np.linalg.norm(rows, 2) ** 2 / nb + mu
+    # the routes agree to roundoff amplified by the conditioning (||G|| /
+    # mu); the dual route forms its nrow x nrow Gram matrix in FP64 in both
+    # precisions, so it meets the FP64 bound; the split primal metric is
+    # judged by backward error
+    up = api.ngd_step(net, rows, b, nb, mu, api.PREC_F64)
+    ud = api.ngd_step(net, rows, b, nb, mu, api.PREC_F64, dual=True)
+    uds = api.ngd_step(net, rows, b, nb, mu, api.PREC_SPLIT, dual=True)
+    ups = api.ngd_step(net, rows, b, nb, mu, api.PREC_SPLIT)
+    assert rel_err(ud, up) < 1e-9, rel_err(ud, up)
+    assert rel_err(uds, ud) < 1e-9     # FP64 both; atomics order the sums differently
+    for u, bound in ((up, 1e-12), (ud, 1e-12), (ups, 1e-6)):
+        berr = np.linalg.norm(G @ u - bn) / (g2 * np.linalg.norm(u) + np.linalg.norm(bn))
+        assert berr < bound, berr
+    with pytest.raises(api.Dnnf90Error):
+        api.ngd_step(net, rows, b, nb, 0.0, api.PREC_F64, dual=True)   # mu must be > 0
+    r.free(); net.free(); ts.free()
