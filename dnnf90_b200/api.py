@@ -46,7 +46,8 @@ EXTENSION_SYMBOLS = [
     "dnnf90_ngd_step_noalloc", "dnnf90_committee_step", "dnnf90_committee_info",
     "dnnf90_tune_report", "dnnf90_tune_force", "dnnf90_tabset_free",
     "dnnf90_seed_rule_sys", "dnnf90_grad_sys_batch", "dnnf90_grad_value_batch",
-    "dnnf90_ngd_step_dual",
+    "dnnf90_ngd_step_dual", "dnnf90_kf_create", "dnnf90_kf_free", "dnnf90_kf_update_rows",
+    "dnnf90_kf_update_rows_dev", "dnnf90_kf_read",
 ]
 
 _lib = None
@@ -133,6 +134,11 @@ def lib():
         "dnnf90_seed_rule_sys": [i, i, pi, pd, pi, pi, pi, pd, d],
         "dnnf90_grad_sys_batch": [i, i, i, pd, pd, i, i, pd, pd],
         "dnnf90_grad_value_batch": [i, i, i, pd, pd, d, i, pd],
+        "dnnf90_kf_create": [i, d, d, d, i, d, d],
+        "dnnf90_kf_free": [i],
+        "dnnf90_kf_update_rows": [i, i, pd, pd, pd],
+        "dnnf90_kf_update_rows_dev": [i, i, p, p, p, p, p],
+        "dnnf90_kf_read": [i, pd, pi, pd],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -432,6 +438,49 @@ def ngd_step(net: Net, rows, b, nb: int, mu: float, prec: int = PREC_F64, dual: 
     call("dnnf90_ngd_step_dual" if dual else "dnnf90_ngd_step", net.nid, rows.shape[0],
          _pd(rows), _pd(b), int(nb), float(mu), int(prec), _pd(u))
     return u
+
+
+class Kalman:
+    """Extended Kalman filter on a network's weights (kalman_t,
+    lib/kalman_module.f90): dnnf90_kf_create / dnnf90_kf_update_rows."""
+
+    def __init__(self, net: Net, p0: float, lam_ini: float, lam0: float,
+                 decoupled: bool = False, q: float = 0.0, gate: float = 0.0):
+        self.net = net
+        self.decoupled = bool(decoupled)
+        self.kid = check("dnnf90_kf_create",
+                         lib().dnnf90_kf_create(net.nid, float(p0), float(lam_ini),
+                                                float(lam0), int(decoupled), float(q),
+                                                float(gate)))
+
+    def update_rows(self, rows, xi, scale=None):
+        """Rank-one updates from rows[k] = dy/dw with innovations xi[k]."""
+        rows, xi = _f64(np.atleast_2d(rows)), _f64(np.atleast_1d(xi))
+        sc = None if scale is None else _f64(np.broadcast_to(scale, xi.shape))
+        call("dnnf90_kf_update_rows", self.kid, rows.shape[0], _pd(rows), _pd(xi),
+             None if sc is None else _pd(sc))
+
+    def state(self):
+        lam = ctypes.c_double()
+        ng = ctypes.c_int()
+        call("dnnf90_kf_read", self.kid, ctypes.byref(lam), ctypes.byref(ng), None)
+        return lam.value, ng.value
+
+    def cov(self):
+        """Dense [nw][nw], or the decoupled blocks concatenated (flat)."""
+        dims = self.net.dims
+        if self.decoupled:
+            n = sum(d * (dims[l - 1] + 1) ** 2 for l, d in enumerate(dims) if l > 0)
+            P = np.zeros(n)
+        else:
+            P = np.zeros((self.net.nw, self.net.nw))
+        call("dnnf90_kf_read", self.kid, None, None, _pd(P))
+        return P
+
+    def free(self):
+        if self.kid > 0:
+            lib().dnnf90_kf_free(self.kid)
+            self.kid = 0
 
 
 def committee_step(nets, rules, xs, grads, loss, stream=None):

@@ -17,7 +17,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libdnnf90_b200.so")
 
 SOURCES = ["tables.cpp", "bell_plan.cpp", "api.cpp", "engine.cu", "bell.cu", "gemm_tc.cu",
-           "ngd.cu"]
+           "ngd.cu", "kalman.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
            "--expt-relaxed-constexpr", "-Xcompiler", "-Wall"]

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <memory>
@@ -81,6 +82,16 @@ struct RuleH {
   DevRule d;
 };
 
+// extended Kalman filter bound to a network (kalman_t, lib/kalman_module.f90:47-90)
+struct KfH {
+  bool used = false;
+  int nid = 0, gen = 0;
+  bool decoupled = false;
+  std::vector<int> bsz, boff;
+  KfDev d;
+  cudaStream_t st = nullptr;
+};
+
 std::recursive_mutex g_mu;
 TabH g_tab[MAXH + 1];
 NetH g_net[MAXH + 1];
@@ -89,6 +100,7 @@ WorkH g_wrk[MAXH + 1];
 WorkH g_twk[MAXH + 1];
 GradH g_grd[MAXH + 1];
 RuleH g_rule[MAXH + 1];
+KfH g_kf[MAXH + 1];
 TableSet g_cur;
 bool g_cur_ready = false;
 
@@ -1599,6 +1611,173 @@ int dnnf90_committee_info(int *policy, float *graph_ms) {
   if (policy) *policy = g_comm_policy;
   if (graph_ms) *graph_ms = g_comm_ms;
   return g_comm_policy >= 0 ? RC_OK : RC_BAD_ARG;
+}
+
+// ------------------------------------------------------------- Kalman filter
+int dnnf90_kf_create(int nid, double p0, double lam_ini, double lam0, int decoupled, double q,
+                     double gate) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (bad_net(nid)) return RC_BAD_ARG;
+  // kf_init contract (lib/kalman_module.f90:118-127)
+  if (!(p0 > 0.0)) {
+    set_error("kf_create: p0 must be positive");
+    return RC_BAD_ARG;
+  }
+  if (!(lam_ini > 0.0 && lam_ini <= 1.0 && lam0 > 0.0 && lam0 <= 1.0)) {
+    set_error("kf_create: forgetting parameters must lie in (0,1]");
+    return RC_BAD_ARG;
+  }
+  if (!(q >= 0.0) || !(gate >= 0.0)) {
+    set_error("kf_create: process noise and gate must not be negative");
+    return RC_BAD_ARG;
+  }
+  int rc = device_ready();
+  if (rc) return rc;
+  const int id = free_slot(g_kf);
+  if (id < 0) return RC_BAD_ARG;
+  const NetH &n = g_net[nid];
+  KfH &k = g_kf[id];
+  k = KfH();
+  k.nid = nid;
+  k.gen = g_gen[nid];
+  k.decoupled = decoupled != 0;
+  if (k.decoupled) {  // one block per neuron over (bias, fan-in), kf_block_map :172-189
+    int m = 0;
+    for (int l = 1; l < n.nlayer; ++l)
+      for (int j = 0; j < n.dims[l]; ++j) {
+        k.bsz.push_back(n.dims[l - 1] + 1);
+        k.boff.push_back(m);
+        m += n.dims[l - 1] + 1;
+      }
+  } else {
+    k.bsz.push_back((int)n.w.size());
+    k.boff.push_back(0);
+  }
+  if ((rc = kf_create(k.d, k.bsz, k.boff, p0, lam_ini, lam0, q, gate))) {
+    k.d.release();
+    k = KfH();
+    return rc;
+  }
+  k.used = true;
+  return id;
+}
+
+int dnnf90_kf_free(int kid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (kid < 1 || kid > MAXH || !g_kf[kid].used) return RC_BAD_ARG;
+  KfH &k = g_kf[kid];
+  if (k.st) cudaStreamSynchronize(k.st);
+  k.d.release();
+  if (k.st) cudaStreamDestroy(k.st);
+  k = KfH();
+  return RC_OK;
+}
+
+namespace {
+int kf_check(int kid) {
+  if (kid < 1 || kid > MAXH || !g_kf[kid].used) return RC_BAD_ARG;
+  const KfH &k = g_kf[kid];
+  if (bad_net(k.nid) || g_gen[k.nid] != k.gen) {
+    set_error("kalman: the filter's network was freed");
+    return RC_BAD_ARG;
+  }
+  return RC_OK;
+}
+
+int kf_status_rc(const KfState &s) {
+  if (!s.status) return RC_OK;
+  set_error("kalman: nonpositive innovation denominator at observation " +
+            std::to_string(s.status) + "; the covariance has lost positive definiteness");
+  return RC_BAD_ARG;
+}
+}  // namespace
+
+int dnnf90_kf_update_rows(int kid, int nobs, const double *rows, const double *xi,
+                          const double *scale) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = kf_check(kid);
+  if (rc) return rc;
+  if (nobs < 0 || (nobs > 0 && (!rows || !xi))) return RC_BAD_ARG;
+  if (nobs == 0) return RC_OK;
+  KfH &k = g_kf[kid];
+  NetH &n = g_net[k.nid];
+  flush_for_net(k.nid);  // queued points belong to the weights before the update
+  if (!k.st && (rc = ck(cudaStreamCreateWithFlags(&k.st, cudaStreamNonBlocking), "stream")))
+    return rc;
+  const size_t nw = n.w.size();
+  // rows staged in chunks of at most 256 MiB (DNNF90_KF_STAGE_KB overrides);
+  // each chunk carries the first row of the next, whose products the
+  // chunk's last tile pass forms
+  size_t stage = 256u << 20;
+  if (const char *e = std::getenv("DNNF90_KF_STAGE_KB")) stage = (size_t)std::max(1, std::atoi(e)) << 10;
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>(nobs, stage / (8 * nw)));
+  const size_t need = ((size_t)(chunk + 1) * (nw + 2) + nw) * sizeof(double);
+  if (k.d.stage_bytes < need) {
+    cudaFree(k.d.stage);
+    k.d.stage = nullptr;
+    k.d.stage_bytes = 0;
+    if ((rc = ck(cudaMalloc(&k.d.stage, need), "cudaMalloc"))) return rc;
+    k.d.stage_bytes = need;
+  }
+  double *dw = k.d.stage, *dr = dw + nw, *dxi = dr + (size_t)(chunk + 1) * nw,
+         *dsc = dxi + chunk + 1;
+  if ((rc = ck(cudaMemcpyAsync(dw, n.w.data(), nw * 8, cudaMemcpyHostToDevice, k.st), "H2D")))
+    return rc;
+  for (int k0 = 0; k0 < nobs; k0 += chunk) {
+    const int k1 = std::min(nobs, k0 + chunk);
+    const int ncp = std::min(nobs, k1 + 1) - k0;  // rows staged, with the next chunk's first
+    if ((rc = ck(cudaMemcpyAsync(dr, rows + (size_t)k0 * nw, (size_t)ncp * nw * 8,
+                                 cudaMemcpyHostToDevice, k.st), "H2D")))
+      return rc;
+    if ((rc = ck(cudaMemcpyAsync(dxi, xi + k0, (size_t)ncp * 8, cudaMemcpyHostToDevice, k.st),
+                 "H2D")))
+      return rc;
+    if (scale && (rc = ck(cudaMemcpyAsync(dsc, scale + k0, (size_t)ncp * 8,
+                                          cudaMemcpyHostToDevice, k.st), "H2D")))
+      return rc;
+    if ((rc = kf_run(k.d, k1 - k0, dr, nw, dxi, scale ? dsc : nullptr, dw, k.st, k0,
+                     k1 < nobs)))
+      return rc;
+  }
+  if ((rc = ck(cudaMemcpyAsync(n.w.data(), dw, nw * 8, cudaMemcpyDeviceToHost, k.st), "D2H")))
+    return rc;
+  KfState s;
+  if ((rc = kf_state(k.d, &s, k.st))) return rc;
+  n.wver++;
+  return kf_status_rc(s);
+}
+
+int dnnf90_kf_update_rows_dev(int kid, int nobs, const double *rows_dev, const double *xi_dev,
+                              const double *scale_dev, double *w_dev, void *stream) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = kf_check(kid);
+  if (rc) return rc;
+  if (nobs < 0 || (nobs > 0 && (!rows_dev || !xi_dev || !w_dev))) return RC_BAD_ARG;
+  if (nobs == 0) return RC_OK;
+  KfH &k = g_kf[kid];
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = kf_run(k.d, nobs, rows_dev, k.d.nw, xi_dev, scale_dev, w_dev, st, 0, false)))
+    return rc;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return RC_OK;
+  KfState s;
+  if ((rc = kf_state(k.d, &s, st))) return rc;
+  return kf_status_rc(s);
+}
+
+int dnnf90_kf_read(int kid, double *lam, int *ngated, double *P) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (kid < 1 || kid > MAXH || !g_kf[kid].used) return RC_BAD_ARG;
+  KfH &k = g_kf[kid];
+  if (k.st) cudaStreamSynchronize(k.st);
+  KfState s;
+  int rc = kf_state(k.d, &s, nullptr);
+  if (rc) return rc;
+  if (lam) *lam = s.lam;
+  if (ngated) *ngated = s.ngated;
+  if (P) rc = kf_read_cov(k.d, k.bsz, k.boff, !k.decoupled, P, nullptr);
+  return rc;
 }
 
 int dnnf90_ngd_step_noalloc(int nrow, int nw, const double *rows_dev, const double *b_dev,

@@ -199,6 +199,48 @@ int ngd_device_noalloc(const double *rows, int nrow, int nw, const double *b, in
                        double mu, double *u, cudaStream_t st);
 int ngd_noalloc_maxw();
 
+// Extended Kalman filter (lib/kalman_module.f90): device scalars of the
+// filter and of the observation being applied.
+struct KfState {
+  double lam, lam0, q, gate;       // current lambda, schedule, process noise, gate
+  double lamk, denom, sg, xi;      // observation k: its lambda, denominator, gate scale, innovation
+  int ngated;                      // gated updates so far
+  int status;                      // 0, or 1 + the observation whose denominator was not positive
+};
+
+// covariance in packed 32 x 32 tiles of each block's upper triangle
+struct KfDev {
+  int nw = 0, ntile = 0, tmax = 0, nred = 0;
+  double *P = nullptr;       // [ntile][32][32]
+  int4 *tiles = nullptr;     // per tile: block offset, block size, I, J
+  int *rt = nullptr;         // [nw] tiles per side of the weight's block
+  double *part = nullptr;    // [tmax][nw] partial products with the next row
+  double *pj = nullptr;      // [nw] P j of the observation being applied
+  double *dotp = nullptr;    // per reduce CTA: its share of j.Pj
+  unsigned *ctr = nullptr;   // reduce CTAs finished
+  KfState *st = nullptr;
+  double *stage = nullptr;   // host-call staging (rows, innovations, scales, weights)
+  size_t stage_bytes = 0;
+  void release();
+};
+
+// blocks (sizes bsz at flat offsets boff; one block of nw for the dense
+// filter), P = p0 I
+int kf_create(KfDev &d, const std::vector<int> &bsz, const std::vector<int> &boff, double p0,
+              double lam_ini, double lam0, double q, double gate);
+// nobs updates of kf_update_grad in order: rows[k*ld + i] = dy/dw_i,
+// xi[k] = target - prediction, scale[k] (null = 1); w[nw] updated in place.
+// Stops at the first nonpositive denominator (KfState::status = kbase + k + 1).
+// A sequence split into calls passes kbase = the index of its first
+// observation; a call with has_next also stages row nobs (the next call's
+// first), whose products its last tile pass forms.
+int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
+           const double *scale, double *w, cudaStream_t s, int kbase, bool has_next);
+int kf_state(const KfDev &d, KfState *out, cudaStream_t s);
+// covariance to the host: dense [nw][nw], or the blocks [bsz][bsz] one after another
+int kf_read_cov(const KfDev &d, const std::vector<int> &bsz, const std::vector<int> &boff,
+                bool dense, double *out, cudaStream_t s);
+
 // SMs a persistent launch may fill: the device's count, or a cap that the
 // committee step sets on its host thread while it issues one member's
 // launches, so that concurrent members share the device instead of each

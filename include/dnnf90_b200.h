@@ -109,6 +109,35 @@ int dnnf90_ngd_step(int nid, int nrow, const double *rows, const double *b,
 int dnnf90_ngd_step_dual(int nid, int nrow, const double *rows, const double *b,
                          int nb, double mu, int prec, double *u);
 
+/* ---- extended Kalman filter (lib/kalman_module.f90; new at the C boundary,
+ * the reference reaches it from its trainer, app/lib_net_module.f90:455-570) */
+/* kf_init (:107-170) on network nid: P = p0 I, lambda = lam_ini, forgetting
+ * schedule lambda <- lam0 lambda + 1 - lam0.  decoupled != 0 keeps one
+ * covariance block per neuron over (bias, fan-in) instead of the dense
+ * nw x nw matrix.  q >= 0 is added to the diagonal after every update and
+ * gate >= 0 bounds the normalised innovation (0 = off for both).  p0 > 0 and
+ * lam_ini, lam0 in (0, 1], else -1.  Returns the filter handle (> 0). */
+int dnnf90_kf_create(int nid, double p0, double lam_ini, double lam0, int decoupled,
+                     double q, double gate);
+int dnnf90_kf_free(int kid);
+/* nobs rank-one updates, in order, of kf_update_grad (:353-490): rows[k][nw]
+ * = dy/dw of observation k in the flat layout, xi[k] = target - prediction,
+ * scale[k] (NULL = 1) multiplying both (1/sqrt of an observation noise).
+ * The network's weights are updated.  A denominator lambda + j.Pj that is
+ * not positive stops the sequence there with -1 (the observations before it
+ * stay applied); the reference stops the process instead. */
+int dnnf90_kf_update_rows(int kid, int nobs, const double *rows, const double *xi,
+                          const double *scale);
+/* the same on device arrays; w_dev[nw] (flat layout) is updated in place
+ * and the network's own weights are left alone */
+int dnnf90_kf_update_rows_dev(int kid, int nobs, const double *rows_dev,
+                              const double *xi_dev, const double *scale_dev,
+                              double *w_dev, void *stream);
+/* filter state: lambda, the count of gated updates, and (P not NULL) the
+ * covariance, dense [nw][nw] or the decoupled blocks [n_b][n_b] one after
+ * another in the weight order */
+int dnnf90_kf_read(int kid, double *lam, int *ngated, double *P);
+
 /* ---- device-pointer entry points (pointers to device memory; stream is
  * a cudaStream_t, NULL for the legacy default stream).  On the split path
  * the compute entries return after the work on stream has finished, having

@@ -883,6 +883,90 @@ int orc_grad_sys_batch(const orc_tables *t, int nlayer, const int *dims, const d
   return 0;
 }
 
+int orc_kf_update(int nw, double *w, double *P, int nblk, const int *bsz, const int *boff,
+                  const double *jrow, double xi_in, double scale, double *lam, double lam0,
+                  double q, double gate, int *ngated) {
+  double *jf = (double *)malloc(sizeof(double) * nw);
+  double *pj = (double *)malloc(sizeof(double) * nw);
+  double *kv = (double *)malloc(sizeof(double) * nw);
+  double xi = scale * xi_in;
+  for (int m = 0; m < nw; ++m) jf[m] = scale * jrow[m];
+  if (nblk > 0) { /* decoupled: P j per node block */
+    const double *Pb = P;
+    for (int b = 0; b < nblk; ++b) {
+      const int n = bsz[b], o = boff[b];
+      for (int i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int r = 0; r < n; ++r) s += Pb[(size_t)r * n + i] * jf[o + r];
+        pj[o + i] = s;
+      }
+      Pb += (size_t)n * n;
+    }
+  } else {
+    for (int i = 0; i < nw; ++i) {
+      double s = 0.0;
+      for (int r = 0; r < nw; ++r) s += P[(size_t)r * nw + i] * jf[r];
+      pj[i] = s;
+    }
+  }
+  double dot = 0.0;
+  for (int m = 0; m < nw; ++m) dot += jf[m] * pj[m];
+  double denom = *lam + dot;
+  if (!(denom > 0.0)) {
+    free(jf); free(pj); free(kv);
+    return -1;
+  }
+  if (gate > 0.0) {
+    const double jpj = denom - *lam;
+    if (xi * xi > gate * gate * denom) {
+      const double s2 = gate * gate * *lam / (xi * xi - gate * gate * jpj);
+      const double sq = sqrt(s2);
+      xi = sq * xi;
+      for (int m = 0; m < nw; ++m) pj[m] = sq * pj[m];
+      denom = *lam + s2 * jpj;
+      ++*ngated;
+    }
+  }
+  for (int m = 0; m < nw; ++m) kv[m] = pj[m] / denom;
+  for (int m = 0; m < nw; ++m) w[m] = w[m] + kv[m] * xi;
+  /* downdate (P - kv pj^T) / lambda, then the average with the transpose
+   * and the process noise on the diagonal */
+  const double lm = *lam;
+  if (nblk > 0) {
+    double *Pb = P;
+    for (int b = 0; b < nblk; ++b) {
+      const int n = bsz[b], o = boff[b];
+      for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r)
+          Pb[(size_t)r * n + c] = (Pb[(size_t)r * n + c] - kv[o + r] * pj[o + c]) / lm;
+      for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) {
+          const double a = 0.5 * (Pb[(size_t)i * n + j] + Pb[(size_t)j * n + i]);
+          Pb[(size_t)i * n + j] = a;
+          Pb[(size_t)j * n + i] = a;
+        }
+      if (q > 0.0)
+        for (int i = 0; i < n; ++i) Pb[(size_t)i * n + i] += q;
+      Pb += (size_t)n * n;
+    }
+  } else {
+    for (int c = 0; c < nw; ++c)
+      for (int r = 0; r < nw; ++r)
+        P[(size_t)r * nw + c] = (P[(size_t)r * nw + c] - kv[r] * pj[c]) / lm;
+    for (int i = 0; i < nw; ++i)
+      for (int j = i + 1; j < nw; ++j) {
+        const double a = 0.5 * (P[(size_t)i * nw + j] + P[(size_t)j * nw + i]);
+        P[(size_t)i * nw + j] = a;
+        P[(size_t)j * nw + i] = a;
+      }
+    if (q > 0.0)
+      for (int i = 0; i < nw; ++i) P[(size_t)i * nw + i] += q;
+  }
+  *lam = lam0 * *lam + 1.0 - lam0;
+  free(jf); free(pj); free(kv);
+  return 0;
+}
+
 int orc_eval_batch(const orc_tables *t, int nlayer, const int *dims,
                    const double *w, int npts, const double *X, double *tout,
                    int nthreads) {

@@ -150,6 +150,19 @@ int orc_grad_sys_batch(const orc_tables *t, int nlayer, const int *dims, const d
                        const double *src, double *grad, double *tout, double *loss,
                        int nthreads);
 
+/* Extended Kalman filter, rank-one update of kf_update_grad
+ * (lib/kalman_module.f90:353-490) from one observation row jrow[nw]
+ * (dy/dw in the flat layer order) with innovation xi and scale s (row and
+ * innovation both scaled by s).  P is dense [nw][nw], or, decoupled,
+ * nblk diagonal blocks [bsz][bsz] stored one after another (bsz[b] at
+ * offset boff[b] of the flat weights); the denominator lambda + j.Pj is
+ * global.  Optional innovation gate (gate > 0) and process noise q.
+ * Updates w, P, *lam (lambda <- lam0 lambda + 1 - lam0) and *ngated.
+ * Returns -1 if the denominator is not positive. */
+int orc_kf_update(int nw, double *w, double *P, int nblk, const int *bsz, const int *boff,
+                  const double *jrow, double xi_in, double scale, double *lam, double lam0,
+                  double q, double gate, int *ngated);
+
 /* Forward only over a batch (net_eval_hod per point). */
 int orc_eval_batch(const orc_tables *t, int nlayer, const int *dims,
                    const double *w, int npts, const double *X, double *tout,

@@ -52,6 +52,7 @@ def lib():
         L.orc_tanh_derivs.argtypes = [vp, cd, ci, vp]
         L.orc_act_derivs.argtypes = [vp, cd, ci, vp]
         L.orc_besj_all.argtypes = [ci, cd, vp]
+        L.orc_kf_update.argtypes = [ci, vp, vp, ci, vp, vp, vp, cd, cd, vp, cd, cd, cd, vp]
         L.orc_tables_set_activation.argtypes = [vp, ci]
         L.orc_weight_count.argtypes = [ci, P(ci)]
         L.orc_eval_point.argtypes = [vp, ci, P(ci), vp, vp, vp, vp]
@@ -257,6 +258,37 @@ def besj_all(n: int, x: float) -> np.ndarray:
     bj = np.zeros(n + 1)
     lib().orc_besj_all(int(n), float(x), _p(bj))
     return bj
+
+
+class Kalman:
+    """The reference's extended Kalman filter (kalman_t, kf_init,
+    kf_update_grad; lib/kalman_module.f90) over the flat weights."""
+
+    def __init__(self, dims, p0, lam_ini, lam0, decoupled=False, q=0.0, gate=0.0):
+        self.nw = weight_count(dims)
+        self.lam, self.lam0, self.q, self.gate = float(lam_ini), float(lam0), float(q), float(gate)
+        self.ngated = ctypes.c_int(0)
+        if decoupled:  # one block per neuron over (bias, fan-in), kf_block_map
+            self.bsz = np.array([dims[l - 1] + 1 for l in range(1, len(dims))
+                                 for _ in range(dims[l])], np.int32)
+            self.boff = np.concatenate([[0], np.cumsum(self.bsz)[:-1]]).astype(np.int32)
+            self.P = np.concatenate([p0 * np.eye(n).reshape(-1) for n in self.bsz])
+        else:
+            self.bsz = self.boff = None
+            self.P = p0 * np.eye(self.nw).reshape(-1)
+
+    def update(self, w, jrow, xi, scale=1.0):
+        """One observation: w (float64, updated in place), jrow = dy/dw."""
+        assert w.dtype == np.float64 and w.flags.c_contiguous
+        lam = ctypes.c_double(self.lam)
+        jr = np.ascontiguousarray(jrow, np.float64)
+        nb = 0 if self.bsz is None else len(self.bsz)
+        rc = lib().orc_kf_update(self.nw, _p(w), _p(self.P), nb, _p(self.bsz), _p(self.boff),
+                                 _p(jr), float(xi), float(scale), ctypes.byref(lam), self.lam0,
+                                 self.q, self.gate, ctypes.byref(self.ngated))
+        if rc != 0:
+            raise ValueError("oracle kf_update: nonpositive innovation denominator")
+        self.lam = lam.value
 
 
 def eval_batch(tab: Tables, dims, w, X, nthreads=0):

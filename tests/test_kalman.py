@@ -1,0 +1,251 @@
+"""Extended Kalman filter (lib/kalman_module.f90): the rank-one update of
+kf_update_grad (:353-490) on the dense and the node-wise decoupled
+covariance, with the forgetting schedule, process noise and innovation gate.
+
+The oracle restatement is pinned on the CPU by the reference's own known
+answer (tools/example_libverify.f90:215-286: on a linear network, lambda = 1,
+the filter reproduces the ridge normal-equation solution to 1e-9) and by
+properties of the algebra: a decoupled filter with one block is the dense
+one, and a gated update is the ungated update of the row and innovation
+scaled by the gate's s.  On the GPU the device filter is checked against the
+oracle observation by observation (weights, covariance, lambda, gate count),
+through the ridge known answer, across call and staging boundaries, and on a
+nonpositive denominator.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import rel_err
+
+D0, NS, P0 = 3, 60, 50.0
+
+
+def _ridge_samples():
+    """The deterministic samples of the reference's check (1-based n, i)."""
+    n = np.arange(1, NS + 1)[:, None]
+    i = np.arange(1, D0 + 1)[None, :]
+    x = np.sin(1.7 * n + 0.9 * i)
+    y = 0.7 - 1.3 * x[:, 0] + 0.4 * x[:, 1] + 2.1 * x[:, 2]
+    return x, y
+
+
+def _ridge_solution(x, y):
+    xe = np.hstack([np.ones((len(x), 1)), x])
+    A = np.eye(D0 + 1) / P0 + xe.T @ xe
+    return np.linalg.solve(A, xe.T @ y)
+
+
+def test_oracle_kalman_is_the_ridge_solution_on_a_linear_net():
+    x, y = _ridge_samples()
+    kf = po.Kalman([D0, 1], P0, 1.0, 1.0)
+    w = np.zeros(D0 + 1)                        # net_init zeroes the weights
+    for n in range(NS):
+        xe = np.concatenate([[1.0], x[n]])
+        kf.update(w, xe, y[n] - w @ xe)
+    b = _ridge_solution(x, y)
+    assert np.abs(w - b).max() / np.abs(b).max() < 1e-9
+
+
+def _random_sequence(nw, nobs, seed):
+    rng = np.random.default_rng(seed)
+    rows = rng.normal(size=(nobs, nw)) / np.sqrt(nw)
+    xi = 2.0 * rng.normal(size=nobs)
+    scale = rng.uniform(0.5, 2.0, nobs)
+    return rows, xi, scale
+
+
+def test_oracle_one_block_decoupled_is_dense():
+    dims = [3, 1]                               # one neuron: one block of 4
+    rows, xi, sc = _random_sequence(4, 25, 1)
+    a, b = po.Kalman(dims, 3.0, 0.98, 0.99, q=1e-3), po.Kalman(dims, 3.0, 0.98, 0.99, True, q=1e-3)
+    wa, wb = np.zeros(4), np.zeros(4)
+    for r, e, s in zip(rows, xi, sc):
+        a.update(wa, r, e, s)
+        b.update(wb, r, e, s)
+    assert np.array_equal(wa, wb) and np.array_equal(a.P, b.P) and a.lam == b.lam
+
+
+def test_oracle_gate_is_a_noise_scale():
+    """A tripped gate applies the update of the row and innovation scaled
+    by s, s^2 = gate^2 lambda / (xi^2 - gate^2 j.Pj), which leaves the
+    normalised innovation at the gate."""
+    dims = [2, 4, 1]
+    nw = po.weight_count(dims)
+    rows, _, _ = _random_sequence(nw, 1, 2)
+    j, xi, gate = rows[0], 40.0, 2.0
+    g = po.Kalman(dims, 2.0, 0.99, 0.995, gate=gate)
+    wg = np.zeros(nw)
+    jpj = j @ (g.P.reshape(nw, nw) @ j)
+    lam = g.lam
+    g.update(wg, j, xi)
+    assert g.ngated.value == 1
+    s = np.sqrt(gate ** 2 * lam / (xi ** 2 - gate ** 2 * jpj))
+    assert abs((s * xi) ** 2 - gate ** 2 * (lam + s ** 2 * jpj)) < 1e-9 * xi ** 2
+    u = po.Kalman(dims, 2.0, 0.99, 0.995)
+    wu = np.zeros(nw)
+    u.update(wu, j, xi, s)
+    assert rel_err(wg, wu) < 1e-14 and rel_err(g.P, u.P) < 1e-14
+    # an innovation inside the gate leaves the update alone
+    h, k = po.Kalman(dims, 2.0, 0.99, 0.995, gate=gate), po.Kalman(dims, 2.0, 0.99, 0.995)
+    wh, wk = np.zeros(nw), np.zeros(nw)
+    h.update(wh, j, 0.1)
+    k.update(wk, j, 0.1)
+    assert h.ngated.value == 0 and np.array_equal(wh, wk) and np.array_equal(h.P, k.P)
+
+
+# ---------------------------------------------------------------- device
+
+
+def _net(dims, w=None):
+    from dnnf90_b200 import api
+    ts = api.TableSet(dims[0], 1)
+    return api.Net(ts, dims, weights=w), ts
+
+
+@pytest.mark.gpu
+def test_device_kalman_is_the_ridge_solution_on_a_linear_net():
+    from dnnf90_b200 import api
+    x, y = _ridge_samples()
+    net, ts = _net([D0, 1], np.zeros(D0 + 1))
+    kf = api.Kalman(net, P0, 1.0, 1.0)
+    for n in range(NS):                         # one observation per call
+        xe = np.concatenate([[1.0], x[n]])
+        w = net.get_weights()
+        kf.update_rows(xe, y[n] - w @ xe)
+    b = _ridge_solution(x, y)
+    assert np.abs(net.get_weights() - b).max() / np.abs(b).max() < 1e-9
+    kf.free(); net.free(); ts.free()
+
+
+CASES = [  # dims, decoupled, q, gate, nobs
+    ([3, 20, 20, 1], False, 0.0, 0.0, 40),
+    ([3, 20, 20, 1], False, 1e-4, 1.5, 40),
+    ([3, 20, 20, 1], True, 0.0, 0.0, 40),
+    ([3, 20, 20, 1], True, 1e-4, 1.5, 40),
+    ([2, 3, 1], False, 1e-3, 0.0, 30),          # nw = 13: one padded tile
+    ([2, 3, 1], True, 0.0, 1.0, 30),
+    ([4, 40, 33, 2], False, 0.0, 2.0, 12),      # nw = 1485, block edges off the tile grid
+    ([4, 40, 33, 2], True, 1e-5, 0.0, 12),
+]
+
+
+def _run_both(dims, decoupled, q, gate, nobs, seed=3):
+    from dnnf90_b200 import api
+    nw = po.weight_count(dims)
+    rows, xi, sc = _random_sequence(nw, nobs, seed)
+    w0 = np.random.default_rng(seed + 1).normal(size=nw) * 0.1
+    net, ts = _net(dims, w0)
+    kf = api.Kalman(net, 0.7, 0.98, 0.9987, decoupled, q, gate)
+    ref = po.Kalman(dims, 0.7, 0.98, 0.9987, decoupled, q, gate)
+    wref = w0.copy()
+    for r, e, s in zip(rows, xi, sc):
+        ref.update(wref, r, e, s)
+    return (kf, net, ts), ref, wref, (rows, xi, sc)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,decoupled,q,gate,nobs", CASES)
+def test_device_kalman_matches_the_oracle(dims, decoupled, q, gate, nobs):
+    (kf, net, ts), ref, wref, (rows, xi, sc) = _run_both(dims, decoupled, q, gate, nobs)
+    kf.update_rows(rows, xi, sc)
+    lam, ng = kf.state()
+    assert ng == ref.ngated.value
+    if gate > 0 and len(dims) > 3:
+        assert ng > 0                           # the gate was exercised
+    assert abs(lam - ref.lam) <= 1e-15
+    assert rel_err(net.get_weights(), wref) < 1e-11, rel_err(net.get_weights(), wref)
+    P = kf.cov().reshape(-1)
+    assert rel_err(P, ref.P) < 1e-11, rel_err(P, ref.P)
+    if not decoupled:
+        Pm = P.reshape(net.nw, net.nw)
+        assert np.array_equal(Pm, Pm.T)         # exactly symmetric
+    kf.free(); net.free(); ts.free()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("decoupled", [False, True])
+def test_device_kalman_split_across_calls_and_stages(decoupled, monkeypatch):
+    """The same sequence in one call, in several calls, and through a
+    staging area of a few rows gives the same filter."""
+    from dnnf90_b200 import api
+    dims = [3, 20, 20, 1]
+    (kf, net, ts), ref, wref, (rows, xi, sc) = _run_both(dims, decoupled, 1e-4, 1.5, 40)
+    kf.update_rows(rows, xi, sc)
+    w1, P1, s1 = net.get_weights(), kf.cov(), kf.state()
+    for parts, stage_kb in (([7, 1, 20, 12], None), ([40], 9)):
+        net2, ts2 = _net(dims, np.random.default_rng(4).normal(size=net.nw) * 0.1)
+        kf2 = api.Kalman(net2, 0.7, 0.98, 0.9987, decoupled, 1e-4, 1.5)
+        if stage_kb:                            # 9 KB: two rows of 521 weights per stage
+            monkeypatch.setenv("DNNF90_KF_STAGE_KB", str(stage_kb))
+        k0 = 0
+        for m in parts:
+            kf2.update_rows(rows[k0:k0 + m], xi[k0:k0 + m], sc[k0:k0 + m])
+            k0 += m
+        monkeypatch.delenv("DNNF90_KF_STAGE_KB", raising=False)
+        assert np.array_equal(net2.get_weights(), w1)
+        assert np.array_equal(kf2.cov(), P1) and kf2.state() == s1
+        kf2.free(); net2.free(); ts2.free()
+    kf.free(); net.free(); ts.free()
+
+
+@pytest.mark.gpu
+def test_device_kalman_stops_at_a_nonpositive_denominator():
+    from dnnf90_b200 import api
+    dims = [3, 20, 20, 1]
+    nw = po.weight_count(dims)
+    rows, xi, sc = _random_sequence(nw, 10, 5)
+    rows[6, 17] = np.nan                        # j.Pj is NaN at observation 7
+    net, ts = _net(dims, np.zeros(nw))
+    kf = api.Kalman(net, 0.7, 0.98, 0.9987)
+    with pytest.raises(api.Dnnf90Error):
+        kf.update_rows(rows, xi, sc)
+    assert "observation 7" in api.lib().dnnf90_last_error().decode()
+    ref = po.Kalman(dims, 0.7, 0.98, 0.9987)
+    wref = np.zeros(nw)
+    for k in range(6):
+        ref.update(wref, rows[k], xi[k], sc[k])
+    assert rel_err(net.get_weights(), wref) < 1e-11
+    assert rel_err(kf.cov().reshape(-1), ref.P) < 1e-11 and abs(kf.state()[0] - ref.lam) < 1e-15
+    kf.update_rows(rows[7:], xi[7:], sc[7:])    # the filter goes on from there
+    for k in range(7, 10):
+        ref.update(wref, rows[k], xi[k], sc[k])
+    assert rel_err(net.get_weights(), wref) < 1e-11
+    kf.free(); net.free(); ts.free()
+
+
+@pytest.mark.gpu
+def test_device_kalman_device_entry():
+    import torch
+    from dnnf90_b200 import api
+    dims = [3, 20, 20, 1]
+    (kf, net, ts), ref, wref, (rows, xi, sc) = _run_both(dims, True, 1e-4, 1.5, 40)
+    dev = torch.device("cuda", 0)
+    w0 = net.get_weights()
+    wd = torch.tensor(w0, device=dev)
+    rd, xd, sd = (torch.tensor(a, device=dev) for a in (rows, xi, sc))
+    api.call("dnnf90_kf_update_rows_dev", kf.kid, len(xi), rd.data_ptr(), xd.data_ptr(),
+             sd.data_ptr(), wd.data_ptr(), torch.cuda.current_stream(dev).cuda_stream)
+    assert rel_err(wd.cpu().numpy(), wref) < 1e-11
+    assert np.array_equal(net.get_weights(), w0)   # the network's own weights untouched
+    assert rel_err(kf.cov().reshape(-1), ref.P) < 1e-11
+    kf.free(); net.free(); ts.free()
+
+
+@pytest.mark.gpu
+def test_kalman_argument_checks():
+    from dnnf90_b200 import api
+    net, ts = _net([3, 8, 1])
+    for args in ((0.0, 0.98, 0.99), (1.0, 0.0, 0.99), (1.0, 0.98, 1.5), (1.0, 1.2, 0.9)):
+        with pytest.raises(api.Dnnf90Error):
+            api.Kalman(net, *args)
+    with pytest.raises(api.Dnnf90Error):
+        api.Kalman(net, 1.0, 0.98, 0.99, q=-1.0)
+    kf = api.Kalman(net, 1.0, 0.98, 0.99)
+    net.free()
+    with pytest.raises(api.Dnnf90Error):        # the network is gone
+        kf.update_rows(np.zeros(net.nw), [0.0])
+    kid = kf.kid
+    kf.free()
+    assert api.lib().dnnf90_kf_free(kid) < 0      # freed twice
+    ts.free()
