@@ -291,6 +291,179 @@ def committee_bench(api, dev, nsteps, nnet=64):
 
 
 # ------------------------------------------------------------------ our arm
+# ------------------------------------------------------------------ Kalman filter
+KF_METRIC = "EKF rank-one updates/s (kf_update_grad), dense covariance, FP64"
+KF_DIMS = [2, 128, 128, 1]
+
+
+def kf_workload(nobs):
+    nw = sum(KF_DIMS[l] * (KF_DIMS[l - 1] + 1) for l in range(1, len(KF_DIMS)))
+    return nw, (f"EKF: dense global filter on MLP {'-'.join(map(str, KF_DIMS))} (nw={nw}, "
+                f"P packed upper triangle {nw * (nw + 1) * 4 / 2**30:.2f} GiB FP64), p0=0.01, "
+                f"lambda 0.98 -> 1 (lam0 0.9987), synthetic Jacobian rows N(0,1)/sqrt(nw) and "
+                f"innovations N(0,1); one step = {nobs} sequential rank-one updates")
+
+
+def kf_rows(nw, nobs, step):
+    rng = np.random.default_rng(1000 + step)
+    return rng.normal(size=(nobs, nw)) / np.sqrt(nw), rng.normal(size=nobs)
+
+
+def kf_cpu_baseline(nobs=1):
+    """The oracle's kf_update_grad (one thread, dense nw x nw as the
+    reference stores it) on a bounded sample: nobs updates."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    nw, _ = kf_workload(nobs)
+    kf = po.Kalman(KF_DIMS, 0.01, 0.98, 0.9987)
+    w = xavier(KF_DIMS, 7)
+    rows, xi = kf_rows(nw, nobs, 0)
+    t0 = time.perf_counter()
+    for r, e in zip(rows, xi):
+        kf.update(w, r, e)
+    dt = time.perf_counter() - t0
+    return {"value": nobs / dt, "unit": "updates/s", "cores": 1, "kind": "port",
+            "sample": f"{nobs} update(s) of the workload's filter, one host thread, FP64, "
+                      f"dense {nw}x{nw} covariance"}
+
+
+def kalman_bench(args):
+    import torch
+
+    from dnnf90_b200 import api
+
+    rank = int(os.environ.get("RANK", "0"))
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    nobs = args.kf_obs
+    nw, workload = kf_workload(nobs)
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        kf_cpu_baseline(1)                       # warm (page in the covariance)
+        times = []
+        for s in range(args.warmup + args.steps):
+            c = kf_cpu_baseline(1)
+            if s >= args.warmup:
+                times.append(1.0 / c["value"])
+        v = len(times) / sum(times)
+        c["value"] = v
+        print(json.dumps({
+            "impl": "reference", "metric": KF_METRIC, "value": v, "unit": "updates/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload, "sample_updates_per_step": 1},
+            "cpu_baseline": c,
+            "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
+    # one filter per GPU on its own network: replicas, no exchange
+    _, _, local = dist_init()
+    dev = torch.device("cuda", local)
+    ts = api.TableSet(KF_DIMS[0], 1)
+    net = api.Net(ts, KF_DIMS, weights=xavier(KF_DIMS, 7))
+    kf = api.Kalman(net, 0.01, 0.98, 0.9987)
+    stream = torch.cuda.current_stream(dev)
+    nstep = args.warmup + args.steps
+    host = [kf_rows(nw, nobs, s) for s in range(nstep)]
+    rows_d = [torch.tensor(r, device=dev) for r, _ in host]
+    xi_d = [torch.tensor(x, device=dev) for _, x in host]
+    w_d = torch.tensor(net.get_weights(), device=dev)
+
+    def dev_step(s):
+        api.call("dnnf90_kf_update_rows_dev", kf.kid, nobs, rows_d[s].data_ptr(),
+                 xi_d[s].data_ptr(), None, w_d.data_ptr(), stream.cuda_stream)
+
+    def sync_all():
+        torch.cuda.synchronize(dev)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if ws > 1:
+            import torch.distributed as dist
+            t = torch.tensor([v], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return v
+
+    for s in range(args.warmup):
+        dev_step(s)
+    ck = Clocks(local)
+    ck.__enter__()
+    ck.wait_first()
+    ck.mark()
+    sync_all()
+    l0 = api.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for s in range(args.warmup, nstep):
+        dev_step(s)
+    e1.record(stream)
+    sync_all()
+    launches = api.launch_count() - l0
+    ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+    ck.__exit__()
+    clk = ck.summary()
+    value = ws * nobs * 1000.0 / ms
+
+    # end to end through the host entry: rows and innovations H2D, weights
+    # H2D and D2H, inside the timed region
+    sync_all()
+    e0.record(stream)
+    t0 = time.perf_counter()
+    for s in range(args.warmup, nstep):
+        kf.update_rows(host[s][0], host[s][1])
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(1000.0 * (time.perf_counter() - t0)) / args.steps
+    e2e = {"value": ws * nobs * 1000.0 / e2e_ms, "unit": "updates/s",
+           "h2d_bytes_per_step": ws * (nobs * (nw + 1) * 8 + nw * 8),
+           "d2h_bytes_per_step": ws * (nw * 8 + 80)}
+
+    # per-kernel device time over one more step (events around every launch)
+    api.profile_enable(True)
+    dev_step(nstep - 1)
+    torch.cuda.synchronize(dev)
+    prof = api.profile_read()
+    api.profile_enable(False)
+    hbm, _, src = peaks()
+    tl_n, tl_ms = prof.get("k_kf_tiles", (0, 0.0))
+    roof = None
+    if tl_n:
+        per = tl_ms / tl_n
+        alg = nw * (nw + 1) / 2 * 8 * 2          # packed triangle read and written once
+        ach = alg / (per * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "k_kf_tiles", "achieved": ach, "peak": hbm,
+                "unit": "GB/s", "frac": ach / hbm, "peak_source": src,
+                "alg_bytes_per_launch": alg, "launch_ms": per, "traffic": None,
+                "note": "one launch applies one update: the upper triangle of P read and "
+                        "written once, the products with the next row formed in the same read"}
+    cpu = kf_cpu_baseline(1) if (rank == 0 and ws == 1) else None
+    if rank == 0:
+        print(json.dumps({
+            "metric": KF_METRIC, "value": value, "unit": "updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Jacobian rows and innovations)",
+            "config": {"workload": workload, "updates_per_step": nobs,
+                       "parallelism": f"replicas: one filter per GPU ({ws})",
+                       "l2": "inputs larger than L2: the covariance is "
+                             f"{nw * (nw + 1) * 4 / 2**30:.2f} GiB, read and written per update"},
+            "kernel_ms_per_step": {k: v[1] for k, v in prof.items()},
+            "kernel_launches_per_step": {k: v[0] for k, v in prof.items()},
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clk,
+            "cpu_baseline": cpu}), flush=True)
+    kf.free()
+    net.free()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -309,7 +482,13 @@ def main():
                          "launches upset the autotuner's timings")
     ap.add_argument("--prof-steps", type=int, default=1,
                     help="steps of the per-kernel event-profiled pass (untimed)")
+    ap.add_argument("--workload", default="zk7", choices=["zk7", "kalman"],
+                    help="zk7: the collocation training step (default); kalman: the "
+                         "extended Kalman filter's rank-one updates")
+    ap.add_argument("--kf-obs", type=int, default=16, help="Kalman updates per step")
     args = ap.parse_args()
+    if args.workload == "kalman":
+        return kalman_bench(args)
     if args.impl == "reference":
         return run_reference(args)
 

@@ -210,13 +210,15 @@ struct KfState {
 
 // covariance in packed 32 x 32 tiles of each block's upper triangle
 struct KfDev {
-  int nw = 0, ntile = 0, tmax = 0, nred = 0;
+  int nw = 0, ntile = 0, nred = 0;
+  bool dense = false;        // a single block (the global filter)
   double *P = nullptr;       // [ntile][32][32]
-  int4 *tiles = nullptr;     // per tile: block offset, block size, I, J
-  int *rt = nullptr;         // [nw] tiles per side of the weight's block
-  double *part = nullptr;    // [tmax][nw] partial products with the next row
+  int4 *tiles = nullptr;     // per tile: block offset, block size, I | J << 16, slot offset
+  int4 *rtl = nullptr;       // per row tile: first weight, rows, slots, slot offset
+  double *part = nullptr;    // per block [row tile][slot][32]: partial products
+                             // of P with the next row
   double *pj = nullptr;      // [nw] P j of the observation being applied
-  double *dotp = nullptr;    // per reduce CTA: its share of j.Pj
+  double *dotp = nullptr;    // per row tile: its share of j.Pj
   unsigned *ctr = nullptr;   // reduce CTAs finished
   KfState *st = nullptr;
   double *stage = nullptr;   // host-call staging (rows, innovations, scales, weights)

@@ -11,9 +11,11 @@
 // and the symmetrisation of the reference,
 //     P <- (P - kv pj^T) / lambda,  P_ij <- (P_ij + P_ji) / 2,  P_ii += q,
 // give, for an element whose old value a is the same on both sides,
-//     P_ij <- ((a - kv_i pj_j)/lambda + (a - kv_j pj_i)/lambda) / 2,
+//     P_ij <- ((a - kv_i pj_j) + (a - kv_j pj_i)) / (2 lambda),
 // an expression symmetric in (i, j), so each stored element is updated from
-// its own value alone and the triangle never needs the transposed entry.
+// its own value alone and the triangle never needs the transposed entry
+// (the reference divides each term by lambda before the average; the two
+// differ by rounding only).
 //
 // One observation is two launches.  The tile pass applies observation k
 // (downdate, process noise, and w += kv xi on the diagonal tiles) and, in
@@ -29,6 +31,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -47,7 +50,7 @@ namespace dnnf90 {
 
 constexpr int KT = 32;          // tile side
 constexpr int KTE = KT * KT;    // elements per tile
-constexpr int RED_THREADS = 256;
+constexpr int RED_THREADS = 512;
 
 // tile pass modes
 constexpr int KM_PJ = 0;        // products with the first row only
@@ -65,17 +68,55 @@ __device__ __forceinline__ double row_scale(const KfRowArgs &a, int k) {
   return a.scale ? a.scale[k] : 1.0;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(256) k_kf_tiles(const int4 *__restrict__ tiles,
-                                                  double *__restrict__ P, int nw,
-                                                  const double *__restrict__ pj,
-                                                  KfState *__restrict__ st, double *__restrict__ w,
-                                                  KfRowArgs ra, int knext,
-                                                  double *__restrict__ part) {
-  if (st->status) return;
-  const int4 t = tiles[blockIdx.x];   // x: block offset, y: block size, z: I, w: J
-  const int o = t.x, n = t.y, I = t.z, J = t.w;
+// (I, J) of tile t in the row-major upper triangle of tb x tb tiles, where
+// row I starts at t0(I) = I tb - I (I - 1) / 2
+__device__ __forceinline__ void tri_tile(int t, int tb, int &I, int &J) {
+  const double b = 2.0 * tb + 1.0;
+  int i = (int)((b - sqrt(b * b - 8.0 * t)) * 0.5);
+  auto t0 = [tb](int r) { return (long long)r * tb - (long long)r * (r - 1) / 2; };
+  while (i > 0 && t0(i) > t) --i;
+  while (i + 1 < tb && t0(i + 1) <= t) ++i;
+  I = i;
+  J = i + (int)(t - t0(i));
+}
+
+// One CTA per tile.  DENSE (a single block of nw) derives the tile's
+// position from its index, so that nothing the vector loads need waits on
+// a table read; the decoupled filter reads its tile table.
+template <int MODE, bool DENSE>
+__global__ void __launch_bounds__(256, 8) k_kf_tiles(const int4 *__restrict__ tiles,
+                                                     double *__restrict__ P, int nw,
+                                                     const double *__restrict__ pj,
+                                                     KfState *__restrict__ st,
+                                                     double *__restrict__ w, KfRowArgs ra,
+                                                     int knext, double *__restrict__ part) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // the tile's own elements first: their addresses depend on nothing else,
+  // so the HBM reads are in flight while the scalars and vectors arrive.
+  // The covariance streams through with evict-first loads and stores, so
+  // that the partial slots written beside it stay in L2 for the reduce.
+  double *tp = P + (size_t)blockIdx.x * KTE;
+  double v[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) v[m] = __ldcs(tp + (warp + 8 * m) * KT + lane);
+  int o, n, I, J;
+  double *pslot;  // the block's partial slots, [row tile][slot][32]
+  if (DENSE) {
+    o = 0;
+    n = nw;
+    tri_tile(blockIdx.x, (nw + KT - 1) / KT, I, J);
+    pslot = part;
+  } else {
+    // x: block offset, y: block size, z: I | J << 16, w: the block's partial slots
+    const int4 t = tiles[blockIdx.x];
+    o = t.x;
+    n = t.y;
+    I = t.z & 0xffff;
+    J = t.z >> 16;
+    pslot = part + t.w;
+  }
+  const int tb = (n + KT - 1) / KT;
+  if (st->status) return;
   __shared__ double s_pjR[KT], s_kvR[KT], s_pjC[KT], s_kvC[KT], s_jR[KT], s_jC[KT];
   __shared__ double s_col[8][KT + 1];
   double lam = 1.0, denom = 1.0, sg = 1.0, xi = 0.0, q = 0.0;
@@ -104,28 +145,27 @@ __global__ void __launch_bounds__(256) k_kf_tiles(const int4 *__restrict__ tiles
     }
   }
   __syncthreads();
-  double *tp = P + (size_t)blockIdx.x * KTE;
-  double v[4];
-#pragma unroll
-  for (int m = 0; m < 4; ++m) v[m] = tp[(warp + 8 * m) * KT + lane];
   const int C = J * KT + lane;
   if (MODE != KM_PJ) {
+    // 1/lambda once per tile: an FP64 division per element would cost as
+    // much as the element's HBM traffic (lambda = 1 is exact either way)
+    const double rl = 1.0 / lam, hl = 0.5 * rl;
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const int r = warp + 8 * m, R = I * KT + r;
       if (R < n && C < n) {
         const double a = v[m];
         if (R == C) {
-          double d = (a - s_kvR[r] * s_pjR[r]) / lam;
+          double d = __fma_rn(-s_kvR[r], s_pjR[r], a) * rl;
           if (q > 0.0) d += q;
           v[m] = d;
         } else {
           const double x = __fma_rn(-s_kvR[r], s_pjC[lane], a);
           const double y = __fma_rn(-s_kvC[lane], s_pjR[r], a);
-          v[m] = 0.5 * (x / lam + y / lam);
+          v[m] = (x + y) * hl;
         }
       }
-      tp[r * KT + lane] = v[m];
+      __stcs(tp + r * KT + lane, v[m]);
     }
     if (I == J && threadIdx.x < KT) {
       const int R = I * KT + lane;
@@ -140,7 +180,7 @@ __global__ void __launch_bounds__(256) k_kf_tiles(const int4 *__restrict__ tiles
 #pragma unroll
       for (int off = 16; off; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
       const int R = I * KT + warp + 8 * m;
-      if (lane == 0 && R < n) part[(size_t)J * nw + o + R] = s;
+      if (lane == 0 && R < n) pslot[((size_t)I * tb + J) * KT + warp + 8 * m] = s;
     }
     if (I != J) {  // column sums -> slot I of the rows of tile J
       double s = 0.0;
@@ -152,15 +192,17 @@ __global__ void __launch_bounds__(256) k_kf_tiles(const int4 *__restrict__ tiles
         double c = 0.0;
 #pragma unroll
         for (int u = 0; u < 8; ++u) c += s_col[u][lane];
-        if (C < n) part[(size_t)I * nw + o + C] = c;
+        if (C < n) pslot[((size_t)J * tb + I) * KT + lane] = c;
       }
     }
   }
 }
 
 // P j of row k from the partial slots, j.Pj per CTA, and in the last CTA
-// the scalars of observation k (denominator, gate, lambda).
-__global__ void __launch_bounds__(RED_THREADS) k_kf_reduce(int nw, const int *__restrict__ rt,
+// the scalars of observation k (denominator, gate, lambda).  One CTA per
+// row tile: its slots are contiguous ([slot][32]), warp g of 16 sums slots
+// g, g + 16, ..., and the sixteen sums of a row are added in a fixed order.
+__global__ void __launch_bounds__(RED_THREADS) k_kf_reduce(const int4 *__restrict__ rtl,
                                                            const double *__restrict__ part,
                                                            double *__restrict__ pj, KfRowArgs ra,
                                                            int k, int kbase,
@@ -168,27 +210,32 @@ __global__ void __launch_bounds__(RED_THREADS) k_kf_reduce(int nw, const int *__
                                                            unsigned *__restrict__ ctr,
                                                            KfState *__restrict__ st) {
   if (st->status) return;
-  const int R = blockIdx.x * RED_THREADS + threadIdx.x;
-  double prod = 0.0;
-  if (R < nw) {
-    double s = 0.0;
-    const int ns = rt[R];
-    for (int i = 0; i < ns; ++i) s += part[(size_t)i * nw + R];
-    pj[R] = s;
-    prod = row_scale(ra, k) * ra.rows[(size_t)k * ra.ld + R] * s;
-  }
-  __shared__ double s_red[RED_THREADS / 32];
+  const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int4 rt = rtl[blockIdx.x];  // x: first weight, y: rows, z: slots, w: slot offset
+  const double *src = part + rt.w;
+  __shared__ double s_sum[RED_THREADS / 32][33];
   __shared__ bool s_last;
-#pragma unroll
-  for (int off = 16; off; off >>= 1) prod += __shfl_xor_sync(0xffffffffu, prod, off);
-  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = prod;
+  double s = 0.0;
+#pragma unroll 8
+  for (int i = g; i < rt.z; i += RED_THREADS / 32) s += src[(size_t)i * KT + lane];
+  s_sum[g][lane] = s;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double b = 0.0;
-    for (int u = 0; u < RED_THREADS / 32; ++u) b += s_red[u];
-    dotp[blockIdx.x] = b;
-    __threadfence();
-    s_last = atomicAdd(ctr, 1u) == gridDim.x - 1;
+  if (g == 0) {
+    double p = 0.0, prod = 0.0;
+#pragma unroll
+    for (int u = 0; u < RED_THREADS / 32; ++u) p += s_sum[u][lane];
+    if (lane < rt.y) {
+      const int R = rt.x + lane;
+      pj[R] = p;
+      prod = row_scale(ra, k) * ra.rows[(size_t)k * ra.ld + R] * p;
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) prod += __shfl_xor_sync(0xffffffffu, prod, off);
+    if (lane == 0) {
+      dotp[blockIdx.x] = prod;
+      __threadfence();
+      s_last = atomicAdd(ctr, 1u) == gridDim.x - 1;
+    }
   }
   __syncthreads();
   if (!s_last || threadIdx.x != 0) return;
@@ -227,7 +274,7 @@ __global__ void k_kf_init_tiles(const int4 *__restrict__ tiles, double *__restri
   double *tp = P + (size_t)blockIdx.x * KTE;
   for (int e = threadIdx.x; e < KTE; e += blockDim.x) {
     const int r = e / KT, c = e - r * KT;
-    const int R = t.z * KT + r, C = t.w * KT + c;
+    const int R = (t.z & 0xffff) * KT + r, C = (t.z >> 16) * KT + c;
     tp[e] = (R == C && R < t.y) ? p0 : 0.0;
   }
 }
@@ -235,7 +282,7 @@ __global__ void k_kf_init_tiles(const int4 *__restrict__ tiles, double *__restri
 void KfDev::release() {
   cudaFree(P);
   cudaFree(tiles);
-  cudaFree(rt);
+  cudaFree(rtl);
   cudaFree(part);
   cudaFree(pj);
   cudaFree(dotp);
@@ -250,29 +297,41 @@ int kf_create(KfDev &d, const std::vector<int> &bsz, const std::vector<int> &bof
   d.release();
   int nw = 0;
   for (size_t b = 0; b < bsz.size(); ++b) nw = std::max(nw, boff[b] + bsz[b]);
-  std::vector<int4> tl;
-  std::vector<int> rt(nw, 0);
-  d.tmax = 0;
+  // tiles (I <= J) of each block's triangle, and the block's partial slots:
+  // [row tile K][slot s][32] at a per-block offset
+  std::vector<int4> tl, rtl;
+  size_t pslots = 0;
   for (size_t b = 0; b < bsz.size(); ++b) {
     const int n = bsz[b], o = boff[b], tb = (n + KT - 1) / KT;
-    d.tmax = std::max(d.tmax, tb);
+    if (tb > 0xffff) {
+      set_error("kalman: covariance block too large");
+      return RC_UNSUPPORTED;
+    }
     for (int I = 0; I < tb; ++I)
-      for (int J = I; J < tb; ++J) tl.push_back(make_int4(o, n, I, J));
-    for (int r = 0; r < n; ++r) rt[o + r] = tb;
+      for (int J = I; J < tb; ++J) tl.push_back(make_int4(o, n, I | J << 16, (int)pslots));
+    for (int K = 0; K < tb; ++K)
+      rtl.push_back(make_int4(o + K * KT, std::min(KT, n - K * KT), tb,
+                              (int)(pslots + (size_t)K * tb * KT)));
+    pslots += (size_t)tb * tb * KT;
+    if (pslots > (size_t)INT32_MAX) {
+      set_error("kalman: covariance too large for the partial-slot index");
+      return RC_UNSUPPORTED;
+    }
   }
   d.nw = nw;
+  d.dense = bsz.size() == 1;
   d.ntile = (int)tl.size();
-  d.nred = (nw + RED_THREADS - 1) / RED_THREADS;
+  d.nred = (int)rtl.size();
   CKK(cudaMalloc(&d.P, (size_t)d.ntile * KTE * sizeof(double)));
   CKK(cudaMalloc(&d.tiles, tl.size() * sizeof(int4)));
-  CKK(cudaMalloc(&d.rt, nw * sizeof(int)));
-  CKK(cudaMalloc(&d.part, (size_t)d.tmax * nw * sizeof(double)));
+  CKK(cudaMalloc(&d.rtl, rtl.size() * sizeof(int4)));
+  CKK(cudaMalloc(&d.part, pslots * sizeof(double)));
   CKK(cudaMalloc(&d.pj, nw * sizeof(double)));
   CKK(cudaMalloc(&d.dotp, d.nred * sizeof(double)));
   CKK(cudaMalloc(&d.ctr, sizeof(unsigned)));
   CKK(cudaMalloc(&d.st, sizeof(KfState)));
   CKK(cudaMemcpy(d.tiles, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice));
-  CKK(cudaMemcpy(d.rt, rt.data(), nw * sizeof(int), cudaMemcpyHostToDevice));
+  CKK(cudaMemcpy(d.rtl, rtl.data(), rtl.size() * sizeof(int4), cudaMemcpyHostToDevice));
   CKK(cudaMemset(d.ctr, 0, sizeof(unsigned)));
   KfState s{};
   s.lam = lam_ini;
@@ -292,22 +351,22 @@ int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
   KfRowArgs ra{rows, ld, xi, scale};
   if (kbase == 0) {  // start of a sequence: the products with its first row
     CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
-    LAUNCH("k_kf_tiles", s,
-           (k_kf_tiles<KM_PJ><<<d.ntile, 256, 0, s>>>(d.tiles, d.P, d.nw, d.pj, d.st, w, ra, 0,
-                                                       d.part)));
+    LAUNCH("k_kf_tiles_pj", s,
+           (d.dense ? k_kf_tiles<KM_PJ, true> : k_kf_tiles<KM_PJ, false>)<<<d.ntile, 256, 0, s>>>(
+               d.tiles, d.P, d.nw, d.pj, d.st, w, ra, 0, d.part));
   }
   for (int k = 0; k < nobs; ++k) {
     LAUNCH("k_kf_reduce", s,
-           (k_kf_reduce<<<d.nred, RED_THREADS, 0, s>>>(d.nw, d.rt, d.part, d.pj, ra, k, kbase,
+           (k_kf_reduce<<<d.nred, RED_THREADS, 0, s>>>(d.rtl, d.part, d.pj, ra, k, kbase,
                                                        d.dotp, d.ctr, d.st)));
     if (k + 1 < nobs || has_next)
       LAUNCH("k_kf_tiles", s,
-             (k_kf_tiles<KM_UPD_PJ><<<d.ntile, 256, 0, s>>>(d.tiles, d.P, d.nw, d.pj, d.st, w,
-                                                             ra, k + 1, d.part)));
+             (d.dense ? k_kf_tiles<KM_UPD_PJ, true> : k_kf_tiles<KM_UPD_PJ, false>)<<<
+                 d.ntile, 256, 0, s>>>(d.tiles, d.P, d.nw, d.pj, d.st, w, ra, k + 1, d.part));
     else
       LAUNCH("k_kf_tiles", s,
-             (k_kf_tiles<KM_UPD><<<d.ntile, 256, 0, s>>>(d.tiles, d.P, d.nw, d.pj, d.st, w, ra,
-                                                          0, d.part)));
+             (d.dense ? k_kf_tiles<KM_UPD, true> : k_kf_tiles<KM_UPD, false>)<<<
+                 d.ntile, 256, 0, s>>>(d.tiles, d.P, d.nw, d.pj, d.st, w, ra, 0, d.part));
   }
   CKK(cudaGetLastError());
   return RC_OK;
@@ -336,7 +395,7 @@ int kf_read_cov(const KfDev &d, const std::vector<int> &bsz, const std::vector<i
     const int n = t.y;
     for (int r = 0; r < KT; ++r)
       for (int c = 0; c < KT; ++c) {
-        const int R = t.z * KT + r, C = t.w * KT + c;
+        const int R = (t.z & 0xffff) * KT + r, C = (t.z >> 16) * KT + c;
         if (R >= n || C >= n) continue;
         const double v = h[(size_t)i * KTE + r * KT + c];
         if (dense) {
