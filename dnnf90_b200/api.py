@@ -47,7 +47,8 @@ EXTENSION_SYMBOLS = [
     "dnnf90_tune_report", "dnnf90_tune_force", "dnnf90_tabset_free",
     "dnnf90_seed_rule_sys", "dnnf90_grad_sys_batch", "dnnf90_grad_value_batch",
     "dnnf90_ngd_step_dual", "dnnf90_kf_create", "dnnf90_kf_free", "dnnf90_kf_update_rows",
-    "dnnf90_kf_update_rows_dev", "dnnf90_kf_read",
+    "dnnf90_kf_update_rows_dev", "dnnf90_kf_read", "dnnf90_kf_iekf_begin",
+    "dnnf90_kf_iekf_iter",
 ]
 
 _lib = None
@@ -139,6 +140,8 @@ def lib():
         "dnnf90_kf_update_rows": [i, i, pd, pd, pd],
         "dnnf90_kf_update_rows_dev": [i, i, p, p, p, p, p],
         "dnnf90_kf_read": [i, pd, pi, pd],
+        "dnnf90_kf_iekf_begin": [i],
+        "dnnf90_kf_iekf_iter": [i, pd, d, d, i],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -459,6 +462,15 @@ class Kalman:
         sc = None if scale is None else _f64(np.broadcast_to(scale, xi.shape))
         call("dnnf90_kf_update_rows", self.kid, rows.shape[0], _pd(rows), _pd(xi),
              None if sc is None else _pd(sc))
+
+    def iekf_begin(self):
+        """The network's current weights become the prior of the iteration."""
+        call("dnnf90_kf_iekf_begin", self.kid)
+
+    def iekf_iter(self, row, resid, rnoise, final):
+        """One relinearisation from dR/dw and R at the current weights."""
+        call("dnnf90_kf_iekf_iter", self.kid, _pd(_f64(row)), float(resid), float(rnoise),
+             int(bool(final)))
 
     def state(self):
         lam = ctypes.c_double()

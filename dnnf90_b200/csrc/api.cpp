@@ -1766,6 +1766,61 @@ int dnnf90_kf_update_rows_dev(int kid, int nobs, const double *rows_dev, const d
   return kf_status_rc(s);
 }
 
+int dnnf90_kf_iekf_begin(int kid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = kf_check(kid);
+  if (rc) return rc;
+  KfH &k = g_kf[kid];
+  const NetH &n = g_net[k.nid];
+  if ((rc = ck(cudaMemcpy(k.d.wprior, n.w.data(), n.w.size() * 8, cudaMemcpyHostToDevice),
+               "H2D")))
+    return rc;
+  k.d.prior = true;
+  return RC_OK;
+}
+
+int dnnf90_kf_iekf_iter(int kid, const double *row, double resid, double rnoise, int final) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = kf_check(kid);
+  if (rc) return rc;
+  if (!row) return RC_BAD_ARG;
+  KfH &k = g_kf[kid];
+  if (!k.d.prior) {
+    set_error("kf_iekf_iter: no prior (call dnnf90_kf_iekf_begin first)");
+    return RC_BAD_ARG;
+  }
+  if (!(rnoise > 0.0)) {  // kf_iekf_iter :547-550
+    set_error("kf_iekf_iter: observation noise must be > 0");
+    return RC_BAD_ARG;
+  }
+  NetH &n = g_net[k.nid];
+  flush_for_net(k.nid);
+  if (!k.st && (rc = ck(cudaStreamCreateWithFlags(&k.st, cudaStreamNonBlocking), "stream")))
+    return rc;
+  const size_t nw = n.w.size();
+  const size_t need = (2 * nw + 2) * sizeof(double);
+  if (k.d.stage_bytes < need) {
+    cudaFree(k.d.stage);
+    k.d.stage = nullptr;
+    k.d.stage_bytes = 0;
+    if ((rc = ck(cudaMalloc(&k.d.stage, need), "cudaMalloc"))) return rc;
+    k.d.stage_bytes = need;
+  }
+  double *dw = k.d.stage, *dr = dw + nw, *dsc = dr + nw;
+  const double sc[2] = {1.0 / std::sqrt(rnoise), resid};
+  if ((rc = ck(cudaMemcpyAsync(dw, n.w.data(), nw * 8, cudaMemcpyHostToDevice, k.st), "H2D")) ||
+      (rc = ck(cudaMemcpyAsync(dr, row, nw * 8, cudaMemcpyHostToDevice, k.st), "H2D")) ||
+      (rc = ck(cudaMemcpyAsync(dsc, sc, 16, cudaMemcpyHostToDevice, k.st), "H2D")))
+    return rc;
+  if ((rc = kf_iekf(k.d, dr, dsc + 1, dsc, dw, final != 0, k.st))) return rc;
+  if ((rc = ck(cudaMemcpyAsync(n.w.data(), dw, nw * 8, cudaMemcpyDeviceToHost, k.st), "D2H")))
+    return rc;
+  KfState s;
+  if ((rc = kf_state(k.d, &s, k.st))) return rc;
+  n.wver++;
+  return kf_status_rc(s);
+}
+
 int dnnf90_kf_read(int kid, double *lam, int *ngated, double *P) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (kid < 1 || kid > MAXH || !g_kf[kid].used) return RC_BAD_ARG;

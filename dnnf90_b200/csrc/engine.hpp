@@ -218,9 +218,11 @@ struct KfDev {
   double *part = nullptr;    // per block [row tile][slot][32]: partial products
                              // of P with the next row
   double *pj = nullptr;      // [nw] P j of the observation being applied
-  double *dotp = nullptr;    // per row tile: its share of j.Pj
+  double *dotp = nullptr;    // per row tile: its shares of j.Pj and of j.(w- - w)
   unsigned *ctr = nullptr;   // reduce CTAs finished
   KfState *st = nullptr;
+  double *wprior = nullptr;  // [nw] iterated EKF: the prior weights
+  bool prior = false;        // set by an IEKF begin
   double *stage = nullptr;   // host-call staging (rows, innovations, scales, weights)
   size_t stage_bytes = 0;
   void release();
@@ -238,6 +240,12 @@ int kf_create(KfDev &d, const std::vector<int> &bsz, const std::vector<int> &bof
 // first), whose products its last tile pass forms.
 int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
            const double *scale, double *w, cudaStream_t s, int kbase, bool has_next);
+// one relinearisation of the iterated EKF (kf_iekf_iter): row = dR/dw at
+// the current weights w, resid[0] = R, scale[0] = 1/sqrt(rnoise); w <- w- +
+// kv xi with the prior d.wprior; the covariance and lambda change only when
+// final
+int kf_iekf(KfDev &d, const double *row, const double *resid, const double *scale, double *w,
+            bool final, cudaStream_t s);
 int kf_state(const KfDev &d, KfState *out, cudaStream_t s);
 // covariance to the host: dense [nw][nw], or the blocks [bsz][bsz] one after another
 int kf_read_cov(const KfDev &d, const std::vector<int> &bsz, const std::vector<int> &boff,

@@ -64,6 +64,14 @@ struct KfRowArgs {
   const double *scale; // [nobs] or null (1)
 };
 
+// iterated EKF: the prior weights and the current ones (wprior null: a
+// plain update)
+struct KfIekf {
+  const double *wprior;
+  const double *w;
+  int final;
+};
+
 __device__ __forceinline__ double row_scale(const KfRowArgs &a, int k) {
   return a.scale ? a.scale[k] : 1.0;
 }
@@ -88,8 +96,10 @@ __global__ void __launch_bounds__(256, 8) k_kf_tiles(const int4 *__restrict__ ti
                                                      double *__restrict__ P, int nw,
                                                      const double *__restrict__ pj,
                                                      KfState *__restrict__ st,
-                                                     double *__restrict__ w, KfRowArgs ra,
-                                                     int knext, double *__restrict__ part) {
+                                                     double *__restrict__ w,
+                                                     const double *__restrict__ wb,
+                                                     KfRowArgs ra, int knext,
+                                                     double *__restrict__ part) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // the tile's own elements first: their addresses depend on nothing else,
   // so the HBM reads are in flight while the scalars and vectors arrive.
@@ -169,7 +179,7 @@ __global__ void __launch_bounds__(256, 8) k_kf_tiles(const int4 *__restrict__ ti
     }
     if (I == J && threadIdx.x < KT) {
       const int R = I * KT + lane;
-      if (R < n) w[o + R] = w[o + R] + s_kvR[lane] * xi;
+      if (R < n) w[o + R] = wb[o + R] + s_kvR[lane] * xi;
     }
   }
   if (MODE != KM_UPD) {
@@ -205,7 +215,7 @@ __global__ void __launch_bounds__(256, 8) k_kf_tiles(const int4 *__restrict__ ti
 __global__ void __launch_bounds__(RED_THREADS) k_kf_reduce(const int4 *__restrict__ rtl,
                                                            const double *__restrict__ part,
                                                            double *__restrict__ pj, KfRowArgs ra,
-                                                           int k, int kbase,
+                                                           int k, int kbase, KfIekf ie,
                                                            double *__restrict__ dotp,
                                                            unsigned *__restrict__ ctr,
                                                            KfState *__restrict__ st) {
@@ -221,18 +231,24 @@ __global__ void __launch_bounds__(RED_THREADS) k_kf_reduce(const int4 *__restric
   s_sum[g][lane] = s;
   __syncthreads();
   if (g == 0) {
-    double p = 0.0, prod = 0.0;
+    double p = 0.0, prod = 0.0, corr = 0.0;
 #pragma unroll
     for (int u = 0; u < RED_THREADS / 32; ++u) p += s_sum[u][lane];
     if (lane < rt.y) {
       const int R = rt.x + lane;
+      const double jf = row_scale(ra, k) * ra.rows[(size_t)k * ra.ld + R];
       pj[R] = p;
-      prod = row_scale(ra, k) * ra.rows[(size_t)k * ra.ld + R] * p;
+      prod = jf * p;
+      if (ie.wprior) corr = jf * (ie.wprior[R] - ie.w[R]);
     }
 #pragma unroll
-    for (int off = 16; off; off >>= 1) prod += __shfl_xor_sync(0xffffffffu, prod, off);
+    for (int off = 16; off; off >>= 1) {
+      prod += __shfl_xor_sync(0xffffffffu, prod, off);
+      corr += __shfl_xor_sync(0xffffffffu, corr, off);
+    }
     if (lane == 0) {
-      dotp[blockIdx.x] = prod;
+      dotp[2 * blockIdx.x] = prod;
+      dotp[2 * blockIdx.x + 1] = corr;
       __threadfence();
       s_last = atomicAdd(ctr, 1u) == gridDim.x - 1;
     }
@@ -240,8 +256,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_kf_reduce(const int4 *__restric
   __syncthreads();
   if (!s_last || threadIdx.x != 0) return;
   __threadfence();
-  double dot = 0.0;
-  for (unsigned b = 0; b < gridDim.x; ++b) dot += ((volatile double *)dotp)[b];
+  double dot = 0.0, cor = 0.0;
+  for (unsigned b = 0; b < gridDim.x; ++b) {
+    dot += ((volatile double *)dotp)[2 * b];
+    cor += ((volatile double *)dotp)[2 * b + 1];
+  }
   *ctr = 0;
   const double lam = st->lam;
   double denom = lam + dot;
@@ -249,24 +268,39 @@ __global__ void __launch_bounds__(RED_THREADS) k_kf_reduce(const int4 *__restric
     st->status = kbase + k + 1;
     return;
   }
-  double xi = row_scale(ra, k) * ra.xi[k];
-  double sg = 1.0;
-  const double gate = st->gate;
-  if (gate > 0.0) {
-    const double jpj = denom - lam;
-    if (xi * xi > gate * gate * denom) {
-      const double s2 = gate * gate * lam / (xi * xi - gate * gate * jpj);
-      sg = sqrt(s2);
-      xi = sg * xi;
-      denom = lam + s2 * jpj;
-      st->ngated += 1;
+  double xi, sg = 1.0;
+  if (ie.wprior) {
+    // iterated EKF (kf_iekf_iter :534-640): the innovation linearised at the
+    // prior, xi = -scale R - jf.(w- - w_i); no gate; lambda advances only
+    // with the covariance on the final iteration
+    xi = -row_scale(ra, k) * ra.xi[k] - cor;
+  } else {
+    xi = row_scale(ra, k) * ra.xi[k];
+    const double gate = st->gate;
+    if (gate > 0.0) {
+      const double jpj = denom - lam;
+      if (xi * xi > gate * gate * denom) {
+        const double s2 = gate * gate * lam / (xi * xi - gate * gate * jpj);
+        sg = sqrt(s2);
+        xi = sg * xi;
+        denom = lam + s2 * jpj;
+        st->ngated += 1;
+      }
     }
   }
   st->lamk = lam;
   st->denom = denom;
   st->sg = sg;
   st->xi = xi;
-  st->lam = __dadd_rn(__dmul_rn(st->lam0, lam), 1.0) - st->lam0;
+  if (!ie.wprior || ie.final) st->lam = __dadd_rn(__dmul_rn(st->lam0, lam), 1.0) - st->lam0;
+}
+
+// w = w- + kv xi without touching the covariance (a non-final IEKF iteration)
+__global__ void k_kf_wonly(int nw, double *__restrict__ w, const double *__restrict__ wb,
+                           const double *__restrict__ pj, const KfState *__restrict__ st) {
+  if (st->status) return;
+  const int R = blockIdx.x * blockDim.x + threadIdx.x;
+  if (R < nw) w[R] = wb[R] + (st->sg * pj[R] / st->denom) * st->xi;
 }
 
 __global__ void k_kf_init_tiles(const int4 *__restrict__ tiles, double *__restrict__ P, double p0) {
@@ -289,6 +323,7 @@ void KfDev::release() {
   cudaFree(ctr);
   cudaFree(st);
   cudaFree(stage);
+  cudaFree(wprior);
   *this = KfDev();
 }
 
@@ -327,7 +362,8 @@ int kf_create(KfDev &d, const std::vector<int> &bsz, const std::vector<int> &bof
   CKK(cudaMalloc(&d.rtl, rtl.size() * sizeof(int4)));
   CKK(cudaMalloc(&d.part, pslots * sizeof(double)));
   CKK(cudaMalloc(&d.pj, nw * sizeof(double)));
-  CKK(cudaMalloc(&d.dotp, d.nred * sizeof(double)));
+  CKK(cudaMalloc(&d.dotp, 2 * d.nred * sizeof(double)));
+  CKK(cudaMalloc(&d.wprior, nw * sizeof(double)));
   CKK(cudaMalloc(&d.ctr, sizeof(unsigned)));
   CKK(cudaMalloc(&d.st, sizeof(KfState)));
   CKK(cudaMemcpy(d.tiles, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice));
@@ -353,21 +389,45 @@ int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
     CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
     LAUNCH("k_kf_tiles_pj", s,
            (d.dense ? k_kf_tiles<KM_PJ, true> : k_kf_tiles<KM_PJ, false>)<<<d.ntile, 256, 0, s>>>(
-               d.tiles, d.P, d.nw, d.pj, d.st, w, ra, 0, d.part));
+               d.tiles, d.P, d.nw, d.pj, d.st, w, w, ra, 0, d.part));
   }
+  const KfIekf plain{nullptr, nullptr, 0};
   for (int k = 0; k < nobs; ++k) {
     LAUNCH("k_kf_reduce", s,
            (k_kf_reduce<<<d.nred, RED_THREADS, 0, s>>>(d.rtl, d.part, d.pj, ra, k, kbase,
-                                                       d.dotp, d.ctr, d.st)));
+                                                       plain, d.dotp, d.ctr, d.st)));
     if (k + 1 < nobs || has_next)
       LAUNCH("k_kf_tiles", s,
              (d.dense ? k_kf_tiles<KM_UPD_PJ, true> : k_kf_tiles<KM_UPD_PJ, false>)<<<
-                 d.ntile, 256, 0, s>>>(d.tiles, d.P, d.nw, d.pj, d.st, w, ra, k + 1, d.part));
+                 d.ntile, 256, 0, s>>>(d.tiles, d.P, d.nw, d.pj, d.st, w, w, ra, k + 1, d.part));
     else
       LAUNCH("k_kf_tiles", s,
              (d.dense ? k_kf_tiles<KM_UPD, true> : k_kf_tiles<KM_UPD, false>)<<<
-                 d.ntile, 256, 0, s>>>(d.tiles, d.P, d.nw, d.pj, d.st, w, ra, 0, d.part));
+                 d.ntile, 256, 0, s>>>(d.tiles, d.P, d.nw, d.pj, d.st, w, w, ra, 0, d.part));
   }
+  CKK(cudaGetLastError());
+  return RC_OK;
+}
+
+int kf_iekf(KfDev &d, const double *row, const double *resid, const double *scale, double *w,
+            bool final, cudaStream_t s) {
+  KfRowArgs ra{row, (size_t)d.nw, resid, scale};
+  const KfIekf ie{d.wprior, w, final ? 1 : 0};
+  CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
+  LAUNCH("k_kf_tiles_pj", s,
+         (d.dense ? k_kf_tiles<KM_PJ, true> : k_kf_tiles<KM_PJ, false>)<<<d.ntile, 256, 0, s>>>(
+             d.tiles, d.P, d.nw, d.pj, d.st, w, w, ra, 0, d.part));
+  LAUNCH("k_kf_reduce", s,
+         (k_kf_reduce<<<d.nred, RED_THREADS, 0, s>>>(d.rtl, d.part, d.pj, ra, 0, 0, ie, d.dotp,
+                                                     d.ctr, d.st)));
+  if (final)
+    LAUNCH("k_kf_tiles", s,
+           (d.dense ? k_kf_tiles<KM_UPD, true> : k_kf_tiles<KM_UPD, false>)<<<d.ntile, 256, 0,
+                                                                              s>>>(
+               d.tiles, d.P, d.nw, d.pj, d.st, w, d.wprior, ra, 0, d.part));
+  else
+    LAUNCH("k_kf_wonly", s,
+           (k_kf_wonly<<<(d.nw + 255) / 256, 256, 0, s>>>(d.nw, w, d.wprior, d.pj, d.st)));
   CKK(cudaGetLastError());
   return RC_OK;
 }

@@ -133,6 +133,18 @@ int dnnf90_kf_update_rows(int kid, int nobs, const double *rows, const double *x
 int dnnf90_kf_update_rows_dev(int kid, int nobs, const double *rows_dev,
                               const double *xi_dev, const double *scale_dev,
                               double *w_dev, void *stream);
+/* iterated EKF (kf_iekf_begin / kf_iekf_iter, :509-640): begin stores the
+ * network's current weights as the prior w-.  Each iteration takes
+ * row = dR/dw and resid = R evaluated by the caller at the network's current
+ * weights w_i, and sets the weights to w- + K_i (-s R - s row.(w- - w_i)),
+ * s = 1/sqrt(rnoise), with the gain from the unchanged prior covariance.
+ * final != 0 also downdates the covariance and advances lambda, so one
+ * observation costs one covariance update however many iterations it
+ * takes; one final iteration is the plain update.  The gate does not
+ * apply.  -1 without a prior, for rnoise <= 0 or a nonpositive
+ * denominator. */
+int dnnf90_kf_iekf_begin(int kid);
+int dnnf90_kf_iekf_iter(int kid, const double *row, double resid, double rnoise, int final);
 /* filter state: lambda, the count of gated updates, and (P not NULL) the
  * covariance, dense [nw][nw] or the decoupled blocks [n_b][n_b] one after
  * another in the weight order */

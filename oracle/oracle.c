@@ -883,32 +883,20 @@ int orc_grad_sys_batch(const orc_tables *t, int nlayer, const int *dims, const d
   return 0;
 }
 
+static void kf_downdate(int nw, double *P, int nblk, const int *bsz, const int *boff,
+                        const double *kv, const double *pj, double lm, double q);
+static void kf_pj(int nw, const double *P, int nblk, const int *bsz, const int *boff,
+                  const double *jf, double *pj);
+
 int orc_kf_update(int nw, double *w, double *P, int nblk, const int *bsz, const int *boff,
                   const double *jrow, double xi_in, double scale, double *lam, double lam0,
                   double q, double gate, int *ngated) {
-  double *jf = (double *)malloc(sizeof(double) * nw);
+  double *jf = (double *)calloc(nw > 0 ? nw : 1, sizeof(double));
   double *pj = (double *)malloc(sizeof(double) * nw);
   double *kv = (double *)malloc(sizeof(double) * nw);
   double xi = scale * xi_in;
   for (int m = 0; m < nw; ++m) jf[m] = scale * jrow[m];
-  if (nblk > 0) { /* decoupled: P j per node block */
-    const double *Pb = P;
-    for (int b = 0; b < nblk; ++b) {
-      const int n = bsz[b], o = boff[b];
-      for (int i = 0; i < n; ++i) {
-        double s = 0.0;
-        for (int r = 0; r < n; ++r) s += Pb[(size_t)r * n + i] * jf[o + r];
-        pj[o + i] = s;
-      }
-      Pb += (size_t)n * n;
-    }
-  } else {
-    for (int i = 0; i < nw; ++i) {
-      double s = 0.0;
-      for (int r = 0; r < nw; ++r) s += P[(size_t)r * nw + i] * jf[r];
-      pj[i] = s;
-    }
-  }
+  kf_pj(nw, P, nblk, bsz, boff, jf, pj);
   double dot = 0.0;
   for (int m = 0; m < nw; ++m) dot += jf[m] * pj[m];
   double denom = *lam + dot;
@@ -929,9 +917,69 @@ int orc_kf_update(int nw, double *w, double *P, int nblk, const int *bsz, const 
   }
   for (int m = 0; m < nw; ++m) kv[m] = pj[m] / denom;
   for (int m = 0; m < nw; ++m) w[m] = w[m] + kv[m] * xi;
-  /* downdate (P - kv pj^T) / lambda, then the average with the transpose
-   * and the process noise on the diagonal */
-  const double lm = *lam;
+  kf_downdate(nw, P, nblk, bsz, boff, kv, pj, *lam, q);
+  *lam = lam0 * *lam + 1.0 - lam0;
+  free(jf); free(pj); free(kv);
+  return 0;
+}
+
+/* P j per block (dense: nblk = 0) */
+static void kf_pj(int nw, const double *P, int nblk, const int *bsz, const int *boff,
+                  const double *jf, double *pj) {
+  if (nblk > 0) {
+    const double *Pb = P;
+    for (int b = 0; b < nblk; ++b) {
+      const int n = bsz[b], o = boff[b];
+      for (int i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int r = 0; r < n; ++r) s += Pb[(size_t)r * n + i] * jf[o + r];
+        pj[o + i] = s;
+      }
+      Pb += (size_t)n * n;
+    }
+  } else {
+    for (int i = 0; i < nw; ++i) {
+      double s = 0.0;
+      for (int r = 0; r < nw; ++r) s += P[(size_t)r * nw + i] * jf[r];
+      pj[i] = s;
+    }
+  }
+}
+
+int orc_kf_iekf_iter(int nw, double *w, const double *wprior, double *P, int nblk,
+                     const int *bsz, const int *boff, const double *jrow, double resid,
+                     double rnoise, double *lam, double lam0, double q, int final) {
+  if (!(rnoise > 0.0)) return -1;
+  const double scale = 1.0 / sqrt(rnoise);
+  double *jf = (double *)calloc(nw > 0 ? nw : 1, sizeof(double));
+  double *pj = (double *)malloc(sizeof(double) * nw);
+  double *kv = (double *)malloc(sizeof(double) * nw);
+  for (int m = 0; m < nw; ++m) jf[m] = scale * jrow[m];
+  kf_pj(nw, P, nblk, bsz, boff, jf, pj);
+  double dot = 0.0;
+  for (int m = 0; m < nw; ++m) dot += jf[m] * pj[m];
+  const double denom = *lam + dot;
+  if (!(denom > 0.0)) {
+    free(jf); free(pj); free(kv);
+    return -1;
+  }
+  for (int m = 0; m < nw; ++m) kv[m] = pj[m] / denom;
+  double corr = 0.0;
+  for (int m = 0; m < nw; ++m) corr += jf[m] * (wprior[m] - w[m]);
+  const double xi = -scale * resid - corr;
+  for (int m = 0; m < nw; ++m) w[m] = wprior[m] + kv[m] * xi;
+  if (final) {
+    kf_downdate(nw, P, nblk, bsz, boff, kv, pj, *lam, q);
+    *lam = lam0 * *lam + 1.0 - lam0;
+  }
+  free(jf); free(pj); free(kv);
+  return 0;
+}
+
+/* (P - kv pj^T) / lambda, the average with the transpose and the process
+ * noise on the diagonal, per block (kf_update_grad :449-489) */
+static void kf_downdate(int nw, double *P, int nblk, const int *bsz, const int *boff,
+                        const double *kv, const double *pj, double lm, double q) {
   if (nblk > 0) {
     double *Pb = P;
     for (int b = 0; b < nblk; ++b) {
@@ -962,9 +1010,6 @@ int orc_kf_update(int nw, double *w, double *P, int nblk, const int *bsz, const 
     if (q > 0.0)
       for (int i = 0; i < nw; ++i) P[(size_t)i * nw + i] += q;
   }
-  *lam = lam0 * *lam + 1.0 - lam0;
-  free(jf); free(pj); free(kv);
-  return 0;
 }
 
 int orc_eval_batch(const orc_tables *t, int nlayer, const int *dims,

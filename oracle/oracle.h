@@ -163,6 +163,16 @@ int orc_kf_update(int nw, double *w, double *P, int nblk, const int *bsz, const 
                   const double *jrow, double xi_in, double scale, double *lam, double lam0,
                   double q, double gate, int *ngated);
 
+/* One relinearisation of the iterated EKF, kf_iekf_iter
+ * (lib/kalman_module.f90:534-640): jrow = dR/dw at the current weights w,
+ * resid = R there, scale = 1/sqrt(rnoise).  w <- wprior + kv xi with
+ * xi = -scale resid - (scale jrow).(wprior - w); the covariance and lambda
+ * change only when final != 0.  No innovation gate.  -1 on rnoise <= 0 or a
+ * nonpositive denominator. */
+int orc_kf_iekf_iter(int nw, double *w, const double *wprior, double *P, int nblk,
+                     const int *bsz, const int *boff, const double *jrow, double resid,
+                     double rnoise, double *lam, double lam0, double q, int final);
+
 /* Forward only over a batch (net_eval_hod per point). */
 int orc_eval_batch(const orc_tables *t, int nlayer, const int *dims,
                    const double *w, int npts, const double *X, double *tout,

@@ -53,6 +53,7 @@ def lib():
         L.orc_act_derivs.argtypes = [vp, cd, ci, vp]
         L.orc_besj_all.argtypes = [ci, cd, vp]
         L.orc_kf_update.argtypes = [ci, vp, vp, ci, vp, vp, vp, cd, cd, vp, cd, cd, cd, vp]
+        L.orc_kf_iekf_iter.argtypes = [ci, vp, vp, vp, ci, vp, vp, vp, cd, cd, vp, cd, cd, ci]
         L.orc_tables_set_activation.argtypes = [vp, ci]
         L.orc_weight_count.argtypes = [ci, P(ci)]
         L.orc_eval_point.argtypes = [vp, ci, P(ci), vp, vp, vp, vp]
@@ -288,6 +289,25 @@ class Kalman:
                                  self.q, self.gate, ctypes.byref(self.ngated))
         if rc != 0:
             raise ValueError("oracle kf_update: nonpositive innovation denominator")
+        self.lam = lam.value
+
+    def iekf_begin(self, w):
+        """kf_iekf_begin: the prior is the current weights."""
+        self.wprior = np.array(w, np.float64)
+
+    def iekf_iter(self, w, jrow, resid, rnoise, final):
+        """kf_iekf_iter: one relinearisation from jrow = dR/dw and R at the
+        current weights w (updated in place)."""
+        assert w.dtype == np.float64 and w.flags.c_contiguous
+        lam = ctypes.c_double(self.lam)
+        jr = np.ascontiguousarray(jrow, np.float64)
+        nb = 0 if self.bsz is None else len(self.bsz)
+        rc = lib().orc_kf_iekf_iter(self.nw, _p(w), _p(self.wprior), _p(self.P), nb,
+                                    _p(self.bsz), _p(self.boff), _p(jr), float(resid),
+                                    float(rnoise), ctypes.byref(lam), self.lam0, self.q,
+                                    int(bool(final)))
+        if rc != 0:
+            raise ValueError("oracle kf_iekf_iter: bad noise or nonpositive denominator")
         self.lam = lam.value
 
 

@@ -249,3 +249,81 @@ def test_kalman_argument_checks():
     kf.free()
     assert api.lib().dnnf90_kf_free(kid) < 0      # freed twice
     ts.free()
+
+
+# ------------------------------------------------- iterated EKF (kf_iekf_*)
+
+
+def _obs(a, z):
+    """A nonlinear scalar observation h(w) = sum a_i sin(w_i) with target z:
+    R(w) = h(w) - z and dR/dw = a cos(w)."""
+    return (lambda w: float(a @ np.sin(w)) - z), (lambda w: a * np.cos(w))
+
+
+def test_oracle_one_final_iteration_is_the_plain_update():
+    dims = [3, 6, 1]
+    nw = po.weight_count(dims)
+    rng = np.random.default_rng(8)
+    w0 = rng.normal(size=nw)
+    R, J = _obs(rng.normal(size=nw), 0.3)
+    for dec in (False, True):
+        a, b = po.Kalman(dims, 0.5, 0.98, 0.99, dec, 1e-3), po.Kalman(dims, 0.5, 0.98, 0.99, dec, 1e-3)
+        wa, wb = w0.copy(), w0.copy()
+        a.iekf_begin(wa)
+        a.iekf_iter(wa, J(wa), R(wa), 0.25, True)
+        b.update(wb, J(w0), -R(w0), 1.0 / np.sqrt(0.25))
+        assert np.array_equal(wa, wb) and np.array_equal(a.P, b.P) and a.lam == b.lam
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("decoupled", [False, True])
+def test_device_iekf_matches_the_oracle(decoupled):
+    from dnnf90_b200 import api
+    dims = [3, 20, 20, 1]
+    nw = po.weight_count(dims)
+    rng = np.random.default_rng(9)
+    w0 = rng.normal(size=nw) * 0.5
+    net, ts = _net(dims, w0)
+    kf = api.Kalman(net, 0.3, 0.98, 0.9987, decoupled, 1e-4, gate=0.5)  # the gate is ignored
+    ref = po.Kalman(dims, 0.3, 0.98, 0.9987, decoupled, 1e-4, gate=0.5)
+    wref = w0.copy()
+    for obs in range(3):
+        R, J = _obs(rng.normal(size=nw) / np.sqrt(nw), rng.normal())
+        kf.iekf_begin()
+        ref.iekf_begin(wref)
+        for it in range(3):
+            final = it == 2
+            wd = net.get_weights()
+            kf.iekf_iter(J(wd), R(wd), 0.5, final)
+            ref.iekf_iter(wref, J(wref), R(wref), 0.5, final)
+            assert rel_err(net.get_weights(), wref) < 1e-11
+        assert abs(kf.state()[0] - ref.lam) <= 1e-15
+    assert rel_err(kf.cov().reshape(-1), ref.P) < 1e-11
+    assert kf.state()[1] == 0
+    kf.free(); net.free(); ts.free()
+
+
+@pytest.mark.gpu
+def test_device_iekf_single_final_iteration_is_the_plain_update():
+    from dnnf90_b200 import api
+    dims = [3, 20, 20, 1]
+    nw = po.weight_count(dims)
+    rng = np.random.default_rng(10)
+    w0 = rng.normal(size=nw) * 0.5
+    R, J = _obs(rng.normal(size=nw) / np.sqrt(nw), 0.2)
+    na, tsa = _net(dims, w0)
+    nb, tsb = _net(dims, w0)
+    a, b = api.Kalman(na, 0.3, 0.98, 0.9987), api.Kalman(nb, 0.3, 0.98, 0.9987)
+    a.iekf_begin()
+    a.iekf_iter(J(w0), R(w0), 0.5, True)
+    b.update_rows(J(w0), -R(w0), 1.0 / np.sqrt(0.5))
+    assert np.array_equal(na.get_weights(), nb.get_weights())
+    assert np.array_equal(a.cov(), b.cov()) and a.state() == b.state()
+    with pytest.raises(api.Dnnf90Error):
+        a.iekf_iter(J(w0), R(w0), 0.0, True)       # rnoise must be positive
+    c = api.Kalman(na, 0.3, 0.98, 0.9987)
+    with pytest.raises(api.Dnnf90Error):
+        c.iekf_iter(J(w0), R(w0), 0.5, True)       # no prior yet
+    for k in (a, b, c):
+        k.free()
+    na.free(); nb.free(); tsa.free(); tsb.free()
