@@ -48,7 +48,8 @@ EXTENSION_SYMBOLS = [
     "dnnf90_seed_rule_sys", "dnnf90_grad_sys_batch", "dnnf90_grad_value_batch",
     "dnnf90_ngd_step_dual", "dnnf90_kf_create", "dnnf90_kf_free", "dnnf90_kf_update_rows",
     "dnnf90_kf_update_rows_dev", "dnnf90_kf_read", "dnnf90_kf_iekf_begin",
-    "dnnf90_kf_iekf_iter",
+    "dnnf90_kf_iekf_iter", "dnnf90_ngd_gram_dev", "dnnf90_ngd_solve_dev",
+    "dnnf90_ngd_step_dual_dev",
 ]
 
 _lib = None
@@ -142,6 +143,9 @@ def lib():
         "dnnf90_kf_read": [i, pd, pi, pd],
         "dnnf90_kf_iekf_begin": [i],
         "dnnf90_kf_iekf_iter": [i, pd, d, d, i],
+        "dnnf90_ngd_gram_dev": [i, i, p, i, p, p],
+        "dnnf90_ngd_solve_dev": [i, p, p, i, d, p, p],
+        "dnnf90_ngd_step_dual_dev": [i, i, p, p, i, d, p, p],
     }
     for name, args in sig.items():
         f = getattr(L, name)

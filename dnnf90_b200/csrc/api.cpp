@@ -1613,6 +1613,32 @@ int dnnf90_committee_info(int *policy, float *graph_ms) {
   return g_comm_policy >= 0 ? RC_OK : RC_BAD_ARG;
 }
 
+int dnnf90_ngd_gram_dev(int nrow, int nw, const double *rows_dev, int prec, double *G_dev,
+                        void *stream) {
+  if (nrow < 1 || nw < 1 || !rows_dev || !G_dev) return RC_BAD_ARG;
+  if (prec != PREC_F64 && prec != PREC_SPLIT) return RC_BAD_ARG;
+  int rc = device_ready();
+  if (rc) return rc;
+  return ngd_gram_device(rows_dev, nrow, nw, G_dev, prec, (cudaStream_t)stream);
+}
+
+int dnnf90_ngd_solve_dev(int nw, double *G_dev, const double *b_dev, int nb, double mu,
+                         double *u_dev, void *stream) {
+  if (nw < 1 || nb < 1 || !G_dev || !b_dev || !u_dev) return RC_BAD_ARG;
+  int rc = device_ready();
+  if (rc) return rc;
+  return ngd_solve_device(G_dev, nw, b_dev, nb, mu, u_dev, (cudaStream_t)stream);
+}
+
+int dnnf90_ngd_step_dual_dev(int nrow, int nw, const double *rows_dev, const double *b_dev,
+                             int nb, double mu, double *u_dev, void *stream) {
+  if (nrow < 1 || nw < 1 || nb < 1 || !rows_dev || !b_dev || !u_dev) return RC_BAD_ARG;
+  int rc = device_ready();
+  if (rc) return rc;
+  return ngd_device_dual(rows_dev, nrow, nw, b_dev, nb, mu, u_dev, PREC_F64,
+                         (cudaStream_t)stream);
+}
+
 // ------------------------------------------------------------- Kalman filter
 int dnnf90_kf_create(int nid, double p0, double lam_ini, double lam0, int decoupled, double q,
                      double gate) {

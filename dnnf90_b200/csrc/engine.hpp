@@ -189,6 +189,12 @@ int adam_device(double *w, const double *g, double *m, double *v, int nw,
 // (prec), then Cholesky-factored and solved in FP64.
 int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
                double mu, double *u, int prec, cudaStream_t st);
+// The primal step in two halves: G = J^T J (lower triangle, FP64; prec as
+// above) and the damped solve u = (G / nb + mu I)^{-1} (b / nb), which
+// overwrites G with its factor
+int ngd_gram_device(const double *rows, int nrow, int nw, double *G, int prec, cudaStream_t st);
+int ngd_solve_device(double *G, int nw, const double *b, int nb, double mu, double *u,
+                     cudaStream_t st);
 // the same step by the dual (Gram-space) route, app/optimizer_module.f90:408-446
 int ngd_device_dual(const double *rows, int nrow, int nw, const double *b, int nb, double mu,
                     double *u, int prec, cudaStream_t st);

@@ -304,6 +304,25 @@ int ngd_device(const double *rows, int nrow, int nw, const double *b, int nb,
   return rc;
 }
 
+// The two halves of the primal step, for a step whose rows are spread over
+// ranks: each rank forms its own J^T J, the caller sums the metrics (and
+// the gradients) over the ranks, and every rank solves the summed system,
+// as app/optimizer_module.f90:310-321 does with sum_over_ranks.
+int ngd_gram_device(const double *rows, int nrow, int nw, double *G, int prec, cudaStream_t st) {
+  return gram(rows, nrow, nw, G, prec, st);
+}
+
+int ngd_solve_device(double *G, int nw, const double *b, int nb, double mu, double *u,
+                     cudaStream_t st) {
+  int *info = nullptr;
+  CKN(cudaMalloc(&info, sizeof(int)));
+  LAUNCH("k_scale_damp", st, k_scale_damp<<<1024, 256, 0, st>>>(G, nw, 1.0 / (double)nb, mu, b, u));
+  int rc = cudaGetLastError() == cudaSuccess ? RC_OK : RC_DEVICE;
+  if (!rc) rc = chol_solve(G, nw, u, info, st);
+  cudaFree(info);
+  return rc;
+}
+
 // ------------------------------------------------- dual (Gram-space) route
 // The dual route of app/optimizer_module.f90:408-446: with G = J^T J / nb
 // and the damping mu, the push-through identity gives

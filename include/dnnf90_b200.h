@@ -109,6 +109,21 @@ int dnnf90_ngd_step(int nid, int nrow, const double *rows, const double *b,
 int dnnf90_ngd_step_dual(int nid, int nrow, const double *rows, const double *b,
                          int nb, double mu, int prec, double *u);
 
+/* the primal step in two halves on device arrays, for rows spread over
+ * ranks (app/optimizer_module.f90:310-321): G_dev[nw][nw] = J^T J of this
+ * rank's rows (lower triangle; prec as in dnnf90_ngd_step), then, after the
+ * caller has summed G and b over the ranks, u_dev = (G / nb + mu I)^{-1}
+ * (b / nb) with nb the total row count.  The solve overwrites G_dev with
+ * its Cholesky factor. */
+int dnnf90_ngd_gram_dev(int nrow, int nw, const double *rows_dev, int prec, double *G_dev,
+                        void *stream);
+int dnnf90_ngd_solve_dev(int nw, double *G_dev, const double *b_dev, int nb, double mu,
+                         double *u_dev, void *stream);
+/* the dual route of dnnf90_ngd_step_dual on device arrays (rows gathered
+ * from every rank, app/optimizer_module.f90:303-307) */
+int dnnf90_ngd_step_dual_dev(int nrow, int nw, const double *rows_dev, const double *b_dev,
+                             int nb, double mu, double *u_dev, void *stream);
+
 /* ---- extended Kalman filter (lib/kalman_module.f90; new at the C boundary,
  * the reference reaches it from its trainer, app/lib_net_module.f90:455-570) */
 /* kf_init (:107-170) on network nid: P = p0 I, lambda = lam_ini, forgetting

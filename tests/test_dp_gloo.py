@@ -95,3 +95,75 @@ def test_two_gloo_ranks_sum_to_the_full_gradient():
         assert p.exitcode == 0
     assert rel_err(g, gref) < 1e-13
     assert abs(L - Lref) <= 1e-13 * abs(Lref)
+
+
+# ------------------------------------------------ sharded natural gradient
+
+
+class _CpuNGD:
+    """The device halves restated in numpy (CPU ranks have no device)."""
+
+    def gram(self, rows, G):
+        J = rows.numpy()
+        G.copy_(__import__("torch").from_numpy(np.tril(J.T @ J)))
+
+    def solve(self, G, b, nb, mu, u):
+        L = np.tril(G.numpy())
+        A = L + np.tril(L, -1).T
+        u.copy_(__import__("torch").from_numpy(
+            np.linalg.solve(A / nb + mu * np.eye(len(b)), b.numpy() / nb)))
+
+    def dual(self, rows, b, nb, mu, u):
+        J, bb = rows.numpy(), b.numpy() / nb
+        K = mu * np.eye(len(J)) + J @ J.T / nb
+        y = np.linalg.solve(K, J @ bb)
+        u.copy_(__import__("torch").from_numpy((bb - J.T @ y / nb) / mu))
+
+
+def _ngd_rank(rank, world, port, J, B, splits, out_q):
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from dnnf90_b200.dp import ngd_step_sharded
+
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        a, c = splits[rank], splits[rank + 1]
+        rows = torch.from_numpy(J[a:c].copy())
+        b = torch.from_numpy(B[rank].copy())
+        out = {}
+        for route in ("primal", "dual"):
+            out[route] = ngd_step_sharded(rows, b, 1e-3, route=route, ops=_CpuNGD()).numpy()
+        out_q.put((rank, out))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_natural_gradient_over_two_gloo_ranks():
+    """Rows split 9 : 4 over two ranks (the shares need not be equal): both
+    routes give the single-process step over all rows, on every rank."""
+    rng = np.random.default_rng(3)
+    nw, nrow = 20, 13
+    J = rng.normal(size=(nrow, nw))
+    B = rng.normal(size=(2, nw))
+    mu = 1e-3
+    G = J.T @ J / nrow + mu * np.eye(nw)
+    uref = np.linalg.solve(G, B.sum(axis=0) / nrow)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_ngd_rank, args=(r, 2, port, J, B, [0, 9, 13], q))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r in (0, 1):
+        for route in ("primal", "dual"):
+            assert rel_err(res[r][route], uref) < 1e-10, (r, route)

@@ -266,3 +266,37 @@ def test_ngd_dual_route_equals_the_primal_step():
     with pytest.raises(api.Dnnf90Error):
         api.ngd_step(net, rows, b, nb, 0.0, api.PREC_F64, dual=True)   # mu must be > 0
     r.free(); net.free(); ts.free()
+
+
+@pytest.mark.gpu
+def test_sharded_ngd_halves_on_the_device():
+    """The step for rows spread over ranks (dp.ngd_step_sharded) on one
+    device: the metric built in two row blocks and summed, then solved
+    (dnnf90_ngd_gram_dev + dnnf90_ngd_solve_dev), and the device dual route,
+    equal the host entry dnnf90_ngd_step on all rows."""
+    import torch
+    from dnnf90_b200.dp import DeviceNGD, ngd_step_sharded
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(21)
+    ts = api.TableSet(2, 1)
+    net = _net(ts, [2, 20, 20, 1], None, api.PREC_F64)   # the host entry takes nw from it
+    nw, nrow, mu = net.nw, 300, 1e-3
+    J = rng.normal(size=(nrow, nw)) / np.sqrt(nw)
+    b = rng.normal(size=nw)
+    up = api.ngd_step(net, J, b, nrow, mu, api.PREC_F64)
+    Jd, bd = torch.tensor(J, device=dev), torch.tensor(b, device=dev)
+    for prec, tol in ((0, 1e-10), (1, 1e-5)):
+        ops = DeviceNGD(prec)
+        u1 = ngd_step_sharded(Jd, bd, mu, ops=ops).cpu().numpy()
+        # two row blocks, their metrics summed as the all-reduce would
+        G = torch.zeros(nw, nw, dtype=torch.float64, device=dev)
+        G2 = torch.zeros_like(G)
+        ops.gram(Jd[:170].contiguous(), G)
+        ops.gram(Jd[170:].contiguous(), G2)
+        G += G2
+        u2 = torch.empty(nw, dtype=torch.float64, device=dev)
+        ops.solve(G, bd, nrow, mu, u2)
+        assert rel_err(u1, up) < tol and rel_err(u2.cpu().numpy(), up) < tol, prec
+    ud = ngd_step_sharded(Jd, bd, mu, route="dual").cpu().numpy()
+    assert rel_err(ud, up) < 1e-9
+    net.free(); ts.free()
