@@ -206,7 +206,9 @@ def tune_report() -> list:
 
 def tune_force(which: int, variant: int) -> None:
     """Pin the Bell forward (which 0) or adjoint (which 1) kernel variant;
-    variant -1 hands the choice back to the autotuner."""
+    variant -1 hands the choice back to the autotuner.  which 2 switches
+    the tanh series forward on where it applies (1) or off (0, -1: the
+    default)."""
     call("dnnf90_tune_force", which, variant)
 
 

@@ -33,9 +33,17 @@ namespace dnnf90 {
     }                                                                  \
   } while (0)
 
+// the tanh series forward (v9), off by default: it carries 2.7x fewer
+// multiply-adds than the Bell recurrence but loads 8 bytes of shared memory
+// per multiply-add against about 4 for the v8 bands, and measured slower
+// (C3: 24.9 against 20.0 ms per FP32 launch).  dnnf90_tune_force(2, 1)
+// switches it on.
+static std::atomic<bool> g_series_fwd{false};
+
 void DevBellPlan::release() {
   {
-    void *q[] = {f8.list, f8.hdr, f8.cpdst, f8.rec};
+    void *q[] = {f8.list, f8.hdr, f8.cpdst, f8.rec, f9.list, f9.hdr, f9.rec, f9.sdeg64,
+                 f9.sdeg32};
     for (void *p : q)
       if (p) cudaFree(p);
   }
@@ -153,6 +161,19 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
     d.f8.zuv = F.zuv;
     d.f8.smem = F.smem;
     d.f8.ok = F.ok;
+  }
+  {
+    const F9Plan &F = P.f9;
+    std::vector<float> s32(F.sdeg.begin(), F.sdeg.end());
+    if ((rc = put(&d.f9.list, F.list))) return rc;
+    if ((rc = put(&d.f9.hdr, F.hdr))) return rc;
+    if ((rc = put(&d.f9.rec, F.rec))) return rc;
+    if ((rc = put(&d.f9.sdeg64, F.sdeg))) return rc;
+    if ((rc = put(&d.f9.sdeg32, s32))) return rc;
+    d.f9.pbase = F.pbase;
+    d.f9.qbase = F.qbase;
+    d.f9.smem = F.smem;
+    d.f9.ok = F.ok;
   }
   d.f5_ok = P.f5_ok;
   d.nrows5 = P.nrows5;
@@ -877,6 +898,161 @@ __global__ void __launch_bounds__(BELL_WORKERS * 32) k_bell_fwd8(Fwd8Args a) {
   cp_async_wait<0>();
 }
 
+// ---------------------------------------------------------------- v9
+// tanh forward by the series identity of tanh' = 1 - tanh^2 (F9Plan):
+//   |a| t~_a = sum_{0<b<=a} |b| s~_b u~_{a-b},  u~_a = -sum_{b+c=a} t~_b t~_c,
+// T_a = a! t~_a and h_a = a! u~_a (h = sigma'(S) = 1 - T^2 for tanh).  One
+// record (b, c) adds (|b| s~_b, t~_b) * (u~_c, t~_c) to the pair (T sum,
+// U sum); the b = a and b = 0 terms are added after the loop.
+struct Fwd9Args {
+  int n, na, npts, iact, gy, pbase, qbase;
+  const double *tpc;
+  const int *list;     // [(K+1) * workers][2]
+  const int4 *hdr;     // ia, first record, records, 0
+  const uint4 *rec;    // two records (P offset, Q offset) per 16 bytes
+  const void *sc;      // [0, na): a!
+  const void *sdeg;    // [na]: |a| / a!
+  const void *S;
+  void *T, *h;
+};
+
+// (t, u) += (x0, x1) * (y0, y1) elementwise, one packed FP32 multiply-add
+__device__ __forceinline__ void fma_pp(float2 &acc, float2 x, float2 y) {
+  asm("{\n\t.reg .b64 a, xx, yy;\n\t"
+      "mov.b64 a, {%0, %1};\n\t"
+      "mov.b64 xx, {%2, %3};\n\t"
+      "mov.b64 yy, {%4, %5};\n\t"
+      "fma.rn.f32x2 a, xx, yy, a;\n\t"
+      "mov.b64 {%0, %1}, a;\n\t}"
+      : "+f"(acc.x), "+f"(acc.y)
+      : "f"(x.x), "f"(x.y), "f"(y.x), "f"(y.y));
+}
+__device__ __forceinline__ void fma_pp(double2 &acc, double2 x, double2 y) {
+  acc.x += x.x * y.x;
+  acc.y += x.y * y.y;
+}
+
+template <typename R, int P>
+__device__ __forceinline__ void fwd9_degree(const Fwd9Args &a, unsigned char *sm, uint32_t lp,
+                                            R t0, R u0, R *T, R *H, bool act, bool wr,
+                                            bool train, int warp) {
+  using PR = typename Pair<R>::T;
+  const int ts = __ldg(a.list + (P * BELL_WORKERS + warp) * 2);
+  const int tn = __ldg(a.list + (P * BELL_WORKERS + warp) * 2 + 1);
+  const R *sc = (const R *)a.sc;
+  for (int t = ts; t < ts + tn; ++t) {
+    const int4 hd = __ldg(a.hdr + t);
+    PR acc;
+    acc.x = (R)0;
+    acc.y = (R)0;
+    if constexpr (P >= 2) {
+      const uint4 *rq = a.rec + (hd.y >> 1);
+      const int m = hd.z >> 1;
+#pragma unroll 2
+      for (int e = 0; e < m; ++e) {
+        const uint4 r = __ldg(rq + e);
+        fma_pp(acc, srow<PR>(sm, r.x + lp), srow<PR>(sm, r.y + lp));
+        fma_pp(acc, srow<PR>(sm, r.z + lp), srow<PR>(sm, r.w + lp));
+      }
+    }
+    const int ia = hd.x;
+    const uint32_t pa = a.pbase + ia * 256 + lp;
+    const R sa = srow<R>(sm, pa);  // |a| s~_a
+    const R tt = (acc.x + sa * u0) * (R)(1.0 / P);
+    const R uu = -(acc.y + (R)2 * t0 * tt);
+    if (wr) {
+      srow<R>(sm, pa + sizeof(R)) = tt;
+      PR q;
+      q.x = uu;
+      q.y = tt;
+      srow<PR>(sm, a.qbase + ia * 256 + lp) = q;
+    }
+    if (act) {
+      const R fa = __ldg(sc + ia);
+      T[(size_t)ia * a.n] = fa * tt;
+      if (train) H[(size_t)ia * a.n] = fa * uu;
+    }
+  }
+}
+
+template <typename R, int KK, int NPB, bool TRAIN>
+__global__ void __launch_bounds__(BELL_WORKERS * 32) k_tanh_fwd9(Fwd9Args a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char *sm = smem_raw;
+  using PR = typename Pair<R>::T;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool lact = lane < NPB;
+  const int ln = lact ? lane : 0;
+  const int n = a.n, na = a.na;
+  const size_t plane = (size_t)na * n;
+  const R *sdeg = (const R *)a.sdeg;
+  const uint32_t lo = ln * sizeof(R), lp = ln * 2 * sizeof(R);
+  // zero rows: S row na, and the P and Q rows na that pad the record lists
+  if (threadIdx.x < 8) {
+    *(uint4 *)(sm + na * 128 + threadIdx.x * 16) = make_uint4(0, 0, 0, 0);
+  } else if (threadIdx.x < 24) {
+    *(uint4 *)(sm + a.pbase + na * 256 + (threadIdx.x - 8) * 16) = make_uint4(0, 0, 0, 0);
+  } else if (threadIdx.x < 40) {
+    *(uint4 *)(sm + a.qbase + na * 256 + (threadIdx.x - 24) * 16) = make_uint4(0, 0, 0, 0);
+  }
+  const long nitem = (long)a.npts * a.gy;
+  const long it0 = (long)blockIdx.x * nitem / gridDim.x;
+  const long it1 = (long)(blockIdx.x + 1) * nitem / gridDim.x;
+  if (it0 < it1)
+    stage_rows<NPB, R>(sm, (const R *)a.S + (it0 % a.npts) * plane, na, n,
+                       (int)(it0 / a.npts) * NPB, BELL_WORKERS * 32);
+  cp_async_commit();
+  for (long it = it0; it < it1; ++it) {
+    const int pt = (int)(it % a.npts);
+    const int j = (int)(it / a.npts) * NPB + ln;
+    const bool act = lact && j < n;
+    cp_async_wait<0>();
+    __syncthreads();  // this item's S rows are in; every warp is done with the last item
+    R *T = (R *)a.T + pt * plane + j;
+    R *H = TRAIN ? (R *)a.h + pt * plane + j : nullptr;
+    if (warp == 0 && lact) {
+      double d[KK + 2];  // the table's polynomials are laid out for K
+      sigma_derivs(a.iact, a.tpc, KK, (double)srow<R>(sm, lo), d);
+      PR q;
+      q.x = (R)d[1];
+      q.y = (R)d[0];
+      srow<PR>(sm, a.qbase + lp) = q;  // (u~_0, t~_0)
+      if (act) {
+        T[0] = (R)d[0];
+        if (TRAIN) H[0] = (R)d[1];
+      }
+    }
+    // P rows: |b| s~_b = |b| S_b / b!
+    for (int ia = 1 + warp; ia < na; ia += BELL_WORKERS)
+      if (lact) srow<R>(sm, a.pbase + ia * 256 + lp) = srow<R>(sm, lo + ia * 128) * __ldg(sdeg + ia);
+    __syncthreads();  // S is read: the next item's rows may stream in
+    if (it + 1 < it1)
+      stage_rows<NPB, R>(sm, (const R *)a.S + ((it + 1) % a.npts) * plane, na, n,
+                         (int)((it + 1) / a.npts) * NPB, BELL_WORKERS * 32);
+    cp_async_commit();
+    const PR q0 = srow<PR>(sm, a.qbase + lp);
+    const R u0 = q0.x, t0 = q0.y;
+#pragma unroll
+    for (int p = 1; p <= 8; ++p) {
+      if (p <= KK) {
+        switch (p) {
+          case 1: fwd9_degree<R, 1>(a, sm, lp, t0, u0, T, H, act, lact, TRAIN, warp); break;
+          case 2: if constexpr (KK >= 2) fwd9_degree<R, 2>(a, sm, lp, t0, u0, T, H, act, lact, TRAIN, warp); break;
+          case 3: if constexpr (KK >= 3) fwd9_degree<R, 3>(a, sm, lp, t0, u0, T, H, act, lact, TRAIN, warp); break;
+          case 4: if constexpr (KK >= 4) fwd9_degree<R, 4>(a, sm, lp, t0, u0, T, H, act, lact, TRAIN, warp); break;
+          case 5: if constexpr (KK >= 5) fwd9_degree<R, 5>(a, sm, lp, t0, u0, T, H, act, lact, TRAIN, warp); break;
+          case 6: if constexpr (KK >= 6) fwd9_degree<R, 6>(a, sm, lp, t0, u0, T, H, act, lact, TRAIN, warp); break;
+          case 7: if constexpr (KK >= 7) fwd9_degree<R, 7>(a, sm, lp, t0, u0, T, H, act, lact, TRAIN, warp); break;
+          case 8: if constexpr (KK >= 8) fwd9_degree<R, 8>(a, sm, lp, t0, u0, T, H, act, lact, TRAIN, warp); break;
+          default: break;
+        }
+        if (p < KK) __syncthreads();  // the top degree ends at the next item's barrier
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
 struct Adj5Args {
   int n, na, npts, gstride, gy;
   int norec, npair;    // counts copied to shared memory (SREC)
@@ -1287,6 +1463,11 @@ std::string tune_report() {
 static std::atomic<int> g_force[2] = {{-1}, {-1}};
 
 int tune_force(int which, int variant) {
+  if (which == 2) {  // the tanh series forward on (1) or off (0, -1: the default)
+    if (variant < -1 || variant > 1) return RC_BAD_ARG;
+    g_series_fwd = variant == 1;
+    return RC_OK;
+  }
   if (which < 0 || which > 1 || variant < -1 || variant > 7) return RC_BAD_ARG;
   g_force[which] = variant;
   return RC_OK;
@@ -1359,6 +1540,21 @@ static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
   a.rec = (const uint2 *)bp.f5_rec; a.rec32 = bp.f6_rec; a.cpdst = bp.f5_cpdst;
   a.sc = sizeof(R) == 8 ? (const void *)bp.sc64 : (const void *)bp.sc32;
   a.S = S; a.T = T; a.h = h;
+  if (t.iact == 0 && bp.f9.ok && g_series_fwd) {
+    Fwd9Args c;
+    c.n = n; c.na = t.na; c.npts = npts; c.iact = t.iact; c.gy = a.gy;
+    c.pbase = bp.f9.pbase; c.qbase = bp.f9.qbase; c.tpc = t.tpc;
+    c.list = bp.f9.list; c.hdr = (const int4 *)bp.f9.hdr; c.rec = (const uint4 *)bp.f9.rec;
+    c.sc = a.sc;
+    c.sdeg = sizeof(R) == 8 ? (const void *)bp.f9.sdeg64 : (const void *)bp.f9.sdeg32;
+    c.S = S; c.T = T; c.h = h;
+    auto k = train ? k_tanh_fwd9<R, KK, NPB, true> : k_tanh_fwd9<R, KK, NPB, false>;
+    CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bp.f9.smem));
+    const int grid = persistent_grid((const void *)k, BELL_WORKERS * 32, bp.f9.smem, (long)npts * a.gy);
+    LAUNCH("k_bell_fwd", st, k<<<grid, BELL_WORKERS * 32, bp.f9.smem, st>>>(c));
+    CKB(cudaGetLastError());
+    return RC_OK;
+  }
   // variant 0: records in global memory; 1: records in shared memory;
   // 2: v8 (lean per-degree loops over 16-bit offset records)
   const bool srec_fits = smem + (size_t)bp.nrec32 * 4 <= 227 * 1024;

@@ -56,6 +56,15 @@ struct DevBellPlan {
     int smem = 0;
     bool ok = false;
   } f8;
+  // v9 tanh series forward (F9Plan)
+  struct F9Dev {
+    int *list = nullptr, *hdr = nullptr;
+    uint32_t *rec = nullptr;
+    double *sdeg64 = nullptr;
+    float *sdeg32 = nullptr;
+    int pbase = 0, qbase = 0, smem = 0;
+    bool ok = false;
+  } f9;
   double *sc64 = nullptr;  // [3][na]: a!, 1/a!, 1/a! (Tb, h, Sb scales)
   float *sc32 = nullptr;
   void release();
@@ -66,7 +75,9 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d);
 // the autotuner's choices: "kernel width precision variant ms..." lines
 std::string tune_report();
 // pin the variant of the Bell forward (which 0) or adjoint (which 1) kernels;
-// variant -1 returns them to the autotuner
+// variant -1 returns them to the autotuner.  which 2 switches the tanh
+// series forward: 1 on wherever it applies, 0 or -1 off (the default: the
+// Bell recurrence everywhere).
 int tune_force(int which, int variant);
 
 // RC_UNSUPPORTED when the set does not fit (K > 8 or the per-point state

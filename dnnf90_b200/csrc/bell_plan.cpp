@@ -2,6 +2,7 @@
 #include "bell_plan.hpp"
 
 #include <algorithm>
+#include <unordered_map>
 #include <cmath>
 #include <map>
 #include <numeric>
@@ -139,6 +140,90 @@ static A7Plan build_a7(const TableSet &t, int aj_workers, int nkmax) {
     for (size_t i = 0; i < P.rec.size(); ++i)
       if (P.rec[i] >= (uint32_t)(2 * na) * ROW) P.ok = false;
   
+  return P;
+}
+
+// the v9 tanh series forward plan (see F9Plan)
+static F9Plan build_f9(const TableSet &t, int workers) {
+  F9Plan P;
+  const int na = t.na, k = t.k, d0 = t.d0;
+  P.pbase = (na + 1) * 128;
+  P.qbase = P.pbase + (na + 1) * 256;
+  P.smem = P.qbase + (na + 1) * 256;
+  if (k > 8 || na < 1) return P;
+  P.sdeg.assign(na, 0.0);
+  for (int ia = 0; ia < na; ++ia) {
+    double f = 1.0;
+    for (int i = 0; i < d0; ++i)
+      for (int v = 2; v <= t.alpha[(size_t)ia * d0 + i]; ++v) f *= v;
+    P.sdeg[ia] = t.deg[ia] / f;
+  }
+  const uint32_t zp = (uint32_t)(P.pbase + na * 256), zq = (uint32_t)(P.qbase + na * 256);
+  // slots by multi-index (digits base k + 1)
+  std::unordered_map<long long, int> slot;
+  auto key = [&](const int *a) {
+    long long v = 0;
+    for (int i = d0 - 1; i >= 0; --i) v = v * (k + 1) + a[i];
+    return v;
+  };
+  for (int ia = 0; ia < na; ++ia) slot[key(&t.alpha[(size_t)ia * d0])] = ia;
+  auto find = [&](const int *a) {
+    auto f = slot.find(key(a));
+    return f == slot.end() ? -1 : f->second;
+  };
+  // every ordered pair (b, a - b) with b != 0, a - b != 0; the set must hold both
+  std::vector<std::vector<uint32_t>> recs(na);
+  std::vector<int> b(d0), c(d0);
+  for (int ia = 1; ia < na; ++ia) {
+    if (t.deg[ia] < 2) continue;
+    const int *a = &t.alpha[(size_t)ia * d0];
+    // odometer over b <= a
+    std::fill(b.begin(), b.end(), 0);
+    while (true) {
+      int i = 0;
+      while (i < d0 && b[i] == a[i]) b[i++] = 0;
+      if (i == d0) break;
+      ++b[i];
+      int db = 0;
+      for (int m = 0; m < d0; ++m) {
+        c[m] = a[m] - b[m];
+        db += b[m];
+      }
+      if (db == t.deg[ia]) continue;  // c = 0
+      const int ib = find(b.data()), ic = find(c.data());
+      if (ib < 0 || ic < 0) return P;  // not downward closed
+      recs[ia].push_back((uint32_t)(P.pbase + ib * 256));
+      recs[ia].push_back((uint32_t)(P.qbase + ic * 256));
+    }
+    if ((recs[ia].size() / 2) % 2) {  // an even count: two records per 16-byte load
+      recs[ia].push_back(zp);
+      recs[ia].push_back(zq);
+    }
+  }
+  P.list.assign((size_t)(k + 1) * workers * 2, 0);
+  for (int p = 1; p <= k; ++p) {
+    std::vector<int> items;
+    std::vector<long> cost;
+    for (int ia = 1; ia < na; ++ia)
+      if (t.deg[ia] == p) {
+        items.push_back(ia);
+        cost.push_back(12 + (long)recs[ia].size() / 2);
+      }
+    auto asg = balance(cost, workers);
+    for (int w = 0; w < workers; ++w) {
+      P.list[((size_t)p * workers + w) * 2] = (int)P.hdr.size() / 4;
+      P.list[((size_t)p * workers + w) * 2 + 1] = (int)asg[w].size();
+      for (int it : asg[w]) {
+        const int ia = items[it];
+        P.hdr.push_back(ia);
+        P.hdr.push_back((int)P.rec.size() / 2);
+        P.hdr.push_back((int)recs[ia].size() / 2);
+        P.hdr.push_back(0);
+        P.rec.insert(P.rec.end(), recs[ia].begin(), recs[ia].end());
+      }
+    }
+  }
+  P.ok = P.smem <= 227 * 1024;
   return P;
 }
 
@@ -503,6 +588,7 @@ BellPlan build_bell_plan(const TableSet &t, int workers, int aj_workers) {
   P.a7f = build_a7(t, aj_workers, 16);
   P.a7d = build_a7(t, aj_workers, 8);
   P.f8 = build_f8(t, workers);
+  P.f9 = build_f9(t, workers);
 
   // adjoint outputs: Sb_0 (pairs (a, a) for every a) and every Sb_b, b >= 1
   std::vector<long> cost;

@@ -59,9 +59,29 @@ struct F8Plan {
   bool ok = false;
 };
 
+// The tanh forward by the series identity of tanh' = 1 - tanh^2 (v9).
+// With t~, u~ and s~ the factorial-normalised series of T, h = 1 - T^2 and
+// S, Euler's relation gives, degree by degree,
+//   |a| t~_a = sum_{0<b<=a} |b| s~_b u~_{a-b},
+//   u~_a = -sum_{b+c=a} t~_b t~_c,
+// and the two sums over the ordered pairs (b, c), b + c = a, b, c != 0, run
+// as one packed multiply-add of (|b| s~_b, t~_b) by (u~_c, t~_c).  Shared
+// memory: S rows [na+1][128 B]; P rows (|b| s~_b, t~_b) and Q rows
+// (u~_c, t~_c), [na+1][256 B] each (row na zero).  Needs a downward-closed
+// set (every b <= a carried).
+struct F9Plan {
+  std::vector<int> list;       // [(k+1) * workers][2]: first target, count
+  std::vector<int> hdr;        // [*][4]: ia, first record, records (even), 0
+  std::vector<uint32_t> rec;   // [*][2]: byte offsets of the P row of b and the Q row of c
+  std::vector<double> sdeg;    // [na]: |a| / a!
+  int pbase = 0, qbase = 0, smem = 0;
+  bool ok = false;
+};
+
 struct BellPlan {
   int workers = 0, k = 0, na = 0, nslot = 0;
   F8Plan f8;
+  F9Plan f9;
   // forward
   std::vector<int> fw_list;   // [(k+1) * workers][2]: start, count into fw_arec
   std::vector<int> fw_arec;   // [*][4]: ia | p << 16, gstart, gcount, bbase

@@ -218,7 +218,11 @@ int dnnf90_tune_report(char *buf, int len);
  * or adjoint (which 1: 0 pairs in global memory, 1 in shared memory,
  * 2 grouped correlation) kernels for every later launch; variant -1 hands
  * the choice back to the autotuner, and a variant a launch shape cannot use
- * runs its default.  For reproducible timing and for tests; new */
+ * runs its default.  which 2 switches the tanh forward by the series
+ * identity tanh' = 1 - tanh^2 (for tanh on sets closed under b <= a whose
+ * state fits shared memory): 1 on, 0 or -1 off (the default; the Bell
+ * recurrence measured faster).  The two forwards agree to rounding.  For
+ * reproducible timing and for tests; new */
 int dnnf90_tune_force(int which, int variant);
 /* policy (0 work, 1 square root, 2 none) and timed replay ms of the graph
  * the last committee step used; new */

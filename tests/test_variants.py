@@ -4,7 +4,8 @@ The autotuner picks one variant per launch shape by timing, so the parity
 tests elsewhere see only the variant that won on the machine at hand.  Here
 each variant is pinned in turn (dnnf90_tune_force) and the whole gradient
 step is checked: derivatives, loss and dL/dw, in both precisions, over dense
-and seeded sets from K = 1 to K = 8."""
+and seeded sets from K = 1 to K = 8.  The tanh series forward (v9, off by
+default) is switched off for the Bell variants and on for its own case."""
 import numpy as np
 import pytest
 
@@ -38,15 +39,17 @@ def pinned():
     yield api.tune_force
     api.tune_force(0, -1)
     api.tune_force(1, -1)
+    api.tune_force(2, -1)
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("d0,k,seeds,dims,npts", CASES)
 @pytest.mark.parametrize("prec", [api.PREC_F64, api.PREC_SPLIT])
-@pytest.mark.parametrize("fwd,adj", [(0, 0), (1, 1), (2, 2)])
-def test_pinned_variant(pinned, d0, k, seeds, dims, npts, prec, fwd, adj):
+@pytest.mark.parametrize("fwd,adj,series", [(0, 0, 0), (1, 1, 0), (2, 2, 0), (2, 2, 1)])
+def test_pinned_variant(pinned, d0, k, seeds, dims, npts, prec, fwd, adj, series):
     pinned(0, fwd)
     pinned(1, adj)
+    pinned(2, series)
     rng = np.random.default_rng(17)
     w = xavier_weights(dims, 23)
     w[np.arange(len(w)) % 6 == 0] += 0.04
@@ -68,6 +71,31 @@ def test_pinned_variant(pinned, d0, k, seeds, dims, npts, prec, fwd, adj):
 @pytest.mark.gpu
 def test_force_rejects_bad_arguments():
     with pytest.raises(api.Dnnf90Error):
-        api.tune_force(2, 0)
+        api.tune_force(3, 0)
+    with pytest.raises(api.Dnnf90Error):
+        api.tune_force(2, 2)
     with pytest.raises(api.Dnnf90Error):
         api.tune_force(0, -2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [api.PREC_F64, api.PREC_SPLIT])
+def test_series_forward_agrees_with_the_bell_recurrence(pinned, prec):
+    """The tanh series forward and the Bell recurrence compute the same
+    planes to rounding (T and dL/dw through the whole step)."""
+    d0, k, seeds, dims, npts = 4, 7, None, [4, 64, 48, 1], 6
+    rng = np.random.default_rng(5)
+    w = xavier_weights(dims, 29)
+    X = rng.uniform(-1, 1, (npts, d0))
+    ts, _ = _tables(d0, k, seeds)
+    out = []
+    for series in (0, 1):
+        pinned(2, series)
+        net = api.Net(ts, dims, weights=w, precision=prec)
+        g = net.grad()
+        r = api.SeedRule(api.SEED_HALFSQ)
+        loss, T = g.rule_batch(X, r, want_t=True)
+        out.append((T, g.read(), loss))
+        r.free(); g.free(); net.free()
+    tol = 1e-13 if prec == api.PREC_F64 else 1e-5
+    assert rel_err(out[1][0], out[0][0]) < tol and rel_err(out[1][1], out[0][1]) < tol
