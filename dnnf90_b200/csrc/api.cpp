@@ -1602,8 +1602,9 @@ int dnnf90_tune_report(char *buf, int len) {
 }
 
 int dnnf90_tune_force(int which, int variant) {
-  const int rc = tune_force(which, variant);
-  if (rc) set_error("dnnf90_tune_force: which must be 0 or 1, variant -1..7");
+  const int rc = which == 3 ? kf_force_path(variant) : tune_force(which, variant);
+  if (rc)
+    set_error("dnnf90_tune_force: which 0 or 1 with variant -1..7, 2 or 3 with -1..1");
   return rc;
 }
 
@@ -1712,6 +1713,10 @@ int kf_check(int kid) {
 
 int kf_status_rc(const KfState &s) {
   if (!s.status) return RC_OK;
+  if (s.status < 0) {
+    set_error("kalman: a grid barrier of the one-launch update gave up waiting");
+    return RC_DEVICE;
+  }
   set_error("kalman: nonpositive innovation denominator at observation " +
             std::to_string(s.status) + "; the covariance has lost positive definiteness");
   return RC_BAD_ARG;

@@ -214,6 +214,11 @@ struct KfState {
   int status;                      // 0, or 1 + the observation whose denominator was not positive
 };
 
+// grid barrier of the one-launch Kalman sequence
+struct KfBar {
+  unsigned count, gen;
+};
+
 // covariance in packed 32 x 32 tiles of each block's upper triangle
 struct KfDev {
   int nw = 0, ntile = 0, nred = 0;
@@ -227,6 +232,8 @@ struct KfDev {
   double *dotp = nullptr;    // per row tile: its shares of j.Pj and of j.(w- - w)
   unsigned *ctr = nullptr;   // reduce CTAs finished
   KfState *st = nullptr;
+  KfBar *bar = nullptr;
+  int seq_grid = 0;          // CTAs of the one-launch sequence (0: no cooperative launch)
   double *wprior = nullptr;  // [nw] iterated EKF: the prior weights
   bool prior = false;        // set by an IEKF begin
   double *stage = nullptr;   // host-call staging (rows, innovations, scales, weights)
@@ -253,6 +260,9 @@ int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
 int kf_iekf(KfDev &d, const double *row, const double *resid, const double *scale, double *w,
             bool final, cudaStream_t s);
 int kf_state(const KfDev &d, KfState *out, cudaStream_t s);
+// the update path: -1 by size (default), 0 two launches per update, 1 one
+// cooperative launch per call
+int kf_force_path(int path);
 // covariance to the host: dense [nw][nw], or the blocks [bsz][bsz] one after another
 int kf_read_cov(const KfDev &d, const std::vector<int> &bsz, const std::vector<int> &boff,
                 bool dense, double *out, cudaStream_t s);

@@ -31,6 +31,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -47,6 +48,16 @@ namespace dnnf90 {
       return e_ == cudaErrorMemoryAllocation ? RC_NOMEM : RC_DEVICE;   \
     }                                                                  \
   } while (0)
+
+// which update path kf_run takes: -1 by size (the one-launch sequence for
+// small filters), 0 two launches per update, 1 the one-launch sequence
+static std::atomic<int> g_kf_path{-1};
+
+int kf_force_path(int path) {
+  if (path < -1 || path > 1) return RC_BAD_ARG;
+  g_kf_path = path;
+  return RC_OK;
+}
 
 constexpr int KT = 32;          // tile side
 constexpr int KTE = KT * KT;    // elements per tile
@@ -88,9 +99,122 @@ __device__ __forceinline__ void tri_tile(int t, int tb, int &I, int &J) {
   J = i + (int)(t - t0(i));
 }
 
-// One CTA per tile.  DENSE (a single block of nw) derives the tile's
-// position from its index, so that nothing the vector loads need waits on
-// a table read; the decoupled filter reads its tile table.
+// the scalars of the observation a tile pass applies
+struct KfScal {
+  double lam, denom, sg, xi, q;
+};
+
+// Where tile t sits: block offset o, block size n, tile (I, J) and the
+// block's partial slots.  DENSE (a single block of nw) derives the position
+// from the index, so that nothing the vector loads need waits on a table
+// read; the decoupled filter reads its tile table.
+template <bool DENSE>
+__device__ __forceinline__ void kf_tile_at(int t, const int4 *__restrict__ tiles, int nw,
+                                           double *part, int &o, int &n, int &I, int &J,
+                                           double *&pslot) {
+  if (DENSE) {
+    o = 0;
+    n = nw;
+    tri_tile(t, (nw + KT - 1) / KT, I, J);
+    pslot = part;
+  } else {
+    // x: block offset, y: block size, z: I | J << 16, w: the block's partial slots
+    const int4 d = tiles[t];
+    o = d.x;
+    n = d.y;
+    I = d.z & 0xffff;
+    J = d.z >> 16;
+    pslot = part + d.w;
+  }
+}
+
+// One tile of the pass, its elements v already loaded: the update of
+// observation k (MODE != KM_PJ) and the products of the result with the
+// next row (MODE != KM_UPD).  Every thread of the CTA calls it.
+template <int MODE, bool CG = false>
+__device__ __forceinline__ void kf_tile_body(double *tp, double (&v)[4], int o, int n, int I,
+                                             int J, double *pslot, const double *__restrict__ pj,
+                                             const KfScal &sc, double *__restrict__ w,
+                                             const double *__restrict__ wb, const KfRowArgs &ra,
+                                             int knext) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tb = (n + KT - 1) / KT;
+  __shared__ double s_pjR[KT], s_kvR[KT], s_pjC[KT], s_kvC[KT], s_jR[KT], s_jC[KT];
+  __shared__ double s_col[8][KT + 1];
+  if (threadIdx.x < KT) {
+    const int R = I * KT + lane, C = J * KT + lane;
+    if (MODE != KM_PJ) {
+      // CG: P j was written by other CTAs of the same launch (the
+      // one-launch sequence), so it is read past L1
+      const double pr = R < n ? sc.sg * (CG ? __ldcg(pj + o + R) : pj[o + R]) : 0.0;
+      const double pc = C < n ? sc.sg * (CG ? __ldcg(pj + o + C) : pj[o + C]) : 0.0;
+      s_pjR[lane] = pr;
+      s_kvR[lane] = pr / sc.denom;
+      s_pjC[lane] = pc;
+      s_kvC[lane] = pc / sc.denom;
+    }
+    if (MODE != KM_UPD) {
+      const double sn = row_scale(ra, knext);
+      const double *jn = ra.rows + (size_t)knext * ra.ld;
+      s_jR[lane] = R < n ? sn * jn[o + R] : 0.0;
+      s_jC[lane] = C < n ? sn * jn[o + C] : 0.0;
+    }
+  }
+  __syncthreads();
+  const int C = J * KT + lane;
+  if (MODE != KM_PJ) {
+    // 1/lambda once per tile: an FP64 division per element would cost as
+    // much as the element's HBM traffic (lambda = 1 is exact either way)
+    const double rl = 1.0 / sc.lam, hl = 0.5 * rl;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const int r = warp + 8 * m, R = I * KT + r;
+      if (R < n && C < n) {
+        const double a = v[m];
+        if (R == C) {
+          double d = __fma_rn(-s_kvR[r], s_pjR[r], a) * rl;
+          if (sc.q > 0.0) d += sc.q;
+          v[m] = d;
+        } else {
+          const double x = __fma_rn(-s_kvR[r], s_pjC[lane], a);
+          const double y = __fma_rn(-s_kvC[lane], s_pjR[r], a);
+          v[m] = (x + y) * hl;
+        }
+      }
+      __stcs(tp + r * KT + lane, v[m]);
+    }
+    if (I == J && threadIdx.x < KT) {
+      const int R = I * KT + lane;
+      if (R < n) w[o + R] = __fma_rn(s_kvR[lane], sc.xi, wb[o + R]);
+    }
+  }
+  if (MODE != KM_UPD) {
+    // row sums -> slot J of the rows of tile I
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      double s = v[m] * s_jC[lane];
+#pragma unroll
+      for (int off = 16; off; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+      const int R = I * KT + warp + 8 * m;
+      if (lane == 0 && R < n) pslot[((size_t)I * tb + J) * KT + warp + 8 * m] = s;
+    }
+    if (I != J) {  // column sums -> slot I of the rows of tile J
+      double s = 0.0;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) s = __fma_rn(v[m], s_jR[warp + 8 * m], s);
+      s_col[warp][lane] = s;
+      __syncthreads();
+      if (threadIdx.x < KT) {
+        double c = 0.0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) c += s_col[u][lane];
+        if (C < n) pslot[((size_t)J * tb + I) * KT + lane] = c;
+      }
+    }
+  }
+}
+
+// One CTA per tile.
 template <int MODE, bool DENSE>
 __global__ void __launch_bounds__(256, 8) k_kf_tiles(const int4 *__restrict__ tiles,
                                                      double *__restrict__ P, int nw,
@@ -110,102 +234,12 @@ __global__ void __launch_bounds__(256, 8) k_kf_tiles(const int4 *__restrict__ ti
 #pragma unroll
   for (int m = 0; m < 4; ++m) v[m] = __ldcs(tp + (warp + 8 * m) * KT + lane);
   int o, n, I, J;
-  double *pslot;  // the block's partial slots, [row tile][slot][32]
-  if (DENSE) {
-    o = 0;
-    n = nw;
-    tri_tile(blockIdx.x, (nw + KT - 1) / KT, I, J);
-    pslot = part;
-  } else {
-    // x: block offset, y: block size, z: I | J << 16, w: the block's partial slots
-    const int4 t = tiles[blockIdx.x];
-    o = t.x;
-    n = t.y;
-    I = t.z & 0xffff;
-    J = t.z >> 16;
-    pslot = part + t.w;
-  }
-  const int tb = (n + KT - 1) / KT;
+  double *pslot;
+  kf_tile_at<DENSE>(blockIdx.x, tiles, nw, part, o, n, I, J, pslot);
   if (st->status) return;
-  __shared__ double s_pjR[KT], s_kvR[KT], s_pjC[KT], s_kvC[KT], s_jR[KT], s_jC[KT];
-  __shared__ double s_col[8][KT + 1];
-  double lam = 1.0, denom = 1.0, sg = 1.0, xi = 0.0, q = 0.0;
-  if (MODE != KM_PJ) {
-    lam = st->lamk;
-    denom = st->denom;
-    sg = st->sg;
-    xi = st->xi;
-    q = st->q;
-  }
-  if (threadIdx.x < KT) {
-    const int R = I * KT + lane, C = J * KT + lane;
-    if (MODE != KM_PJ) {
-      const double pr = R < n ? sg * pj[o + R] : 0.0;
-      const double pc = C < n ? sg * pj[o + C] : 0.0;
-      s_pjR[lane] = pr;
-      s_kvR[lane] = pr / denom;
-      s_pjC[lane] = pc;
-      s_kvC[lane] = pc / denom;
-    }
-    if (MODE != KM_UPD) {
-      const double sn = row_scale(ra, knext);
-      const double *jn = ra.rows + (size_t)knext * ra.ld;
-      s_jR[lane] = R < n ? sn * jn[o + R] : 0.0;
-      s_jC[lane] = C < n ? sn * jn[o + C] : 0.0;
-    }
-  }
-  __syncthreads();
-  const int C = J * KT + lane;
-  if (MODE != KM_PJ) {
-    // 1/lambda once per tile: an FP64 division per element would cost as
-    // much as the element's HBM traffic (lambda = 1 is exact either way)
-    const double rl = 1.0 / lam, hl = 0.5 * rl;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      const int r = warp + 8 * m, R = I * KT + r;
-      if (R < n && C < n) {
-        const double a = v[m];
-        if (R == C) {
-          double d = __fma_rn(-s_kvR[r], s_pjR[r], a) * rl;
-          if (q > 0.0) d += q;
-          v[m] = d;
-        } else {
-          const double x = __fma_rn(-s_kvR[r], s_pjC[lane], a);
-          const double y = __fma_rn(-s_kvC[lane], s_pjR[r], a);
-          v[m] = (x + y) * hl;
-        }
-      }
-      __stcs(tp + r * KT + lane, v[m]);
-    }
-    if (I == J && threadIdx.x < KT) {
-      const int R = I * KT + lane;
-      if (R < n) w[o + R] = wb[o + R] + s_kvR[lane] * xi;
-    }
-  }
-  if (MODE != KM_UPD) {
-    // row sums -> slot J of the rows of tile I
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      double s = v[m] * s_jC[lane];
-#pragma unroll
-      for (int off = 16; off; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-      const int R = I * KT + warp + 8 * m;
-      if (lane == 0 && R < n) pslot[((size_t)I * tb + J) * KT + warp + 8 * m] = s;
-    }
-    if (I != J) {  // column sums -> slot I of the rows of tile J
-      double s = 0.0;
-#pragma unroll
-      for (int m = 0; m < 4; ++m) s += v[m] * s_jR[warp + 8 * m];
-      s_col[warp][lane] = s;
-      __syncthreads();
-      if (threadIdx.x < KT) {
-        double c = 0.0;
-#pragma unroll
-        for (int u = 0; u < 8; ++u) c += s_col[u][lane];
-        if (C < n) pslot[((size_t)J * tb + I) * KT + lane] = c;
-      }
-    }
-  }
+  KfScal sc{1.0, 1.0, 1.0, 0.0, 0.0};
+  if (MODE != KM_PJ) sc = KfScal{st->lamk, st->denom, st->sg, st->xi, st->q};
+  kf_tile_body<MODE>(tp, v, o, n, I, J, pslot, pj, sc, w, wb, ra, knext);
 }
 
 // P j of row k from the partial slots, j.Pj per CTA, and in the last CTA
@@ -303,6 +337,168 @@ __global__ void k_kf_wonly(int nw, double *__restrict__ w, const double *__restr
   if (R < nw) w[R] = wb[R] + (st->sg * pj[R] / st->denom) * st->xi;
 }
 
+// ---------------------------------------------------- whole sequence, one launch
+// For a small filter the two launches of an update cost more than their
+// work.  k_kf_seq runs a whole call as one cooperative launch: the tile
+// pass, the reduce and the scalars of every observation as phases separated
+// by grid barriers, with the same per-tile code and the same summation
+// orders as the two-kernel path, so the results are bit-identical.  The
+// scalars are formed by every CTA from the same values; lambda and the gate
+// count live in registers and CTA 0 writes them back at the end.
+
+constexpr long KF_BAR_LIMIT = 1L << 24;  // polls before a grid barrier gives up
+
+// barrier among the CTAs of a cooperative launch (sense by generation);
+// false, with status -1, when a wait runs out or another CTA gave up
+__device__ bool kf_grid_sync(KfBar *b, KfState *st) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned g = *(volatile unsigned *)&b->gen;
+    __threadfence();
+    if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
+      atomicExch(&b->count, 0u);
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    } else {
+      ok = 0;
+      for (long i = 0; i < KF_BAR_LIMIT; ++i) {
+        if (*(volatile unsigned *)&b->gen != g) {
+          ok = 1;
+          break;
+        }
+        if (*(volatile int *)&st->status < 0) break;
+        if (i > 32) __nanosleep(32);
+      }
+      if (!ok) atomicCAS(&st->status, 0, -1);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// the tiles of this CTA (t = blockIdx, blockIdx + grid, ...)
+template <int MODE, bool DENSE>
+__device__ __forceinline__ void kf_seq_tiles(const int4 *__restrict__ tiles, int ntile,
+                                             double *__restrict__ P, int nw,
+                                             const double *__restrict__ pj, const KfScal &sc,
+                                             double *__restrict__ w, const KfRowArgs &ra,
+                                             int knext, double *__restrict__ part) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+    double *tp = P + (size_t)t * KTE;
+    double v[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) v[m] = __ldcs(tp + (warp + 8 * m) * KT + lane);
+    int o, n, I, J;
+    double *pslot;
+    kf_tile_at<DENSE>(t, tiles, nw, part, o, n, I, J, pslot);
+    kf_tile_body<MODE, true>(tp, v, o, n, I, J, pslot, pj, sc, w, w, ra, knext);
+    __syncthreads();  // the tile's vectors are read before the next tile writes them
+  }
+}
+
+template <bool DENSE>
+__global__ void __launch_bounds__(256) k_kf_seq(const int4 *__restrict__ tiles, int ntile,
+                                                double *__restrict__ P, int nw,
+                                                const int4 *__restrict__ rtl, int nred,
+                                                double *__restrict__ part, double *__restrict__ pj,
+                                                double *__restrict__ dotp,
+                                                KfState *__restrict__ st, KfBar *__restrict__ bar,
+                                                double *__restrict__ w, KfRowArgs ra, int nobs,
+                                                int kbase, int first, int has_next) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ double s_sum[16][33];
+  __shared__ KfScal s_sc;
+  __shared__ int s_fail;
+  if (*(volatile int *)&st->status) return;
+  double lam = st->lam;
+  const double lam0 = st->lam0, q = st->q, gate = st->gate;
+  int ngated = st->ngated;
+  KfScal sc{1.0, 1.0, 1.0, 0.0, q};
+  if (first) {
+    kf_seq_tiles<KM_PJ, DENSE>(tiles, ntile, P, nw, pj, sc, w, ra, 0, part);
+    if (!kf_grid_sync(bar, st)) return;
+  }
+  for (int k = 0; k < nobs; ++k) {
+    // reduce: P j of row k and the row tiles' shares of j.Pj, in the order
+    // of k_kf_reduce (16 slot groups: this warp takes groups warp, warp + 8)
+    for (int rt = blockIdx.x; rt < nred; rt += gridDim.x) {
+      const int4 r = rtl[rt];
+      const double *src = part + r.w;
+      double s0 = 0.0, s1 = 0.0;
+      for (int i = warp; i < r.z; i += 16) s0 += __ldcg(src + (size_t)i * KT + lane);
+      for (int i = warp + 8; i < r.z; i += 16) s1 += __ldcg(src + (size_t)i * KT + lane);
+      s_sum[warp][lane] = s0;
+      s_sum[warp + 8][lane] = s1;
+      __syncthreads();
+      if (warp == 0) {
+        double p = 0.0, prod = 0.0;
+#pragma unroll
+        for (int u = 0; u < 16; ++u) p += s_sum[u][lane];
+        if (lane < r.y) {
+          const int R = r.x + lane;
+          pj[R] = p;
+          prod = row_scale(ra, k) * ra.rows[(size_t)k * ra.ld + R] * p;
+        }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) prod += __shfl_xor_sync(0xffffffffu, prod, off);
+        if (lane == 0) dotp[2 * rt] = prod;
+      }
+      __syncthreads();
+    }
+    if (!kf_grid_sync(bar, st)) return;
+    // the scalars of observation k, the same in every CTA
+    if (threadIdx.x == 0) {
+      double dot = 0.0;
+      for (int b = 0; b < nred; ++b) dot += __ldcg(dotp + 2 * b);
+      double denom = lam + dot;
+      int fail = !(denom > 0.0);
+      double xi = row_scale(ra, k) * ra.xi[k], sg = 1.0;
+      if (!fail && gate > 0.0) {
+        const double jpj = denom - lam;
+        if (xi * xi > gate * gate * denom) {
+          const double s2 = gate * gate * lam / (xi * xi - gate * gate * jpj);
+          sg = sqrt(s2);
+          xi = sg * xi;
+          denom = lam + s2 * jpj;
+          ++ngated;
+        }
+      }
+      s_sc = KfScal{lam, denom, sg, xi, q};
+      s_fail = fail;
+    }
+    __syncthreads();
+    if (s_fail) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->status = kbase + k + 1;
+        st->lam = lam;
+        st->ngated = ngated;
+      }
+      return;
+    }
+    sc = s_sc;
+    lam = __dadd_rn(__dmul_rn(lam0, lam), 1.0) - lam0;
+    if (k + 1 < nobs || has_next) {
+      kf_seq_tiles<KM_UPD_PJ, DENSE>(tiles, ntile, P, nw, pj, sc, w, ra, k + 1, part);
+      if (!kf_grid_sync(bar, st)) return;
+    } else {
+      kf_seq_tiles<KM_UPD, DENSE>(tiles, ntile, P, nw, pj, sc, w, ra, 0, part);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->lam = lam;
+    st->ngated = ngated;
+    st->lamk = sc.lam;
+    st->denom = sc.denom;
+    st->sg = sc.sg;
+    st->xi = sc.xi;
+  }
+}
+
 __global__ void k_kf_init_tiles(const int4 *__restrict__ tiles, double *__restrict__ P, double p0) {
   const int4 t = tiles[blockIdx.x];
   double *tp = P + (size_t)blockIdx.x * KTE;
@@ -322,6 +518,7 @@ void KfDev::release() {
   cudaFree(dotp);
   cudaFree(ctr);
   cudaFree(st);
+  cudaFree(bar);
   cudaFree(stage);
   cudaFree(wprior);
   *this = KfDev();
@@ -366,6 +563,17 @@ int kf_create(KfDev &d, const std::vector<int> &bsz, const std::vector<int> &bof
   CKK(cudaMalloc(&d.wprior, nw * sizeof(double)));
   CKK(cudaMalloc(&d.ctr, sizeof(unsigned)));
   CKK(cudaMalloc(&d.st, sizeof(KfState)));
+  CKK(cudaMalloc(&d.bar, sizeof(KfBar)));
+  CKK(cudaMemset(d.bar, 0, sizeof(KfBar)));
+  {
+    int coop = 0, dev = 0, per_sm = 0;
+    CKK(cudaGetDevice(&dev));
+    CKK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    CKK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, d.dense ? k_kf_seq<true> : k_kf_seq<false>, 256, 0));
+    d.seq_grid = coop && per_sm > 0 ? std::min(grid_sms() * per_sm, std::max(d.ntile, d.nred))
+                                    : 0;
+  }
   CKK(cudaMemcpy(d.tiles, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice));
   CKK(cudaMemcpy(d.rtl, rtl.data(), rtl.size() * sizeof(int4), cudaMemcpyHostToDevice));
   CKK(cudaMemset(d.ctr, 0, sizeof(unsigned)));
@@ -385,6 +593,21 @@ int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
            const double *scale, double *w, cudaStream_t s, int kbase, bool has_next) {
   if (nobs <= 0) return RC_OK;
   KfRowArgs ra{rows, ld, xi, scale};
+  const int path = g_kf_path.load();
+  if (d.seq_grid > 0 && (path == 1 || (path < 0 && d.ntile <= 4 * d.seq_grid))) {
+    if (kbase == 0) CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
+    int first = kbase == 0, hn = has_next ? 1 : 0, ntile = d.ntile, nw = d.nw, nred = d.nred;
+    void *args[] = {&d.tiles, &ntile, &d.P, &nw, &d.rtl, &nred, &d.part, &d.pj, &d.dotp,
+                    &d.st, &d.bar, &w, &ra, &nobs, &kbase, &first, &hn};
+    const void *fn = d.dense ? (const void *)k_kf_seq<true> : (const void *)k_kf_seq<false>;
+    CKK(cudaMemsetAsync(d.bar, 0, sizeof(KfBar), s));  // a barrier that gave up leaves a count
+    int pi = prof_begin("k_kf_seq", s);
+    const cudaError_t e = cudaLaunchCooperativeKernel(fn, d.seq_grid, 256, args, 0, s);
+    prof_end(pi, s);
+    note_launch();
+    CKK(e);
+    return RC_OK;
+  }
   if (kbase == 0) {  // start of a sequence: the products with its first row
     CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
     LAUNCH("k_kf_tiles_pj", s,

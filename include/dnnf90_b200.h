@@ -221,8 +221,11 @@ int dnnf90_tune_report(char *buf, int len);
  * runs its default.  which 2 switches the tanh forward by the series
  * identity tanh' = 1 - tanh^2 (for tanh on sets closed under b <= a whose
  * state fits shared memory): 1 on, 0 or -1 off (the default; the Bell
- * recurrence measured faster).  The two forwards agree to rounding.  For
- * reproducible timing and for tests; new */
+ * recurrence measured faster).  The two forwards agree to rounding.  which 3
+ * picks the Kalman update path: 0 two launches per update, 1 one
+ * cooperative launch per call, -1 by size (the default: one launch for
+ * small filters); the two give identical bits.  For reproducible timing and
+ * for tests; new */
 int dnnf90_tune_force(int which, int variant);
 /* policy (0 work, 1 square root, 2 none) and timed replay ms of the graph
  * the last committee step used; new */

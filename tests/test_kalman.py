@@ -327,3 +327,30 @@ def test_device_iekf_single_final_iteration_is_the_plain_update():
     for k in (a, b, c):
         k.free()
     na.free(); nb.free(); tsa.free(); tsb.free()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("decoupled", [False, True])
+def test_one_launch_and_two_launch_paths_are_bit_identical(decoupled, monkeypatch):
+    """The one-launch sequence (cooperative, grid barriers) and the two
+    launches per update share the tile code and every summation order, so
+    they give the same bits: weights, covariance, lambda and gate count,
+    also across staging chunks."""
+    from dnnf90_b200 import api
+    dims = [3, 20, 20, 1]
+    out = []
+    try:
+        for path in (0, 1):
+            api.tune_force(3, path)
+            (kf, net, ts), ref, wref, (rows, xi, sc) = _run_both(dims, decoupled, 1e-4, 1.5, 40)
+            kf.update_rows(rows[:25], xi[:25], sc[:25])
+            monkeypatch.setenv("DNNF90_KF_STAGE_KB", "9")
+            kf.update_rows(rows[25:], xi[25:], sc[25:])
+            monkeypatch.delenv("DNNF90_KF_STAGE_KB")
+            out.append((net.get_weights(), kf.cov(), kf.state()))
+            assert rel_err(net.get_weights(), wref) < 1e-11
+            kf.free(); net.free(); ts.free()
+    finally:
+        api.tune_force(3, -1)
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]

@@ -71,9 +71,11 @@ def test_pinned_variant(pinned, d0, k, seeds, dims, npts, prec, fwd, adj, series
 @pytest.mark.gpu
 def test_force_rejects_bad_arguments():
     with pytest.raises(api.Dnnf90Error):
-        api.tune_force(3, 0)
+        api.tune_force(4, 0)
     with pytest.raises(api.Dnnf90Error):
         api.tune_force(2, 2)
+    with pytest.raises(api.Dnnf90Error):
+        api.tune_force(3, 2)
     with pytest.raises(api.Dnnf90Error):
         api.tune_force(0, -2)
 
