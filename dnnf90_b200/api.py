@@ -49,7 +49,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_ngd_step_dual", "dnnf90_kf_create", "dnnf90_kf_free", "dnnf90_kf_update_rows",
     "dnnf90_kf_update_rows_dev", "dnnf90_kf_read", "dnnf90_kf_iekf_begin",
     "dnnf90_kf_iekf_iter", "dnnf90_ngd_gram_dev", "dnnf90_ngd_solve_dev",
-    "dnnf90_ngd_step_dual_dev",
+    "dnnf90_ngd_step_dual_dev", "dnnf90_kf_pass",
 ]
 
 _lib = None
@@ -146,6 +146,7 @@ def lib():
         "dnnf90_ngd_gram_dev": [i, i, p, i, p, p],
         "dnnf90_ngd_solve_dev": [i, p, p, i, d, p, p],
         "dnnf90_ngd_step_dual_dev": [i, i, p, p, i, d, p, p],
+        "dnnf90_kf_pass": [i, i, i, pd, i, d],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -468,6 +469,13 @@ class Kalman:
         sc = None if scale is None else _f64(np.broadcast_to(scale, xi.shape))
         call("dnnf90_kf_update_rows", self.kid, rows.shape[0], _pd(rows), _pd(xi),
              None if sc is None else _pd(sc))
+
+    def pass_points(self, X, rule: "SeedRule", rnoise: float = 1.0):
+        """One filter update per point, each from the point's row and
+        residual at the weights the previous update left (dnnf90_kf_pass)."""
+        X = _f64(np.atleast_2d(X))
+        call("dnnf90_kf_pass", self.kid, self.net.tid, X.shape[0], _pd(X), rule.rid,
+             float(rnoise))
 
     def iekf_begin(self):
         """The network's current weights become the prior of the iteration."""

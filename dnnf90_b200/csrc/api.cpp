@@ -1767,7 +1767,7 @@ int dnnf90_kf_update_rows(int kid, int nobs, const double *rows, const double *x
                                           cudaMemcpyHostToDevice, k.st), "H2D")))
       return rc;
     if ((rc = kf_run(k.d, k1 - k0, dr, nw, dxi, scale ? dsc : nullptr, dw, k.st, k0,
-                     k1 < nobs)))
+                     k1 < nobs, k0 == 0)))
       return rc;
   }
   if ((rc = ck(cudaMemcpyAsync(n.w.data(), dw, nw * 8, cudaMemcpyDeviceToHost, k.st), "D2H")))
@@ -1787,7 +1787,7 @@ int dnnf90_kf_update_rows_dev(int kid, int nobs, const double *rows_dev, const d
   if (nobs == 0) return RC_OK;
   KfH &k = g_kf[kid];
   cudaStream_t st = (cudaStream_t)stream;
-  if ((rc = kf_run(k.d, nobs, rows_dev, k.d.nw, xi_dev, scale_dev, w_dev, st, 0, false)))
+  if ((rc = kf_run(k.d, nobs, rows_dev, k.d.nw, xi_dev, scale_dev, w_dev, st, 0, false, true)))
     return rc;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
@@ -1795,6 +1795,74 @@ int dnnf90_kf_update_rows_dev(int kid, int nobs, const double *rows_dev, const d
   KfState s;
   if ((rc = kf_state(k.d, &s, st))) return rc;
   return kf_status_rc(s);
+}
+
+int dnnf90_kf_pass(int kid, int tid, int npts, const double *x, int rid, double rnoise) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = kf_check(kid);
+  if (rc) return rc;
+  KfH &k = g_kf[kid];
+  const int nid = k.nid;
+  if ((rc = check_train(nid, tid, 0, false))) return rc;
+  if (bad_rule(rid) || g_rule[rid].r.kind != SEED_JROW) return RC_BAD_ARG;
+  if (npts < 0 || (npts > 0 && !x)) return RC_BAD_ARG;
+  if (!(rnoise > 0.0)) {  // kf_update_resid_multi :286-290
+    set_error("kf_pass: observation noise must be > 0");
+    return RC_BAD_ARG;
+  }
+  if (npts == 0) return RC_OK;
+  NetH &n = g_net[nid];
+  if (n.prec != PREC_F64) {
+    set_error("kf_pass: the per-point filter pass runs on the FP64 path (the filter moves "
+              "the weights after every point)");
+    return RC_UNSUPPORTED;
+  }
+  WorkH &w = g_twk[tid];
+  RuleH &rule = g_rule[rid];
+  if ((rc = flush_queue(tid))) return rc;
+  flush_for_net(nid);
+  if ((rc = work_stream(w))) return rc;
+  if ((rc = net_device(n, w.st))) return rc;
+  if ((rc = rule_device(rule, n))) return rc;
+  if ((rc = work_planes(w, n, 1, false))) return rc;
+  const int nw = (int)n.w.size(), d0 = n.ts.d0, nout = n.dims[n.nlayer - 1];
+  const size_t need = ((size_t)npts * d0 + nw + 3) * sizeof(double);
+  if (k.d.stage_bytes < need) {
+    cudaFree(k.d.stage);
+    k.d.stage = nullptr;
+    k.d.stage_bytes = 0;
+    if ((rc = ck(cudaMalloc(&k.d.stage, need), "cudaMalloc"))) return rc;
+    k.d.stage_bytes = need;
+  }
+  double *drow = k.d.stage, *dxi = drow + nw, *dsc = dxi + 1, *dloss = dsc + 1,
+         *dX = dloss + 1;
+  const double sc = 1.0 / std::sqrt(rnoise);
+  if ((rc = ck(cudaMemcpyAsync(dX, x, sizeof(double) * (size_t)npts * d0,
+                               cudaMemcpyHostToDevice, w.st), "H2D")) ||
+      (rc = ck(cudaMemcpyAsync(dsc, &sc, sizeof(double), cudaMemcpyHostToDevice, w.st), "H2D")))
+    return rc;
+  // per point: its row and residual at the current weights (the forward
+  // and adjoint read the device weights the filter has just moved), then
+  // the rank-one update of kf_update_resid (:252-275): xi = -R
+  for (int p = 0; p < npts && !rc; ++p) {
+    BatchArgs a;
+    a.npts = 1;
+    a.X = dX + (size_t)p * d0;
+    a.out = w.p.out;
+    a.rows = drow;
+    a.loss = dloss;
+    a.train = true;
+    a.prec = PREC_F64;
+    if ((rc = run_batch(n.dt, n.dn, rule.d, w.p, a, w.st))) break;
+    if ((rc = kf_resid_xi(rule.d, w.p.out, nout, dxi, w.st))) break;
+    rc = kf_run(k.d, 1, drow, nw, dxi, dsc, n.dn.w64, w.st, p, false, true);
+  }
+  if (!rc) rc = ck(cudaMemcpyAsync(n.w.data(), n.dn.w64, sizeof(double) * nw,
+                                   cudaMemcpyDeviceToHost, w.st), "D2H");
+  KfState s;
+  if (!rc) rc = kf_state(k.d, &s, w.st);
+  n.wver++;  // the host copy now holds what the device computed
+  return rc ? rc : kf_status_rc(s);
 }
 
 int dnnf90_kf_iekf_begin(int kid) {

@@ -249,10 +249,15 @@ int kf_create(KfDev &d, const std::vector<int> &bsz, const std::vector<int> &bof
 // xi[k] = target - prediction, scale[k] (null = 1); w[nw] updated in place.
 // Stops at the first nonpositive denominator (KfState::status = kbase + k + 1).
 // A sequence split into calls passes kbase = the index of its first
-// observation; a call with has_next also stages row nobs (the next call's
-// first), whose products its last tile pass forms.
+// observation (the status is reset when it is 0); first forms the products
+// with row 0 (false when the previous call's last pass formed them); a call
+// with has_next also stages row nobs (the next call's first), whose products
+// its last tile pass forms.
 int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
-           const double *scale, double *w, cudaStream_t s, int kbase, bool has_next);
+           const double *scale, double *w, cudaStream_t s, int kbase, bool has_next,
+           bool first);
+// xi[0] = -R of one point's output derivatives under a Jacobian-row rule
+int kf_resid_xi(const DevRule &r, const double *out, int nout, double *xi, cudaStream_t s);
 // one relinearisation of the iterated EKF (kf_iekf_iter): row = dR/dw at
 // the current weights w, resid[0] = R, scale[0] = 1/sqrt(rnoise); w <- w- +
 // kv xi with the prior d.wprior; the covariance and lambda change only when

@@ -590,15 +590,16 @@ int kf_create(KfDev &d, const std::vector<int> &bsz, const std::vector<int> &bof
 }
 
 int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
-           const double *scale, double *w, cudaStream_t s, int kbase, bool has_next) {
+           const double *scale, double *w, cudaStream_t s, int kbase, bool has_next,
+           bool first) {
   if (nobs <= 0) return RC_OK;
   KfRowArgs ra{rows, ld, xi, scale};
   const int path = g_kf_path.load();
   if (d.seq_grid > 0 && (path == 1 || (path < 0 && d.ntile <= 4 * d.seq_grid))) {
     if (kbase == 0) CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
-    int first = kbase == 0, hn = has_next ? 1 : 0, ntile = d.ntile, nw = d.nw, nred = d.nred;
+    int fi = first ? 1 : 0, hn = has_next ? 1 : 0, ntile = d.ntile, nw = d.nw, nred = d.nred;
     void *args[] = {&d.tiles, &ntile, &d.P, &nw, &d.rtl, &nred, &d.part, &d.pj, &d.dotp,
-                    &d.st, &d.bar, &w, &ra, &nobs, &kbase, &first, &hn};
+                    &d.st, &d.bar, &w, &ra, &nobs, &kbase, &fi, &hn};
     const void *fn = d.dense ? (const void *)k_kf_seq<true> : (const void *)k_kf_seq<false>;
     CKK(cudaMemsetAsync(d.bar, 0, sizeof(KfBar), s));  // a barrier that gave up leaves a count
     int pi = prof_begin("k_kf_seq", s);
@@ -608,8 +609,8 @@ int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
     CKK(e);
     return RC_OK;
   }
-  if (kbase == 0) {  // start of a sequence: the products with its first row
-    CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
+  if (kbase == 0) CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
+  if (first) {  // the products with the call's first row
     LAUNCH("k_kf_tiles_pj", s,
            (d.dense ? k_kf_tiles<KM_PJ, true> : k_kf_tiles<KM_PJ, false>)<<<d.ntile, 256, 0, s>>>(
                d.tiles, d.P, d.nw, d.pj, d.st, w, w, ra, 0, d.part));
@@ -651,6 +652,25 @@ int kf_iekf(KfDev &d, const double *row, const double *resid, const double *scal
   else
     LAUNCH("k_kf_wonly", s,
            (k_kf_wonly<<<(d.nw + 255) / 256, 256, 0, s>>>(d.nw, w, d.wprior, d.pj, d.st)));
+  CKK(cudaGetLastError());
+  return RC_OK;
+}
+
+// xi = -R for one point from its output derivatives out[na][nout] (the
+// first component) and a residual rule, in the order of the host's
+// residual (R = sum_k c_k T_k, or c_k T_0 T_k for a nonlinear term)
+__global__ void k_kf_resid(DevRule r, const double *__restrict__ out, int nout,
+                           double *__restrict__ xi) {
+  if (threadIdx.x != 0) return;
+  double R = 0.0;
+  for (int k = 0; k < r.nterm; ++k)
+    R = r.nonlin[k] ? R + r.coeff[k] * out[0] * out[(size_t)r.ind[k] * nout]
+                    : R + r.coeff[k] * out[(size_t)r.ind[k] * nout];
+  *xi = -R;
+}
+
+int kf_resid_xi(const DevRule &r, const double *out, int nout, double *xi, cudaStream_t s) {
+  LAUNCH("k_kf_resid", s, (k_kf_resid<<<1, 32, 0, s>>>(r, out, nout, xi)));
   CKK(cudaGetLastError());
   return RC_OK;
 }

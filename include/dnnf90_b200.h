@@ -148,6 +148,15 @@ int dnnf90_kf_update_rows(int kid, int nobs, const double *rows, const double *x
 int dnnf90_kf_update_rows_dev(int kid, int nobs, const double *rows_dev,
                               const double *xi_dev, const double *scale_dev,
                               double *w_dev, void *stream);
+/* a filter pass over npts points x[npts][d0] with a Jacobian-row rule:
+ * for each point in order, its row dR/dw and residual R at the network's
+ * current weights, then the update with xi = -R and scale 1/sqrt(rnoise)
+ * (kf_update_resid / kf_update_resid_multi, :252-300, as the trainer's
+ * lnet_kalman_resid calls them per point).  Everything stays on the device
+ * between points.  tid: a training work space of the filter's network,
+ * which must run in FP64 (else -5).  -1 for rnoise <= 0 or at a nonpositive
+ * denominator (the points before it stay applied). */
+int dnnf90_kf_pass(int kid, int tid, int npts, const double *x, int rid, double rnoise);
 /* iterated EKF (kf_iekf_begin / kf_iekf_iter, :509-640): begin stores the
  * network's current weights as the prior w-.  Each iteration takes
  * row = dR/dw and resid = R evaluated by the caller at the network's current

@@ -354,3 +354,41 @@ def test_one_launch_and_two_launch_paths_are_bit_identical(decoupled, monkeypatc
         api.tune_force(3, -1)
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
     assert out[0][2] == out[1][2]
+
+
+# ------------------------------------------------ per-point pass on the device
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("decoupled", [False, True])
+def test_device_filter_pass_matches_the_oracle_loop(decoupled):
+    """dnnf90_kf_pass: for each point its row dR/dw and R at the weights the
+    previous update left, then the update with xi = -R; against the oracle
+    running the same loop (its rows from the oracle's adjoint)."""
+    from dnnf90_b200 import api
+    dims = [2, 16, 16, 1]
+    ts = api.TableSet(2, 3, [[0, 1], [1, 0], [3, 0]])
+    tab = po.Tables(2, 3, [[0, 1], [1, 0], [3, 0]])
+    terms = [(1.0, ts.slot((0, 1)), 0), (6.0, ts.slot((1, 0)), 1), (1.0, ts.slot((3, 0)), 0)]
+    w0 = np.random.default_rng(31).normal(size=po.weight_count(dims)) * 0.4
+    X = np.random.default_rng(32).uniform(-1, 1, (30, 2))
+    net = api.Net(ts, dims, weights=w0)
+    rule = api.SeedRule(api.SEED_JROW, terms)
+    kf = api.Kalman(net, 0.5, 0.98, 0.9987, decoupled, 1e-4, gate=2.0)
+    kf.pass_points(X, rule, rnoise=0.25)
+    ref = po.Kalman(dims, 0.5, 0.98, 0.9987, decoupled, 1e-4, gate=2.0)
+    w = w0.copy()
+    for x in X:
+        _, T, _, rows = po.grad_batch(tab, dims, w, x[None, :], kind=po.SEED_JROW, terms=terms)
+        R = sum(c * (T[0, 0] * T[0, s - 1] if nl else T[0, s - 1]) for c, s, nl in terms)
+        ref.update(w, rows[0], -R, 1.0 / np.sqrt(0.25))
+    assert rel_err(net.get_weights(), w) < 1e-10, rel_err(net.get_weights(), w)
+    assert rel_err(kf.cov().reshape(-1), ref.P) < 1e-10
+    lam, ng = kf.state()
+    assert abs(lam - ref.lam) <= 1e-15 and ng == ref.ngated.value
+    with pytest.raises(api.Dnnf90Error):
+        kf.pass_points(X[:2], rule, rnoise=0.0)
+    net.set_precision(api.PREC_SPLIT)
+    with pytest.raises(api.Dnnf90Error):                  # the pass runs in FP64 only
+        kf.pass_points(X[:2], rule)
+    kf.free(); rule.free(); net.free(); ts.free()
