@@ -292,14 +292,20 @@ def committee_bench(api, dev, nsteps, nnet=64):
 
 # ------------------------------------------------------------------ our arm
 # ------------------------------------------------------------------ Kalman filter
-KF_METRIC = "EKF rank-one updates/s (kf_update_grad), dense covariance, FP64"
+def kf_metric():
+    return ("EKF rank-one updates/s (kf_update_grad), "
+            + ("decoupled" if KF_DECOUPLED[0] else "dense") + " covariance, FP64")
 KF_DIMS = [2, 128, 128, 1]   # --kf-dims overrides (e.g. 3,32,32,1 for a small filter)
+
+
+KF_DECOUPLED = [False]        # --kf-decoupled: the node-wise block filter
 
 
 def kf_workload(nobs):
     nw = sum(KF_DIMS[l] * (KF_DIMS[l - 1] + 1) for l in range(1, len(KF_DIMS)))
-    return nw, (f"EKF: dense global filter on MLP {'-'.join(map(str, KF_DIMS))} (nw={nw}, "
-                f"P packed upper triangle {nw * (nw + 1) * 4 / 2**30:.2f} GiB FP64), p0=0.01, "
+    kind = ("decoupled (one block per neuron) filter" if KF_DECOUPLED[0] else
+            f"dense global filter (P packed upper triangle {nw * (nw + 1) * 4 / 2**30:.2f} GiB FP64)")
+    return nw, (f"EKF: {kind} on MLP {'-'.join(map(str, KF_DIMS))} (nw={nw}), p0=0.01, "
                 f"lambda 0.98 -> 1 (lam0 0.9987), synthetic Jacobian rows N(0,1)/sqrt(nw) and "
                 f"innovations N(0,1); one step = {nobs} sequential rank-one updates")
 
@@ -309,6 +315,15 @@ def kf_rows(nw, nobs, step):
     return rng.normal(size=(nobs, nw)) / np.sqrt(nw), rng.normal(size=nobs)
 
 
+def kf_packed_elems(nw):
+    """Elements of the covariance's upper triangles: one block of nw, or one
+    block per neuron over (bias, fan-in)."""
+    if not KF_DECOUPLED[0]:
+        return nw * (nw + 1) // 2
+    return sum(KF_DIMS[l] * (KF_DIMS[l - 1] + 1) * (KF_DIMS[l - 1] + 2) // 2
+               for l in range(1, len(KF_DIMS)))
+
+
 def kf_cpu_baseline(nobs=1):
     """The oracle's kf_update_grad (one thread, dense nw x nw as the
     reference stores it) on a bounded sample: nobs updates."""
@@ -316,7 +331,7 @@ def kf_cpu_baseline(nobs=1):
     import pyoracle as po
 
     nw, _ = kf_workload(nobs)
-    kf = po.Kalman(KF_DIMS, 0.01, 0.98, 0.9987)
+    kf = po.Kalman(KF_DIMS, 0.01, 0.98, 0.9987, KF_DECOUPLED[0])
     w = xavier(KF_DIMS, 7)
     rows, xi = kf_rows(nw, nobs, 0)
     t0 = time.perf_counter()
@@ -325,7 +340,8 @@ def kf_cpu_baseline(nobs=1):
     dt = time.perf_counter() - t0
     return {"value": nobs / dt, "unit": "updates/s", "cores": 1, "kind": "port",
             "sample": f"{nobs} update(s) of the workload's filter, one host thread, FP64, "
-                      f"dense {nw}x{nw} covariance"}
+                      + ("node-wise block covariance" if KF_DECOUPLED[0] else
+                         f"dense {nw}x{nw} covariance")}
 
 
 def kalman_bench(args):
@@ -349,7 +365,7 @@ def kalman_bench(args):
         v = len(times) / sum(times)
         c["value"] = v
         print(json.dumps({
-            "impl": "reference", "metric": KF_METRIC, "value": v, "unit": "updates/s",
+            "impl": "reference", "metric": kf_metric(), "value": v, "unit": "updates/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -363,10 +379,13 @@ def kalman_bench(args):
     dev = torch.device("cuda", local)
     ts = api.TableSet(KF_DIMS[0], 1)
     net = api.Net(ts, KF_DIMS, weights=xavier(KF_DIMS, 7))
-    kf = api.Kalman(net, 0.01, 0.98, 0.9987)
+    kf = api.Kalman(net, 0.01, 0.98, 0.9987, KF_DECOUPLED[0])
     stream = torch.cuda.current_stream(dev)
     nstep = args.warmup + args.steps
-    host = [kf_rows(nw, nobs, s) for s in range(nstep)]
+    # the end-to-end arm copies from pinned host memory, as a host that
+    # streams observations would keep them
+    host = [tuple(torch.from_numpy(a).pin_memory().numpy() for a in kf_rows(nw, nobs, s))
+            for s in range(nstep)]
     rows_d = [torch.tensor(r, device=dev) for r, _ in host]
     xi_d = [torch.tensor(x, device=dev) for _, x in host]
     w_d = torch.tensor(net.get_weights(), device=dev)
@@ -433,26 +452,27 @@ def kalman_bench(args):
     roof = None
     if tl_n:
         per = tl_ms / tl_n
-        alg = nw * (nw + 1) / 2 * 8 * 2          # packed triangle read and written once
+        alg = kf_packed_elems(nw) * 8 * 2        # packed triangles read and written once
         ach = alg / (per * 1e-3) / 1e9
         roof = {"bound": "hbm", "kernel": "k_kf_tiles", "achieved": ach, "peak": hbm,
                 "unit": "GB/s", "frac": ach / hbm, "peak_source": src,
                 "alg_bytes_per_launch": alg, "launch_ms": per, "traffic": None,
                 "note": "one launch applies one update: the upper triangle of P read and "
                         "written once, the products with the next row formed in the same read"}
-    cpu = kf_cpu_baseline(max(1, min(2000, int(3e8 / nw ** 2)))) if (rank == 0 and ws == 1) else None
+    cpu = (kf_cpu_baseline(max(1, min(2000, int(1.5e8 / kf_packed_elems(nw)))))
+           if (rank == 0 and ws == 1) else None)
     if rank == 0:
         print(json.dumps({
-            "metric": KF_METRIC, "value": value, "unit": "updates/s", "n_gpus": ws,
+            "metric": kf_metric(), "value": value, "unit": "updates/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Jacobian rows and innovations)",
             "config": {"workload": workload, "updates_per_step": nobs,
                        "parallelism": f"replicas: one filter per GPU ({ws})",
                        "l2": ("inputs larger than L2: the covariance is "
-                              f"{nw * (nw + 1) * 4 / 2**30:.2f} GiB, read and written per update"
-                              if nw * (nw + 1) * 4 > 126e6 else
-                              f"the covariance ({nw * (nw + 1) * 4 / 2**20:.1f} MiB) stays in L2: "
+                              f"{kf_packed_elems(nw) * 8 / 2**30:.2f} GiB, read and written per update"
+                              if kf_packed_elems(nw) * 8 > 126e6 else
+                              f"the covariance ({kf_packed_elems(nw) * 8 / 2**20:.1f} MiB) stays in L2: "
                               "not flushed, an L2- and launch-bound case")},
             "kernel_ms_per_step": {k: v[1] for k, v in prof.items()},
             "kernel_launches_per_step": {k: v[0] for k, v in prof.items()},
@@ -490,10 +510,12 @@ def main():
                          "extended Kalman filter's rank-one updates")
     ap.add_argument("--kf-obs", type=int, default=16, help="Kalman updates per step")
     ap.add_argument("--kf-dims", default=None, help="Kalman network widths, e.g. 3,32,32,1")
+    ap.add_argument("--kf-decoupled", action="store_true", help="the node-wise block filter")
     args = ap.parse_args()
     if args.workload == "kalman":
         if args.kf_dims:
             KF_DIMS[:] = [int(v) for v in args.kf_dims.split(",")]
+        KF_DECOUPLED[0] = args.kf_decoupled
         return kalman_bench(args)
     if args.impl == "reference":
         return run_reference(args)

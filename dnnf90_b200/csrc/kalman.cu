@@ -242,6 +242,37 @@ __global__ void __launch_bounds__(256, 8) k_kf_tiles(const int4 *__restrict__ ti
   kf_tile_body<MODE>(tp, v, o, n, I, J, pslot, pj, sc, w, wb, ra, knext);
 }
 
+// Sum of the row tiles' shares dotp[2b] (and dotp[2b + 1]) over b < n in a
+// fixed order that does not depend on the block size: thread i < 256 adds
+// b = i, i + 256, ... in turn, and the 256 partial sums are added pairwise
+// (i + 128, i + 64, ...).  Every thread of the block calls it (at least 256
+// of them); the sums are returned to all.  The shares come from other CTAs,
+// so they are read past L1.
+__device__ __forceinline__ void kf_dot_sum(const double *dotp, int n, double &dot, double &cor) {
+  __shared__ double s_d[256], s_c[256];
+  const int i = threadIdx.x;
+  if (i < 256) {
+    double d = 0.0, c = 0.0;
+    for (int b = i; b < n; b += 256) {
+      d += __ldcg(dotp + 2 * b);
+      c += __ldcg(dotp + 2 * b + 1);
+    }
+    s_d[i] = d;
+    s_c[i] = c;
+  }
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if (i < h) {
+      s_d[i] += s_d[i + h];
+      s_c[i] += s_c[i + h];
+    }
+    __syncthreads();
+  }
+  dot = s_d[0];
+  cor = s_c[0];
+  __syncthreads();
+}
+
 // P j of row k from the partial slots, j.Pj per CTA, and in the last CTA
 // the scalars of observation k (denominator, gate, lambda).  One CTA per
 // row tile: its slots are contiguous ([slot][32]), warp g of 16 sums slots
@@ -288,13 +319,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_kf_reduce(const int4 *__restric
     }
   }
   __syncthreads();
-  if (!s_last || threadIdx.x != 0) return;
+  if (!s_last) return;
   __threadfence();
-  double dot = 0.0, cor = 0.0;
-  for (unsigned b = 0; b < gridDim.x; ++b) {
-    dot += ((volatile double *)dotp)[2 * b];
-    cor += ((volatile double *)dotp)[2 * b + 1];
-  }
+  double dot, cor;
+  kf_dot_sum(dotp, gridDim.x, dot, cor);
+  if (threadIdx.x != 0) return;
   *ctr = 0;
   const double lam = st->lam;
   double denom = lam + dot;
@@ -446,15 +475,18 @@ __global__ void __launch_bounds__(256) k_kf_seq(const int4 *__restrict__ tiles, 
         }
 #pragma unroll
         for (int off = 16; off; off >>= 1) prod += __shfl_xor_sync(0xffffffffu, prod, off);
-        if (lane == 0) dotp[2 * rt] = prod;
+        if (lane == 0) {
+          dotp[2 * rt] = prod;
+          dotp[2 * rt + 1] = 0.0;
+        }
       }
       __syncthreads();
     }
     if (!kf_grid_sync(bar, st)) return;
     // the scalars of observation k, the same in every CTA
+    double dot, cor;
+    kf_dot_sum(dotp, nred, dot, cor);
     if (threadIdx.x == 0) {
-      double dot = 0.0;
-      for (int b = 0; b < nred; ++b) dot += __ldcg(dotp + 2 * b);
       double denom = lam + dot;
       int fail = !(denom > 0.0);
       double xi = row_scale(ra, k) * ra.xi[k], sg = 1.0;
