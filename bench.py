@@ -379,6 +379,7 @@ def kalman_bench(args):
     dev = torch.device("cuda", local)
     ts = api.TableSet(KF_DIMS[0], 1)
     net = api.Net(ts, KF_DIMS, weights=xavier(KF_DIMS, 7))
+    api.tune_force(3, args.kf_path)
     kf = api.Kalman(net, 0.01, 0.98, 0.9987, KF_DECOUPLED[0])
     stream = torch.cuda.current_stream(dev)
     nstep = args.warmup + args.steps
@@ -511,6 +512,9 @@ def main():
     ap.add_argument("--kf-obs", type=int, default=16, help="Kalman updates per step")
     ap.add_argument("--kf-dims", default=None, help="Kalman network widths, e.g. 3,32,32,1")
     ap.add_argument("--kf-decoupled", action="store_true", help="the node-wise block filter")
+    ap.add_argument("--kf-path", type=int, default=-1, choices=[-1, 0, 1],
+                    help="Kalman update path: -1 by size, 0 two launches per update, "
+                         "1 one launch per call")
     args = ap.parse_args()
     if args.workload == "kalman":
         if args.kf_dims:

@@ -627,7 +627,10 @@ int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
   if (nobs <= 0) return RC_OK;
   KfRowArgs ra{rows, ld, xi, scale};
   const int path = g_kf_path.load();
-  if (d.seq_grid > 0 && (path == 1 || (path < 0 && d.ntile <= 4 * d.seq_grid))) {
+  // measured: one launch wins up to about 2K tiles (MLP 3-32-32-1 dense, 741
+  // tiles, 70K against 63K updates/s; 2-128-128-1 decoupled, 2063 tiles, 46K
+  // against 43K) and loses from 10K tiles on (3-64-64-1: 13K against 21K)
+  if (d.seq_grid > 0 && (path == 1 || (path < 0 && d.ntile <= 8 * d.seq_grid))) {
     if (kbase == 0) CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
     int fi = first ? 1 : 0, hn = has_next ? 1 : 0, ntile = d.ntile, nw = d.nw, nred = d.nred;
     void *args[] = {&d.tiles, &ntile, &d.P, &nw, &d.rtl, &nred, &d.part, &d.pj, &d.dotp,
