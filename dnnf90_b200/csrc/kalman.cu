@@ -23,11 +23,18 @@
 // the next row: row sums of tile (I, J) land in partial slot J of the rows
 // of I, column sums in slot I of the rows of J, so that every (slot, row)
 // is written once and no atomics are needed.  The reduce pass sums the
-// slots into P j for that row, forms j.Pj block by block, and its last CTA
-// (found with a counter, no waiting) turns the block sums into the global
-// denominator, applies the innovation gate and advances lambda.  A call
-// therefore reads and writes the covariance once per observation, plus one
-// read-only pass for the first row.
+// slots into P j for that row, forms j.Pj per row tile, and its last CTA
+// (found with a counter, no waiting) sums the row tiles' shares in a fixed
+// order into the global denominator, applies the innovation gate and
+// advances lambda.  A call therefore reads and writes the covariance once
+// per observation, plus one read-only pass for the first row.
+//
+// Small filters run a whole call as one cooperative launch (k_kf_seq): the
+// same tile code, reduce and scalar step as phases between bounded grid
+// barriers, with the same summation orders, so both paths give the same
+// bits.  The iterated EKF (kf_iekf_iter) reuses the two-launch kernels, and
+// the per-point pass (dnnf90_kf_pass) calls kf_run once per point with
+// that point's row formed on the device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
