@@ -157,6 +157,16 @@ def test_no_device_fails_loudly():
     with pytest.raises(api.Dnnf90Error):
         g.point(np.zeros(2), np.zeros(ts.na))
     g.free()
+    # the Kalman filter and the natural-gradient entries need the device too
+    with pytest.raises(api.Dnnf90Error) as e:
+        api.Kalman(net, 1.0, 0.98, 0.99)
+    assert e.value.rc == -3
+    with pytest.raises(api.Dnnf90Error) as e:
+        api.call("dnnf90_ngd_solve_dev", net.nw, 1, 1, 1, 1e-3, 1, None)
+    assert e.value.rc == -3
+    # argument checks come first
+    assert api.lib().dnnf90_kf_create(net.nid, 0.0, 0.98, 0.99, 0, 0.0, 0.0) == -1
+    assert api.lib().dnnf90_kf_update_rows(1, 1, None, None, None) == -1
     net.free()
 
 
