@@ -49,7 +49,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_ngd_step_dual", "dnnf90_kf_create", "dnnf90_kf_free", "dnnf90_kf_update_rows",
     "dnnf90_kf_update_rows_dev", "dnnf90_kf_read", "dnnf90_kf_iekf_begin",
     "dnnf90_kf_iekf_iter", "dnnf90_ngd_gram_dev", "dnnf90_ngd_solve_dev",
-    "dnnf90_ngd_step_dual_dev", "dnnf90_kf_pass",
+    "dnnf90_ngd_step_dual_dev", "dnnf90_kf_pass", "dnnf90_kf_pass_iekf",
 ]
 
 _lib = None
@@ -147,6 +147,7 @@ def lib():
         "dnnf90_ngd_solve_dev": [i, p, p, i, d, p, p],
         "dnnf90_ngd_step_dual_dev": [i, i, p, p, i, d, p, p],
         "dnnf90_kf_pass": [i, i, i, pd, i, d],
+        "dnnf90_kf_pass_iekf": [i, i, i, pd, i, d, i],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -470,12 +471,18 @@ class Kalman:
         call("dnnf90_kf_update_rows", self.kid, rows.shape[0], _pd(rows), _pd(xi),
              None if sc is None else _pd(sc))
 
-    def pass_points(self, X, rule: "SeedRule", rnoise: float = 1.0):
+    def pass_points(self, X, rule: "SeedRule", rnoise: float = 1.0, niter: int = 0):
         """One filter update per point, each from the point's row and
-        residual at the weights the previous update left (dnnf90_kf_pass)."""
+        residual at the weights the previous update left (dnnf90_kf_pass);
+        niter >= 1 takes the iterated update with niter relinearisations
+        per point (dnnf90_kf_pass_iekf)."""
         X = _f64(np.atleast_2d(X))
-        call("dnnf90_kf_pass", self.kid, self.net.tid, X.shape[0], _pd(X), rule.rid,
-             float(rnoise))
+        if niter:
+            call("dnnf90_kf_pass_iekf", self.kid, self.net.tid, X.shape[0], _pd(X), rule.rid,
+                 float(rnoise), int(niter))
+        else:
+            call("dnnf90_kf_pass", self.kid, self.net.tid, X.shape[0], _pd(X), rule.rid,
+                 float(rnoise))
 
     def iekf_begin(self):
         """The network's current weights become the prior of the iteration."""

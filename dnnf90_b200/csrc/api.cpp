@@ -1797,8 +1797,10 @@ int dnnf90_kf_update_rows_dev(int kid, int nobs, const double *rows_dev, const d
   return kf_status_rc(s);
 }
 
-int dnnf90_kf_pass(int kid, int tid, int npts, const double *x, int rid, double rnoise) {
-  std::lock_guard<std::recursive_mutex> lk(g_mu);
+namespace {
+// the per-point filter pass: niter = 0 the plain update, >= 1 the iterated
+// one with niter relinearisations per point
+int kf_pass(int kid, int tid, int npts, const double *x, int rid, double rnoise, int niter) {
   int rc = kf_check(kid);
   if (rc) return rc;
   KfH &k = g_kf[kid];
@@ -1843,26 +1845,59 @@ int dnnf90_kf_pass(int kid, int tid, int npts, const double *x, int rid, double 
     return rc;
   // per point: its row and residual at the current weights (the forward
   // and adjoint read the device weights the filter has just moved), then
-  // the rank-one update of kf_update_resid (:252-275): xi = -R
+  // the rank-one update of kf_update_resid (:252-275), xi = -R; or, iterated
+  // (kf_iekf_begin / kf_iekf_iter :509-640), the prior stored and niter
+  // relinearisations from it, the last one downdating the covariance
+  BatchArgs a;
+  a.npts = 1;
+  a.out = w.p.out;
+  a.rows = drow;
+  a.loss = dloss;
+  a.train = true;
+  a.prec = PREC_F64;
+  if (niter > 0 &&
+      (rc = ck(cudaMemsetAsync(&k.d.st->status, 0, sizeof(int), w.st), "status reset")))
+    return rc;
   for (int p = 0; p < npts && !rc; ++p) {
-    BatchArgs a;
-    a.npts = 1;
     a.X = dX + (size_t)p * d0;
-    a.out = w.p.out;
-    a.rows = drow;
-    a.loss = dloss;
-    a.train = true;
-    a.prec = PREC_F64;
-    if ((rc = run_batch(n.dt, n.dn, rule.d, w.p, a, w.st))) break;
-    if ((rc = kf_resid_xi(rule.d, w.p.out, nout, dxi, w.st))) break;
-    rc = kf_run(k.d, 1, drow, nw, dxi, dsc, n.dn.w64, w.st, p, false, true);
+    if (niter == 0) {
+      if ((rc = run_batch(n.dt, n.dn, rule.d, w.p, a, w.st))) break;
+      if ((rc = kf_resid_xi(rule.d, w.p.out, nout, dxi, w.st))) break;
+      rc = kf_run(k.d, 1, drow, nw, dxi, dsc, n.dn.w64, w.st, p, false, true);
+      continue;
+    }
+    if ((rc = ck(cudaMemcpyAsync(k.d.wprior, n.dn.w64, sizeof(double) * nw,
+                                 cudaMemcpyDeviceToDevice, w.st), "D2D")))
+      break;
+    for (int it = 0; it < niter && !rc; ++it) {
+      if ((rc = run_batch(n.dt, n.dn, rule.d, w.p, a, w.st))) break;
+      if ((rc = kf_resid_xi(rule.d, w.p.out, nout, dxi, w.st, 1.0))) break;  // R itself
+      rc = kf_iekf(k.d, drow, dxi, dsc, n.dn.w64, it == niter - 1, w.st, p, false);
+    }
   }
+  if (niter > 0) k.d.prior = false;  // the prior of the last point is not the caller's
   if (!rc) rc = ck(cudaMemcpyAsync(n.w.data(), n.dn.w64, sizeof(double) * nw,
                                    cudaMemcpyDeviceToHost, w.st), "D2H");
   KfState s;
   if (!rc) rc = kf_state(k.d, &s, w.st);
   n.wver++;  // the host copy now holds what the device computed
   return rc ? rc : kf_status_rc(s);
+}
+}  // namespace
+
+int dnnf90_kf_pass(int kid, int tid, int npts, const double *x, int rid, double rnoise) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  return kf_pass(kid, tid, npts, x, rid, rnoise, 0);
+}
+
+int dnnf90_kf_pass_iekf(int kid, int tid, int npts, const double *x, int rid, double rnoise,
+                        int niter) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (niter < 1) {
+    set_error("kf_pass_iekf: at least one iteration per point");
+    return RC_BAD_ARG;
+  }
+  return kf_pass(kid, tid, npts, x, rid, rnoise, niter);
 }
 
 int dnnf90_kf_iekf_begin(int kid) {

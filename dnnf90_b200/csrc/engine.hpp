@@ -256,14 +256,18 @@ int kf_create(KfDev &d, const std::vector<int> &bsz, const std::vector<int> &bof
 int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
            const double *scale, double *w, cudaStream_t s, int kbase, bool has_next,
            bool first);
-// xi[0] = -R of one point's output derivatives under a Jacobian-row rule
-int kf_resid_xi(const DevRule &r, const double *out, int nout, double *xi, cudaStream_t s);
+// xi[0] = sign * R of one point's output derivatives under a Jacobian-row
+// rule (sign -1: the innovation of a residual, whose target is zero)
+int kf_resid_xi(const DevRule &r, const double *out, int nout, double *xi, cudaStream_t s,
+                double sign = -1.0);
 // one relinearisation of the iterated EKF (kf_iekf_iter): row = dR/dw at
 // the current weights w, resid[0] = R, scale[0] = 1/sqrt(rnoise); w <- w- +
 // kv xi with the prior d.wprior; the covariance and lambda change only when
 // final
+// kbase numbers the observation in the status; reset clears the status
+// first (a pass over points keeps it, so that a failure stops the rest)
 int kf_iekf(KfDev &d, const double *row, const double *resid, const double *scale, double *w,
-            bool final, cudaStream_t s);
+            bool final, cudaStream_t s, int kbase = 0, bool reset = true);
 int kf_state(const KfDev &d, KfState *out, cudaStream_t s);
 // the update path: -1 by size (default), 0 two launches per update, 1 one
 // cooperative launch per call

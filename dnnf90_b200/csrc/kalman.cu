@@ -676,16 +676,16 @@ int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
 }
 
 int kf_iekf(KfDev &d, const double *row, const double *resid, const double *scale, double *w,
-            bool final, cudaStream_t s) {
+            bool final, cudaStream_t s, int kbase, bool reset) {
   KfRowArgs ra{row, (size_t)d.nw, resid, scale};
   const KfIekf ie{d.wprior, w, final ? 1 : 0};
-  CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
+  if (reset) CKK(cudaMemsetAsync(&d.st->status, 0, sizeof(int), s));
   LAUNCH("k_kf_tiles_pj", s,
          (d.dense ? k_kf_tiles<KM_PJ, true> : k_kf_tiles<KM_PJ, false>)<<<d.ntile, 256, 0, s>>>(
              d.tiles, d.P, d.nw, d.pj, d.st, w, w, ra, 0, d.part));
   LAUNCH("k_kf_reduce", s,
-         (k_kf_reduce<<<d.nred, RED_THREADS, 0, s>>>(d.rtl, d.part, d.pj, ra, 0, 0, ie, d.dotp,
-                                                     d.ctr, d.st)));
+         (k_kf_reduce<<<d.nred, RED_THREADS, 0, s>>>(d.rtl, d.part, d.pj, ra, 0, kbase, ie,
+                                                     d.dotp, d.ctr, d.st)));
   if (final)
     LAUNCH("k_kf_tiles", s,
            (d.dense ? k_kf_tiles<KM_UPD, true> : k_kf_tiles<KM_UPD, false>)<<<d.ntile, 256, 0,
@@ -702,17 +702,18 @@ int kf_iekf(KfDev &d, const double *row, const double *resid, const double *scal
 // first component) and a residual rule, in the order of the host's
 // residual (R = sum_k c_k T_k, or c_k T_0 T_k for a nonlinear term)
 __global__ void k_kf_resid(DevRule r, const double *__restrict__ out, int nout,
-                           double *__restrict__ xi) {
+                           double *__restrict__ xi, double sign) {
   if (threadIdx.x != 0) return;
   double R = 0.0;
   for (int k = 0; k < r.nterm; ++k)
     R = r.nonlin[k] ? R + r.coeff[k] * out[0] * out[(size_t)r.ind[k] * nout]
                     : R + r.coeff[k] * out[(size_t)r.ind[k] * nout];
-  *xi = -R;
+  *xi = sign * R;
 }
 
-int kf_resid_xi(const DevRule &r, const double *out, int nout, double *xi, cudaStream_t s) {
-  LAUNCH("k_kf_resid", s, (k_kf_resid<<<1, 32, 0, s>>>(r, out, nout, xi)));
+int kf_resid_xi(const DevRule &r, const double *out, int nout, double *xi, cudaStream_t s,
+                double sign) {
+  LAUNCH("k_kf_resid", s, (k_kf_resid<<<1, 32, 0, s>>>(r, out, nout, xi, sign)));
   CKK(cudaGetLastError());
   return RC_OK;
 }

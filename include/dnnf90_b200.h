@@ -157,6 +157,13 @@ int dnnf90_kf_update_rows_dev(int kid, int nobs, const double *rows_dev,
  * which must run in FP64 (else -5).  -1 for rnoise <= 0 or at a nonpositive
  * denominator (the points before it stay applied). */
 int dnnf90_kf_pass(int kid, int tid, int npts, const double *x, int rid, double rnoise);
+/* the same pass with the iterated update: for each point the current
+ * weights become the prior and niter >= 1 relinearisations follow, each from
+ * the row and residual at the weights the last one left; the last downdates
+ * the covariance (kf_iekf_begin / kf_iekf_iter, :509-640).  niter = 1 is the
+ * plain pass. */
+int dnnf90_kf_pass_iekf(int kid, int tid, int npts, const double *x, int rid, double rnoise,
+                        int niter);
 /* iterated EKF (kf_iekf_begin / kf_iekf_iter, :509-640): begin stores the
  * network's current weights as the prior w-.  Each iteration takes
  * row = dR/dw and resid = R evaluated by the caller at the network's current

@@ -392,3 +392,43 @@ def test_device_filter_pass_matches_the_oracle_loop(decoupled):
     with pytest.raises(api.Dnnf90Error):                  # the pass runs in FP64 only
         kf.pass_points(X[:2], rule)
     kf.free(); rule.free(); net.free(); ts.free()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("niter", [1, 3])
+def test_device_iterated_pass_matches_the_oracle(niter):
+    """dnnf90_kf_pass_iekf against the oracle's kf_iekf_begin / kf_iekf_iter
+    loop, each relinearisation from the oracle's row and residual at the
+    current weights; one iteration is the plain pass."""
+    from dnnf90_b200 import api
+    dims = [2, 16, 16, 1]
+    ts = api.TableSet(2, 3, [[0, 1], [1, 0], [3, 0]])
+    tab = po.Tables(2, 3, [[0, 1], [1, 0], [3, 0]])
+    terms = [(1.0, ts.slot((0, 1)), 0), (6.0, ts.slot((1, 0)), 1), (1.0, ts.slot((3, 0)), 0)]
+    w0 = np.random.default_rng(41).normal(size=po.weight_count(dims)) * 0.4
+    X = np.random.default_rng(42).uniform(-1, 1, (20, 2))
+    net = api.Net(ts, dims, weights=w0)
+    rule = api.SeedRule(api.SEED_JROW, terms)
+    kf = api.Kalman(net, 0.5, 0.98, 0.9987, False, 1e-4)
+    kf.pass_points(X, rule, rnoise=0.25, niter=niter)
+    ref = po.Kalman(dims, 0.5, 0.98, 0.9987, False, 1e-4)
+    w = w0.copy()
+    for x in X:
+        ref.iekf_begin(w)
+        for it in range(niter):
+            _, T, _, rows = po.grad_batch(tab, dims, w, x[None, :], kind=po.SEED_JROW,
+                                          terms=terms)
+            R = sum(c * (T[0, 0] * T[0, s - 1] if nl else T[0, s - 1]) for c, s, nl in terms)
+            ref.iekf_iter(w, rows[0], R, 0.25, it == niter - 1)
+    assert rel_err(net.get_weights(), w) < 1e-10, rel_err(net.get_weights(), w)
+    assert rel_err(kf.cov().reshape(-1), ref.P) < 1e-10
+    assert abs(kf.state()[0] - ref.lam) <= 1e-15
+    if niter == 1:   # one iteration per point is the plain pass
+        net2 = api.Net(ts, dims, weights=w0)
+        kf2 = api.Kalman(net2, 0.5, 0.98, 0.9987, False, 1e-4)
+        kf2.pass_points(X, rule, rnoise=0.25)
+        assert rel_err(net2.get_weights(), net.get_weights()) < 1e-13
+        kf2.free(); net2.free()
+    with pytest.raises(api.Dnnf90Error):
+        api.call("dnnf90_kf_pass_iekf", kf.kid, net.tid, 1, api._pd(X), rule.rid, 0.25, 0)
+    kf.free(); rule.free(); net.free(); ts.free()
