@@ -17,7 +17,13 @@ The data are synthetic: no dataset is involved.
 
 For N > 1 it runs under torch.distributed.run, one rank per GPU; points are
 sharded (weak scaling: 65,536 per GPU) and dL/dw is all-reduced over NCCL
-once per step.  Rank 0 prints one JSON line.
+once per step.  Rank 0 prints one JSON line.  At N = 1 the line also carries
+the extended Kalman filter's own line under "kalman" (--no-kalman skips it).
+
+  python bench.py --workload kalman [--kf-dims 3,32,32,1] [--kf-decoupled]
+
+measures the filter alone: rank-one updates/s of the dense (or node-wise)
+covariance, with its roofline, end-to-end figure and CPU baseline.
 """
 from __future__ import annotations
 
@@ -506,6 +512,8 @@ def main():
                          "launches upset the autotuner's timings")
     ap.add_argument("--prof-steps", type=int, default=1,
                     help="steps of the per-kernel event-profiled pass (untimed)")
+    ap.add_argument("--no-kalman", action="store_true",
+                    help="leave the Kalman filter's line out of the default run")
     ap.add_argument("--workload", default="zk7", choices=["zk7", "kalman"],
                     help="zk7: the collocation training step (default); kalman: the "
                          "extended Kalman filter's rank-one updates")
@@ -759,6 +767,25 @@ def main():
         acc = accuracy(api, ts, w, terms)
     committee = committee_bench(api, dev, args.committee_steps) if args.committee_steps > 0 else None
     cpu = cpu_baseline(args.ref_points, 1) if (rank == 0 and ws == 1) else None
+    # the Kalman filter's own line (bench.py --workload kalman), measured in a
+    # child process on the same GPU and carried here
+    kalman = None
+    if rank == 0 and ws == 1 and not args.no_kalman:
+        import subprocess
+
+        try:
+            out = subprocess.run([sys.executable, os.path.abspath(__file__), "--workload", "kalman",
+                                  "--steps", "3", "--warmup", "2"],
+                                 capture_output=True, text=True, timeout=600)
+            if out.returncode == 0:
+                d = json.loads(out.stdout.strip().splitlines()[-1])
+                kalman = {k: d.get(k) for k in ("metric", "value", "unit", "ms_per_step", "steps",
+                                                "warmup", "e2e", "roofline", "clocks",
+                                                "cpu_baseline", "gpu_launches", "config")}
+            else:
+                kalman = {"error": out.stderr[-400:]}
+        except Exception as e:  # the headline line is printed whatever happens here
+            kalman = {"error": str(e)[:400]}
 
     if rank == 0:
         line = {
@@ -781,6 +808,7 @@ def main():
             "kernel_ms_per_step": per_step_ms(prof),
             "accuracy": acc,
             "committee": committee,
+            "kalman": kalman,
             "autotuner": [list(t) for t in api.tune_report()],
             "e2e": e2e,
             "gpu_launches": launches,
