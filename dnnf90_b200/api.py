@@ -49,7 +49,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_ngd_step_dual", "dnnf90_kf_create", "dnnf90_kf_free", "dnnf90_kf_update_rows",
     "dnnf90_kf_update_rows_dev", "dnnf90_kf_read", "dnnf90_kf_iekf_begin",
     "dnnf90_kf_iekf_iter", "dnnf90_ngd_gram_dev", "dnnf90_ngd_solve_dev",
-    "dnnf90_ngd_step_dual_dev", "dnnf90_kf_pass", "dnnf90_kf_pass_iekf",
+    "dnnf90_ngd_step_dual_dev", "dnnf90_kf_pass", "dnnf90_kf_pass_iekf", "dnnf90_kf_pass_sys",
 ]
 
 _lib = None
@@ -148,6 +148,7 @@ def lib():
         "dnnf90_ngd_step_dual_dev": [i, i, p, p, i, d, p, p],
         "dnnf90_kf_pass": [i, i, i, pd, i, d],
         "dnnf90_kf_pass_iekf": [i, i, i, pd, i, d, i],
+        "dnnf90_kf_pass_sys": [i, i, i, pd, pd, i, pd, i],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -483,6 +484,15 @@ class Kalman:
         else:
             call("dnnf90_kf_pass", self.kid, self.net.tid, X.shape[0], _pd(X), rule.rid,
                  float(rnoise))
+
+    def pass_system(self, X, rule: "SeedRule", src=None, rnoise=None, niter: int = 0):
+        """One update per point and residual of a system rule, each from the
+        residual's row and value at the current weights (dnnf90_kf_pass_sys)."""
+        X = _f64(np.atleast_2d(X))
+        sv = None if src is None else _f64(src)
+        rn = None if rnoise is None else _f64(np.atleast_1d(rnoise))
+        call("dnnf90_kf_pass_sys", self.kid, self.net.tid, X.shape[0], _pd(X), _pd(sv),
+             rule.rid, _pd(rn), int(niter))
 
     def iekf_begin(self):
         """The network's current weights become the prior of the iteration."""

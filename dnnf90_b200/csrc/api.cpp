@@ -1900,6 +1900,101 @@ int dnnf90_kf_pass_iekf(int kid, int tid, int npts, const double *x, int rid, do
   return kf_pass(kid, tid, npts, x, rid, rnoise, niter);
 }
 
+int dnnf90_kf_pass_sys(int kid, int tid, int npts, const double *x, const double *src, int rid,
+                       const double *rnoise, int niter) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = kf_check(kid);
+  if (rc) return rc;
+  KfH &k = g_kf[kid];
+  const int nid = k.nid;
+  if ((rc = check_train(nid, tid, 0, false))) return rc;
+  if (bad_rule(rid) || g_rule[rid].r.kind != SEED_SYS) return RC_BAD_ARG;
+  if (npts < 0 || (npts > 0 && !x) || niter < 0) return RC_BAD_ARG;
+  RuleH &rule = g_rule[rid];
+  const int nres = rule.r.nres;
+  std::vector<double> sc(nres, 1.0);
+  for (int r = 0; r < nres && rnoise; ++r) {
+    if (!(rnoise[r] > 0.0)) {  // kf_update_resid_multi :286-290
+      set_error("kf_pass_sys: observation noise must be > 0");
+      return RC_BAD_ARG;
+    }
+    sc[r] = 1.0 / std::sqrt(rnoise[r]);
+  }
+  if (npts == 0) return RC_OK;
+  NetH &n = g_net[nid];
+  if (n.prec != PREC_F64) {
+    set_error("kf_pass_sys: the per-point filter pass runs on the FP64 path");
+    return RC_UNSUPPORTED;
+  }
+  WorkH &w = g_twk[tid];
+  if ((rc = flush_queue(tid))) return rc;
+  flush_for_net(nid);
+  if ((rc = work_stream(w))) return rc;
+  if ((rc = net_device(n, w.st))) return rc;
+  if ((rc = rule_device(rule, n))) return rc;
+  if ((rc = work_planes(w, n, 1, false))) return rc;
+  w.kept = false;  // the kept planes below belong to this pass
+  const int nw = (int)n.w.size(), d0 = n.ts.d0, na = n.ts.na, nout = n.dims[n.nlayer - 1];
+  const size_t need =
+      ((size_t)nw + (size_t)nout * na + 1 + nres + (size_t)npts * (d0 + nres)) * sizeof(double);
+  if (k.d.stage_bytes < need) {
+    cudaFree(k.d.stage);
+    k.d.stage = nullptr;
+    k.d.stage_bytes = 0;
+    if ((rc = ck(cudaMalloc(&k.d.stage, need), "cudaMalloc"))) return rc;
+    k.d.stage_bytes = need;
+  }
+  double *drow = k.d.stage, *dseed = drow + nw, *dxi = dseed + (size_t)nout * na,
+         *dsc = dxi + 1, *dX = dsc + nres, *dsrc = dX + (size_t)npts * d0;
+  if ((rc = ck(cudaMemcpyAsync(dX, x, sizeof(double) * (size_t)npts * d0,
+                               cudaMemcpyHostToDevice, w.st), "H2D")) ||
+      (rc = ck(cudaMemcpyAsync(dsc, sc.data(), sizeof(double) * nres, cudaMemcpyHostToDevice,
+                               w.st), "H2D")))
+    return rc;
+  if (src && (rc = ck(cudaMemcpyAsync(dsrc, src, sizeof(double) * (size_t)npts * nres,
+                                      cudaMemcpyHostToDevice, w.st), "H2D")))
+    return rc;
+  if ((rc = ck(cudaMemsetAsync(&k.d.st->status, 0, sizeof(int), w.st), "status reset")))
+    return rc;
+  // per point and residual, at the current weights: the forward (planes
+  // kept), R_ir and its seed, the adjoint into the row, then the update of
+  // kf_update_resid_multi (xi = -R, scale 1/sqrt(rnoise_ir)); or, iterated,
+  // niter relinearisations from the prior, the last one downdating
+  auto observe = [&](int p, int r, double sign) {
+    const double *xp = dX + (size_t)p * d0;
+    int e = forward_keep(n.dt, n.dn, w.p, PREC_F64, 1, xp, w.p.out, w.st);
+    if (!e) e = kf_sys_seed(rule.d, w.p.out, na, nout, src ? dsrc + (size_t)p * nres : nullptr,
+                            r, dseed, dxi, sign, w.st);
+    if (!e) e = ck(cudaMemsetAsync(drow, 0, sizeof(double) * nw, w.st), "memset");
+    if (!e) e = adjoint_kept(n.dt, n.dn, w.p, PREC_F64, 1, xp, dseed, drow, w.st);
+    return e;
+  };
+  for (int p = 0; p < npts && !rc; ++p)
+    for (int r = 0; r < nres && !rc; ++r) {
+      const int obs = p * nres + r;
+      if (niter == 0) {
+        if ((rc = observe(p, r, -1.0))) break;
+        rc = kf_run(k.d, 1, drow, nw, dxi, dsc + r, n.dn.w64, w.st, obs == 0 ? 0 : obs, false,
+                    true);
+        continue;
+      }
+      if ((rc = ck(cudaMemcpyAsync(k.d.wprior, n.dn.w64, sizeof(double) * nw,
+                                   cudaMemcpyDeviceToDevice, w.st), "D2D")))
+        break;
+      for (int it = 0; it < niter && !rc; ++it) {
+        if ((rc = observe(p, r, 1.0))) break;
+        rc = kf_iekf(k.d, drow, dxi, dsc + r, n.dn.w64, it == niter - 1, w.st, obs, false);
+      }
+    }
+  if (niter > 0) k.d.prior = false;
+  if (!rc) rc = ck(cudaMemcpyAsync(n.w.data(), n.dn.w64, sizeof(double) * nw,
+                                   cudaMemcpyDeviceToHost, w.st), "D2H");
+  KfState s;
+  if (!rc) rc = kf_state(k.d, &s, w.st);
+  n.wver++;
+  return rc ? rc : kf_status_rc(s);
+}
+
 int dnnf90_kf_iekf_begin(int kid) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   int rc = kf_check(kid);

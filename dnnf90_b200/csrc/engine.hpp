@@ -260,6 +260,10 @@ int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
 // rule (sign -1: the innovation of a residual, whose target is zero)
 int kf_resid_xi(const DevRule &r, const double *out, int nout, double *xi, cudaStream_t s,
                 double sign = -1.0);
+// residual ir of a system rule at one point, xi[0] = sign * R_ir, and its
+// seed dR_ir/dT into seed[nout][na]; src[nres] may be null
+int kf_sys_seed(const DevRule &r, const double *out, int na, int nout, const double *src,
+                int ir, double *seed, double *xi, double sign, cudaStream_t s);
 // one relinearisation of the iterated EKF (kf_iekf_iter): row = dR/dw at
 // the current weights w, resid[0] = R, scale[0] = 1/sqrt(rnoise); w <- w- +
 // kv xi with the prior d.wprior; the covariance and lambda change only when

@@ -718,6 +718,47 @@ int kf_resid_xi(const DevRule &r, const double *out, int nout, double *xi, cudaS
   return RC_OK;
 }
 
+// One observation of a system (the trainer's loop over sys_nres,
+// app/sgd_batch_module.f90:497-545): from one point's output derivatives
+// out[na][nout], residual ir of a system rule (calc_sys_residual,
+// app/pinn_module.f90:86-125) as xi = sign * R_ir, and its seed dR_ir/dT
+// in seed[nout][na] (set_sys_seed :127-162 with a one in slot ir, fac 1,
+// unweighted).
+__global__ void k_kf_sys_seed(DevRule r, const double *__restrict__ out, int na, int nout,
+                              const double *__restrict__ src, int ir,
+                              double *__restrict__ seed, double *__restrict__ xi, double sign) {
+  for (int i = threadIdx.x; i < nout * na; i += blockDim.x) seed[i] = 0.0;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  auto T = [&](int f) {  // factor f: (component, slot), 0-based
+    return out[(size_t)r.sfac[2 * f + 1] * nout + r.sfac[2 * f]];
+  };
+  double R = src ? -src[ir] : 0.0;
+  for (int k = 0; k < r.nterm; ++k) {
+    if (r.sys[3 * k] != ir) continue;
+    const int nf = r.sys[3 * k + 1], f0 = r.sys[3 * k + 2];
+    double prod = r.coeff[k];
+    for (int m = 0; m < nf; ++m) prod = prod * T(f0 + m);
+    R = R + prod;
+    for (int m = 0; m < nf; ++m) {
+      double other = r.coeff[k];
+      for (int mm = 0; mm < nf; ++mm)
+        if (mm != m) other = other * T(f0 + mm);
+      const int at = r.sfac[2 * (f0 + m)] * na + r.sfac[2 * (f0 + m) + 1];
+      seed[at] = seed[at] + other;
+    }
+  }
+  *xi = sign * R;
+}
+
+int kf_sys_seed(const DevRule &r, const double *out, int na, int nout, const double *src,
+                int ir, double *seed, double *xi, double sign, cudaStream_t s) {
+  LAUNCH("k_kf_sys_seed", s,
+         (k_kf_sys_seed<<<1, 256, 0, s>>>(r, out, na, nout, src, ir, seed, xi, sign)));
+  CKK(cudaGetLastError());
+  return RC_OK;
+}
+
 int kf_state(const KfDev &d, KfState *out, cudaStream_t s) {
   CKK(cudaMemcpyAsync(out, d.st, sizeof(KfState), cudaMemcpyDeviceToHost, s));
   CKK(cudaStreamSynchronize(s));

@@ -164,6 +164,16 @@ int dnnf90_kf_pass(int kid, int tid, int npts, const double *x, int rid, double 
  * plain pass. */
 int dnnf90_kf_pass_iekf(int kid, int tid, int npts, const double *x, int rid, double rnoise,
                         int niter);
+/* the filter pass over a system of residuals (a rule of
+ * dnnf90_seed_rule_sys), as the trainer presents one (app/sgd_batch_module.f90:
+ * 497-545): for each point and each residual r in turn, at the network's
+ * current weights, R_r (with src[npts][nres], NULL for none) and its row
+ * dR_r/dw (seeded unweighted with dR_r/dT), then the update of
+ * kf_update_resid_multi with xi = -R_r and scale 1/sqrt(rnoise[r])
+ * (rnoise NULL: 1).  niter >= 1 takes the iterated update with niter
+ * relinearisations per residual; 0 the plain one.  FP64 networks only. */
+int dnnf90_kf_pass_sys(int kid, int tid, int npts, const double *x, const double *src,
+                       int rid, const double *rnoise, int niter);
 /* iterated EKF (kf_iekf_begin / kf_iekf_iter, :509-640): begin stores the
  * network's current weights as the prior w-.  Each iteration takes
  * row = dR/dw and resid = R evaluated by the caller at the network's current

@@ -432,3 +432,74 @@ def test_device_iterated_pass_matches_the_oracle(niter):
     with pytest.raises(api.Dnnf90Error):
         api.call("dnnf90_kf_pass_iekf", kf.kid, net.tid, 1, api._pd(X), rule.rid, 0.25, 0)
     kf.free(); rule.free(); net.free(); ts.free()
+
+
+# ------------------------------------------------ systems of residuals
+
+
+def _sys_terms(slot):
+    """Two residuals over outputs (u, v): u u_x + v_y and u_y - v v_x + 0.3 u_xx."""
+    s = {k: slot(v) for k, v in dict(v0=(0, 0), x=(1, 0), y=(0, 1), xx=(2, 0)).items()}
+    U, V = 1, 2
+    return [(1, 1.0, [(U, s["v0"]), (U, s["x"])]), (1, 1.0, [(V, s["y"])]),
+            (2, 1.0, [(U, s["y"])]), (2, -1.0, [(V, s["v0"]), (V, s["x"])]),
+            (2, 0.3, [(U, s["xx"])])]
+
+
+def _oracle_sys_obs(tab, dims, w, x, terms, ir, src):
+    """R_ir at the weights w, and the row dR_ir/dw by the oracle's adjoint
+    seeded with dR_ir/dT (set_sys_seed with a one in slot ir, unweighted)."""
+    _, tall = po.eval_point(tab, dims, w, x)
+    T = lambda f: tall[f[0] - 1, f[1] - 1]
+    R = -src[ir - 1] if src is not None else 0.0
+    seed = np.zeros_like(tall)
+    for r, c, fs in terms:
+        if r != ir:
+            continue
+        R += c * np.prod([T(f) for f in fs])
+        for m, f in enumerate(fs):
+            seed[f[0] - 1, f[1] - 1] += c * np.prod([T(g) for mm, g in enumerate(fs) if mm != m])
+    row, _ = po.grad_point(tab, dims, w, x, seed)
+    return R, row
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("niter", [0, 2])
+def test_device_system_pass_matches_the_oracle_loop(niter):
+    """dnnf90_kf_pass_sys: each point's residuals in turn, each re-evaluated
+    at the weights the previous update left, with per-residual noise; the
+    oracle runs the trainer's loop (app/sgd_batch_module.f90:497-545)."""
+    from dnnf90_b200 import api
+    dims = [2, 16, 16, 2]
+    ts = api.TableSet(2, 2)
+    tab = po.Tables(2, 2)
+    terms = _sys_terms(ts.slot)
+    w0 = np.random.default_rng(51).normal(size=po.weight_count(dims)) * 0.4
+    X = np.random.default_rng(52).uniform(-1, 1, (12, 2))
+    src = np.random.default_rng(53).normal(size=(12, 2)) * 0.1
+    rnoise = np.array([0.5, 2.0])
+    net = api.Net(ts, dims, weights=w0)
+    rule = api.SeedRule.system(2, terms)
+    kf = api.Kalman(net, 0.5, 0.98, 0.9987, False, 1e-4)
+    kf.pass_system(X, rule, src=src, rnoise=rnoise, niter=niter)
+    ref = po.Kalman(dims, 0.5, 0.98, 0.9987, False, 1e-4)
+    w = w0.copy()
+    for p, x in enumerate(X):
+        for ir in (1, 2):
+            if niter == 0:
+                R, row = _oracle_sys_obs(tab, dims, w, x, terms, ir, src[p])
+                ref.update(w, row, -R, 1.0 / np.sqrt(rnoise[ir - 1]))
+                continue
+            ref.iekf_begin(w)
+            for it in range(niter):
+                R, row = _oracle_sys_obs(tab, dims, w, x, terms, ir, src[p])
+                ref.iekf_iter(w, row, R, rnoise[ir - 1], it == niter - 1)
+    assert rel_err(net.get_weights(), w) < 1e-10, rel_err(net.get_weights(), w)
+    assert rel_err(kf.cov().reshape(-1), ref.P) < 1e-10
+    assert abs(kf.state()[0] - ref.lam) <= 1e-15
+    with pytest.raises(api.Dnnf90Error):
+        kf.pass_system(X[:1], rule, rnoise=[1.0, 0.0])
+    jr = api.SeedRule(api.SEED_JROW, [(1.0, ts.slot((1, 0)), 0)])
+    with pytest.raises(api.Dnnf90Error):                    # a system rule is needed
+        kf.pass_system(X[:1], jr)
+    kf.free(); jr.free(); rule.free(); net.free(); ts.free()
