@@ -1711,6 +1711,17 @@ int kf_check(int kid) {
   return RC_OK;
 }
 
+// the filter's device staging area, grown to at least need bytes
+int kf_stage(KfH &k, size_t need) {
+  if (k.d.stage_bytes >= need) return RC_OK;
+  cudaFree(k.d.stage);
+  k.d.stage = nullptr;
+  k.d.stage_bytes = 0;
+  int rc = ck(cudaMalloc(&k.d.stage, need), "cudaMalloc");
+  if (!rc) k.d.stage_bytes = need;
+  return rc;
+}
+
 int kf_status_rc(const KfState &s) {
   if (!s.status) return RC_OK;
   if (s.status < 0) {
@@ -1743,13 +1754,7 @@ int dnnf90_kf_update_rows(int kid, int nobs, const double *rows, const double *x
   if (const char *e = std::getenv("DNNF90_KF_STAGE_KB")) stage = (size_t)std::max(1, std::atoi(e)) << 10;
   const int chunk = (int)std::max<size_t>(1, std::min<size_t>(nobs, stage / (8 * nw)));
   const size_t need = ((size_t)(chunk + 1) * (nw + 2) + nw) * sizeof(double);
-  if (k.d.stage_bytes < need) {
-    cudaFree(k.d.stage);
-    k.d.stage = nullptr;
-    k.d.stage_bytes = 0;
-    if ((rc = ck(cudaMalloc(&k.d.stage, need), "cudaMalloc"))) return rc;
-    k.d.stage_bytes = need;
-  }
+  if ((rc = kf_stage(k, need))) return rc;
   double *dw = k.d.stage, *dr = dw + nw, *dxi = dr + (size_t)(chunk + 1) * nw,
          *dsc = dxi + chunk + 1;
   if ((rc = ck(cudaMemcpyAsync(dw, n.w.data(), nw * 8, cudaMemcpyHostToDevice, k.st), "H2D")))
@@ -1829,13 +1834,7 @@ int kf_pass(int kid, int tid, int npts, const double *x, int rid, double rnoise,
   if ((rc = work_planes(w, n, 1, false))) return rc;
   const int nw = (int)n.w.size(), d0 = n.ts.d0, nout = n.dims[n.nlayer - 1];
   const size_t need = ((size_t)npts * d0 + nw + 3) * sizeof(double);
-  if (k.d.stage_bytes < need) {
-    cudaFree(k.d.stage);
-    k.d.stage = nullptr;
-    k.d.stage_bytes = 0;
-    if ((rc = ck(cudaMalloc(&k.d.stage, need), "cudaMalloc"))) return rc;
-    k.d.stage_bytes = need;
-  }
+  if ((rc = kf_stage(k, need))) return rc;
   double *drow = k.d.stage, *dxi = drow + nw, *dsc = dxi + 1, *dloss = dsc + 1,
          *dX = dloss + 1;
   const double sc = 1.0 / std::sqrt(rnoise);
@@ -1937,13 +1936,7 @@ int dnnf90_kf_pass_sys(int kid, int tid, int npts, const double *x, const double
   const int nw = (int)n.w.size(), d0 = n.ts.d0, na = n.ts.na, nout = n.dims[n.nlayer - 1];
   const size_t need =
       ((size_t)nw + (size_t)nout * na + 1 + nres + (size_t)npts * (d0 + nres)) * sizeof(double);
-  if (k.d.stage_bytes < need) {
-    cudaFree(k.d.stage);
-    k.d.stage = nullptr;
-    k.d.stage_bytes = 0;
-    if ((rc = ck(cudaMalloc(&k.d.stage, need), "cudaMalloc"))) return rc;
-    k.d.stage_bytes = need;
-  }
+  if ((rc = kf_stage(k, need))) return rc;
   double *drow = k.d.stage, *dseed = drow + nw, *dxi = dseed + (size_t)nout * na,
          *dsc = dxi + 1, *dX = dsc + nres, *dsrc = dX + (size_t)npts * d0;
   if ((rc = ck(cudaMemcpyAsync(dX, x, sizeof(double) * (size_t)npts * d0,
@@ -2028,13 +2021,7 @@ int dnnf90_kf_iekf_iter(int kid, const double *row, double resid, double rnoise,
     return rc;
   const size_t nw = n.w.size();
   const size_t need = (2 * nw + 2) * sizeof(double);
-  if (k.d.stage_bytes < need) {
-    cudaFree(k.d.stage);
-    k.d.stage = nullptr;
-    k.d.stage_bytes = 0;
-    if ((rc = ck(cudaMalloc(&k.d.stage, need), "cudaMalloc"))) return rc;
-    k.d.stage_bytes = need;
-  }
+  if ((rc = kf_stage(k, need))) return rc;
   double *dw = k.d.stage, *dr = dw + nw, *dsc = dr + nw;
   const double sc[2] = {1.0 / std::sqrt(rnoise), resid};
   if ((rc = ck(cudaMemcpyAsync(dw, n.w.data(), nw * 8, cudaMemcpyHostToDevice, k.st), "H2D")) ||
