@@ -50,6 +50,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_kf_update_rows_dev", "dnnf90_kf_read", "dnnf90_kf_iekf_begin",
     "dnnf90_kf_iekf_iter", "dnnf90_ngd_gram_dev", "dnnf90_ngd_solve_dev",
     "dnnf90_ngd_step_dual_dev", "dnnf90_kf_pass", "dnnf90_kf_pass_iekf", "dnnf90_kf_pass_sys",
+    "dnnf90_kf_status",
 ]
 
 _lib = None
@@ -149,6 +150,7 @@ def lib():
         "dnnf90_kf_pass": [i, i, i, pd, i, d],
         "dnnf90_kf_pass_iekf": [i, i, i, pd, i, d, i],
         "dnnf90_kf_pass_sys": [i, i, i, pd, pd, i, pd, i],
+        "dnnf90_kf_status": [i],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -2051,6 +2051,17 @@ int dnnf90_kf_read(int kid, double *lam, int *ngated, double *P) {
   return rc;
 }
 
+int dnnf90_kf_status(int kid) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (kid < 1 || kid > MAXH || !g_kf[kid].used) return RC_BAD_ARG;
+  KfH &k = g_kf[kid];
+  if (k.st) cudaStreamSynchronize(k.st);
+  KfState s;
+  const int rc = kf_state(k.d, &s, nullptr);
+  if (rc) return rc;
+  return s.status < 0 ? RC_DEVICE : s.status;
+}
+
 int dnnf90_ngd_step_noalloc(int nrow, int nw, const double *rows_dev, const double *b_dev,
                             int nb, double mu, double *u_dev, void *stream) {
   if (nrow < 1 || nw < 1 || nb < 1 || !rows_dev || !b_dev || !u_dev) return RC_BAD_ARG;

@@ -633,7 +633,12 @@ int kf_run(KfDev &d, int nobs, const double *rows, size_t ld, const double *xi,
            bool first) {
   if (nobs <= 0) return RC_OK;
   KfRowArgs ra{rows, ld, xi, scale};
-  const int path = g_kf_path.load();
+  int path = g_kf_path.load();
+  // a stream being captured into a graph takes the two-launch path, whose
+  // kernels are plain launches
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    path = 0;
   // measured: one launch wins up to about 2K tiles (MLP 3-32-32-1 dense, 741
   // tiles, 70K against 63K updates/s; 2-128-128-1 decoupled, 2063 tiles, 46K
   // against 43K) and loses from 10K tiles on (3-64-64-1: 13K against 21K)

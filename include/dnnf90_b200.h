@@ -144,7 +144,10 @@ int dnnf90_kf_free(int kid);
 int dnnf90_kf_update_rows(int kid, int nobs, const double *rows, const double *xi,
                           const double *scale);
 /* the same on device arrays; w_dev[nw] (flat layout) is updated in place
- * and the network's own weights are left alone */
+ * and the network's own weights are left alone.  Returns after the work on
+ * stream has finished, with the filter's status checked; while the stream
+ * is being captured into a graph it returns without waiting, and
+ * dnnf90_kf_status tells after a replay whether an update failed. */
 int dnnf90_kf_update_rows_dev(int kid, int nobs, const double *rows_dev,
                               const double *xi_dev, const double *scale_dev,
                               double *w_dev, void *stream);
@@ -190,6 +193,10 @@ int dnnf90_kf_iekf_iter(int kid, const double *row, double resid, double rnoise,
  * covariance, dense [nw][nw] or the decoupled blocks [n_b][n_b] one after
  * another in the weight order */
 int dnnf90_kf_read(int kid, double *lam, int *ngated, double *P);
+/* the filter's status after its last call: 0, or 1 + the observation at
+ * which a denominator was not positive (the updates from there on were not
+ * applied); -3 if a device wait gave up; -1 for a bad handle */
+int dnnf90_kf_status(int kid);
 
 /* ---- device-pointer entry points (pointers to device memory; stream is
  * a cudaStream_t, NULL for the legacy default stream).  On the split path

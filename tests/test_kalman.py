@@ -201,6 +201,7 @@ def test_device_kalman_stops_at_a_nonpositive_denominator():
     with pytest.raises(api.Dnnf90Error):
         kf.update_rows(rows, xi, sc)
     assert "observation 7" in api.lib().dnnf90_last_error().decode()
+    assert api.lib().dnnf90_kf_status(kf.kid) == 7
     ref = po.Kalman(dims, 0.7, 0.98, 0.9987)
     wref = np.zeros(nw)
     for k in range(6):
@@ -208,6 +209,7 @@ def test_device_kalman_stops_at_a_nonpositive_denominator():
     assert rel_err(net.get_weights(), wref) < 1e-11
     assert rel_err(kf.cov().reshape(-1), ref.P) < 1e-11 and abs(kf.state()[0] - ref.lam) < 1e-15
     kf.update_rows(rows[7:], xi[7:], sc[7:])    # the filter goes on from there
+    assert api.lib().dnnf90_kf_status(kf.kid) == 0
     for k in range(7, 10):
         ref.update(wref, rows[k], xi[k], sc[k])
     assert rel_err(net.get_weights(), wref) < 1e-11
@@ -503,3 +505,33 @@ def test_device_system_pass_matches_the_oracle_loop(niter):
     with pytest.raises(api.Dnnf90Error):                    # a system rule is needed
         kf.pass_system(X[:1], jr)
     kf.free(); jr.free(); rule.free(); net.free(); ts.free()
+
+
+@pytest.mark.gpu
+def test_device_entry_captured_in_a_cuda_graph():
+    """Under stream capture the update takes the two-launch path and returns
+    without waiting; one replay applies the same updates, to the bit, as a
+    direct call (which takes the one-launch path at this size)."""
+    import torch
+    from dnnf90_b200 import api
+    dims = [3, 20, 20, 1]
+    (kfa, neta, tsa), _, _, (rows, xi, sc) = _run_both(dims, False, 1e-4, 1.5, 24)
+    (kfb, netb, tsb), _, _, _ = _run_both(dims, False, 1e-4, 1.5, 24)
+    dev = torch.device("cuda", 0)
+    rd, xd, sd = (torch.tensor(a, device=dev) for a in (rows, xi, sc))
+    wa = torch.tensor(neta.get_weights(), device=dev)
+    wb = wa.clone()
+    api.call("dnnf90_kf_update_rows_dev", kfa.kid, len(xi), rd.data_ptr(), xd.data_ptr(),
+             sd.data_ptr(), wa.data_ptr(), torch.cuda.current_stream(dev).cuda_stream)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        api.call("dnnf90_kf_update_rows_dev", kfb.kid, len(xi), rd.data_ptr(), xd.data_ptr(),
+                 sd.data_ptr(), wb.data_ptr(), torch.cuda.current_stream(dev).cuda_stream)
+    g.replay()
+    torch.cuda.synchronize(dev)
+    assert api.lib().dnnf90_kf_status(kfb.kid) == 0
+    assert torch.equal(wa, wb)
+    assert np.array_equal(kfa.cov(), kfb.cov()) and kfa.state() == kfb.state()
+    del g
+    for kf, net, ts in ((kfa, neta, tsa), (kfb, netb, tsb)):
+        kf.free(); net.free(); ts.free()
