@@ -182,3 +182,22 @@ def test_tabset_free_releases_the_handle():
     for i in (ids[0], ids[2], again):
         assert L.dnnf90_tabset_free(i) == 0
     assert L.dnnf90_tabset_free(0) == -1 and L.dnnf90_tabset_free(65) == -1
+
+
+def test_headers_parse_as_plain_c(tmp_path):
+    """include/*.h is the boundary a C host compiles against: both headers
+    parse as pedantic C99 (no C++ in the signatures) and as C++."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if not gcc:
+        pytest.skip("no C compiler")
+    src = tmp_path / "h.c"
+    src.write_text('#include "dnnf90.h"\n#include "dnnf90_b200.h"\nint main(void){return 0;}\n')
+    inc = os.path.join(ROOT, "include")
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only",
+                    "-I", inc, str(src)], check=True)
+    gxx = shutil.which("g++")
+    if gxx:
+        subprocess.run([gxx, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", inc,
+                        "-x", "c++", str(src)], check=True)
