@@ -66,6 +66,23 @@ def test_oracle_one_block_decoupled_is_dense():
     assert np.array_equal(wa, wb) and np.array_equal(a.P, b.P) and a.lam == b.lam
 
 
+def test_oracle_decoupled_first_update_is_the_dense_diagonal_blocks():
+    """From P = p0 I (block diagonal) the first update gives both filters
+    the same P j, the same global denominator and the same weight step; the
+    decoupled covariance is then the dense one's diagonal blocks."""
+    dims = [3, 5, 4, 1]
+    nw = po.weight_count(dims)
+    rows, xi, sc = _random_sequence(nw, 1, 9)
+    d, b = po.Kalman(dims, 0.8, 0.97, 0.99, q=1e-3, gate=1.0), po.Kalman(dims, 0.8, 0.97, 0.99, True, q=1e-3, gate=1.0)
+    wd, wb = np.zeros(nw), np.zeros(nw)
+    d.update(wd, rows[0], xi[0], sc[0])
+    b.update(wb, rows[0], xi[0], sc[0])
+    assert np.array_equal(wd, wb) and d.lam == b.lam and d.ngated.value == b.ngated.value
+    Pd = d.P.reshape(nw, nw)
+    blocks = np.concatenate([Pd[o:o + n, o:o + n].reshape(-1) for o, n in zip(b.boff, b.bsz)])
+    assert np.array_equal(blocks, b.P)
+
+
 def test_oracle_gate_is_a_noise_scale():
     """A tripped gate applies the update of the row and innovation scaled
     by s, s^2 = gate^2 lambda / (xi^2 - gate^2 j.Pj), which leaves the
