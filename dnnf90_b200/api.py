@@ -462,6 +462,7 @@ class Kalman:
                  decoupled: bool = False, q: float = 0.0, gate: float = 0.0):
         self.net = net
         self.decoupled = bool(decoupled)
+        self.kid = 0
         self.kid = check("dnnf90_kf_create",
                          lib().dnnf90_kf_create(net.nid, float(p0), float(lam_ini),
                                                 float(lam0), int(decoupled), float(q),
@@ -526,6 +527,12 @@ class Kalman:
         if self.kid > 0:
             lib().dnnf90_kf_free(self.kid)
             self.kid = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def committee_step(nets, rules, xs, grads, loss, stream=None):
