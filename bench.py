@@ -15,15 +15,24 @@ The data are synthetic: no dataset is involved.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-For N > 1 it runs under torch.distributed.run, one rank per GPU; points are
-sharded (weak scaling: 65,536 per GPU) and dL/dw is all-reduced over NCCL
-once per step.  Rank 0 prints one JSON line.  At N = 1 the line also carries
-the extended Kalman filter's own line under "kalman" (--no-kalman skips it).
+For N > 1 it runs as N ranks, one per GPU (started directly with --gpus N
+it re-runs itself under torch.distributed.run); points are sharded (weak
+scaling: 65,536 per GPU) and dL/dw is all-reduced over NCCL once per step.
+Rank 0 prints one JSON line.  The line leads with the split path's speed-up
+over the plain FP64 GPU path and the per-order error of both against the
+oracle.
+
+  python bench.py --workload ngd
+
+measures the damped natural-gradient step of the heat configuration (D0 = 3,
+K = 2, closure of {0, e_t, 2e_x, 2e_y}, MLP 3-64-64-1, 4096 points): the
+Jacobian rows, the metric on the tensor cores and the FP64 Cholesky solve.
 
   python bench.py --workload kalman [--kf-dims 3,32,32,1] [--kf-decoupled]
 
-measures the filter alone: rank-one updates/s of the dense (or node-wise)
-covariance, with its roofline, end-to-end figure and CPU baseline.
+measures the extended Kalman filter alone: rank-one updates/s of the dense
+(or node-wise) covariance, with its roofline, end-to-end figure and CPU
+baseline.
 """
 from __future__ import annotations
 
@@ -154,33 +163,47 @@ def dist_init():
         import datetime
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return ws, rank, local
 
 
 # ------------------------------------------------------------------ CPU baseline
-def cpu_baseline(npts=24, reps=1):
+def cpu_baseline(threads=0, per_thread=32):
     """The oracle (the CPU restatement of the reference's Fortran path,
     OpenMP over points, one work space per thread) on a bounded sample of
-    the same workload."""
+    the same workload: per_thread points for each of the threads, so that
+    every thread carries the same share (the reference's timing protocol,
+    tools/fwd_grad_timing.f90:56-80: one warm-up, then the timed pass)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
 
+    threads = threads or os.cpu_count() or 1
+    npts = threads * per_thread
     tab = po.Tables(D0, K)
     w = xavier(DIMS, 20260801)
     X = points(npts, 0)
     terms = zk7_terms(tab.alpha, tab.slot)
-    po.grad_batch(tab, DIMS, w, X[:2], kind=po.SEED_PINN, terms=terms)  # warm
+    po.grad_batch(tab, DIMS, w, X[:threads], kind=po.SEED_PINN, terms=terms, nthreads=threads,
+                  want_t=False)  # warm
     t0 = time.perf_counter()
-    for _ in range(reps):
-        po.grad_batch(tab, DIMS, w, X, kind=po.SEED_PINN, terms=terms, want_t=False)
+    po.grad_batch(tab, DIMS, w, X, kind=po.SEED_PINN, terms=terms, nthreads=threads,
+                  want_t=False)
     dt = time.perf_counter() - t0
-    cores = os.cpu_count() or 1
-    return {"value": npts * reps / dt, "unit": "pts/s", "cores": cores, "kind": "port",
-            "sample": f"{npts} points of the workload x {reps}, all {cores} host threads "
-                      f"(OpenMP over points), FP64"}
+    return {"value": npts / dt, "unit": "pts/s", "cores": threads, "kind": "port",
+            "seconds": round(dt, 3),
+            "sample": f"{npts} points of the workload ({per_thread} per thread), {threads} "
+                      f"host thread(s), OpenMP over points, FP64"}
+
+
+def cpu_baselines():
+    """All host threads, and one thread (comparable with the reference's
+    published single-core figures)."""
+    full = cpu_baseline()
+    one = cpu_baseline(threads=1)
+    full["one_thread"] = {k: one[k] for k in ("value", "seconds", "sample")}
+    return full
 
 
 def run_reference(args):
@@ -188,54 +211,65 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    per_step = args.ref_points
-    cb = cpu_baseline(per_step, 1)  # also warms the oracle
+    threads = os.cpu_count() or 1
+    cb = cpu_baseline(threads)  # also warms the oracle
     times = []
     for s in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        cpu_baseline(per_step, 1)
+        c = cpu_baseline(threads)
         if s >= args.warmup:
-            times.append(time.perf_counter() - t0)
+            times.append(c["seconds"])
+    per_step = threads * 32
     v = per_step * len(times) / sum(times)
     cb["value"] = v
+    cb.pop("seconds", None)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "pts/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample_points_per_step": per_step,
-                       "implementation": "CPU restatement of the reference's Fortran path "
-                                         "(the reference itself cannot be compiled here: no "
-                                         "Fortran compiler on the image)"},
+            "config": config_of(ws, args.points),
+            "implementation": "CPU restatement of the reference's Fortran path, all host threads "
+                              f"(the reference itself cannot be compiled here: no Fortran "
+                              f"compiler); each step times {per_step} points of the workload",
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
+def config_of(ws, npts):
+    return {"workload": WORKLOAD, "points_per_gpu": npts, "global_points": ws * npts,
+            "parallelism": f"dp{ws}: points sharded, dL/dw all-reduced (NCCL)",
+            "l2": "inputs larger than L2 (126 MB): a work chunk's planes are ~48 GB, so no flush"}
+
+
 # ------------------------------------------------------------------ error check
-def accuracy(api, ts, w, rule_terms, nsample=6):
-    """Per-order error of the split path's T and the gradient error against
-    the FP64 oracle (and of the plain path), on nsample points."""
+def accuracy(api, ts, w, rule_terms, nsample=64):
+    """Per-order error of the carried derivatives and the error of dL/dw
+    against the FP64 oracle, for the split and the plain path, on nsample
+    points of the workload (normwise per order, the reference's convention,
+    app/hod_check_module.f90:216,302)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
 
     tab = po.Tables(D0, K)
     X = points(nsample, 99)
     gref, Tref, lref, _ = po.grad_batch(tab, DIMS, w, X, kind=po.SEED_PINN, terms=rule_terms)
-    out = {}
+    out = {"points": nsample, "bar_split": 1e-5, "bar_f64": 1e-12}
     for name, prec in (("split", api.PREC_SPLIT), ("f64", api.PREC_F64)):
         net = api.Net(ts, DIMS, weights=w, precision=prec)
         g = net.grad()
         r = api.SeedRule(api.SEED_PINN, rule_terms)
         loss, T = g.rule_batch(X, r, want_t=True)
         gd = g.read()
-        per = {}
+        per = []
         for p in range(K + 1):
             m = tab.deg == p
-            per[p] = float(np.max(np.abs(T[:, m] - Tref[:, m])) / np.max(np.abs(Tref[:, m])))
+            per.append(float(np.max(np.abs(T[:, m] - Tref[:, m])) / np.max(np.abs(Tref[:, m]))))
         eg = float(np.max(np.abs(gd - gref)) / np.max(np.abs(gref)))
-        out[name] = {"max_rel_err_T": max(per.values()), "rel_err_grad": eg,
-                     "per_order": {str(k): v for k, v in per.items()}}
+        out[name] = {"max_rel_err_T": float(f"{max(per):.3g}"),
+                     "rel_err_grad": float(f"{eg:.3g}"),
+                     "rel_err_loss": float(f"{abs(loss - lref) / abs(lref):.3g}"),
+                     "per_order": [float(f"{e:.2g}") for e in per]}
         r.free()
         g.free()
         net.free()
@@ -243,34 +277,42 @@ def accuracy(api, ts, w, rule_terms, nsample=6):
 
 
 # ------------------------------------------------------------------ committee
-def committee_bench(api, dev, nsteps, nnet=64):
-    """Uneven committee: nnet independent networks, widths from
-    {32, 64, 128, 256}, 2-4 hidden tanh layers, D0 from 2-4 and K from 2-7
-    (dense sets), 1k-64k points log-uniform in [-1,1]^D0, split precision,
-    L = sum T^2/2 per network; one step = forward + seed + adjoint of every
-    member, replayed as one CUDA graph.  Returns the summary object."""
-    import torch
-
+def committee_members(nnet=64):
+    """The uneven committee's draw, one seeded generator for every member:
+    (d0, K, width, hidden layers, points [npts][d0], weight seed) per
+    network, widths from {32, 64, 128, 256}, 2-4 hidden tanh layers, D0
+    from 2-4, K from 2-7 (dense sets), 1k-64k points log-uniform in
+    [-1,1]^D0."""
     rng = np.random.default_rng(20260804)
-    tabs, nets, xs, grads = {}, [], [], []
-    rule = api.SeedRule(api.SEED_HALFSQ)
-    total = 0
-    shapes = []
+    out = []
     for i in range(nnet):
         width = int(rng.choice([32, 64, 128, 256]))
         depth = int(rng.integers(2, 5))
         d0 = int(rng.integers(2, 5))
         k = int(rng.integers(2, 8))
         npts = int(np.exp(rng.uniform(np.log(1000.0), np.log(64000.0))))
+        out.append((d0, k, width, depth, rng.uniform(-1.0, 1.0, (npts, d0)), 1000 + i))
+    return out
+
+
+def committee_bench(api, dev, nsteps, nnet=64):
+    """Uneven committee (committee_members), split precision, L = sum T^2/2
+    per network; one step = forward + seed + adjoint of every member,
+    replayed as one CUDA graph.  Returns the summary object."""
+    import torch
+
+    tabs, nets, xs, grads = {}, [], [], []
+    rule = api.SeedRule(api.SEED_HALFSQ)
+    total = 0
+    for d0, k, width, depth, X, wseed in committee_members(nnet):
         if (d0, k) not in tabs:
             tabs[(d0, k)] = api.TableSet(d0, k)
         dims = [d0] + [width] * depth + [1]
-        nets.append(api.Net(tabs[(d0, k)], dims, weights=xavier(dims, 1000 + i),
+        nets.append(api.Net(tabs[(d0, k)], dims, weights=xavier(dims, wseed),
                             precision=api.PREC_SPLIT))
-        xs.append(torch.tensor(rng.uniform(-1.0, 1.0, (npts, d0)), device=dev))
+        xs.append(torch.tensor(X, device=dev))
         grads.append(torch.zeros(nets[-1].nw, dtype=torch.float64, device=dev))
-        total += npts
-        shapes.append([d0, k, width, depth, npts])
+        total += X.shape[0]
     loss = torch.zeros(nnet, dtype=torch.float64, device=dev)
     rules = [rule] * nnet
     t0 = time.perf_counter()
@@ -293,7 +335,7 @@ def committee_bench(api, dev, nsteps, nnet=64):
     return {"nets": nnet, "points": total, "ms_per_step": ms, "pts_per_s": total / (ms / 1e3),
             "steps": nsteps, "graph_policy": ["by work", "by sqrt(work)", "uncapped"][policy],
             "graph_replay_ms": graph_ms, "first_call_s": build_s, "losses_finite": finite,
-            "precision": "split", "shapes_d0_k_width_depth_points": shapes}
+            "precision": "split"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -494,6 +536,217 @@ def kalman_bench(args):
     return 0
 
 
+# ------------------------------------------------------------------ natural gradient
+NGD_DIMS = [3, 64, 64, 1]
+NGD_SEEDS = [[1, 0, 0], [0, 2, 0], [0, 0, 2]]
+NGD_POINTS, NGD_MU = 4096, 1e-6
+NGD_METRIC = "damped natural-gradient steps/s (Jacobian rows, J^T J on the tensor cores, FP64 Cholesky)"
+NGD_WORKLOAD = ("heat: D0=3 (t,x,y), K=2, closure of {0, e_t, 2e_x, 2e_y} (6 slots), MLP 3-64-64-1 "
+                "tanh (4481 weights), 4096 points U[0,1]^3, R = u_t - (u_xx + u_yy); one step = "
+                "b = J^T R, the 4096 x 4481 Jacobian rows, G = J^T J / N + mu I (mu = 1e-6, split-BF16 "
+                "tensor-core products, FP32 accumulation per 512 rows, FP64 across), Cholesky solve in FP64")
+
+
+def ngd_case(api):
+    ts = api.TableSet(3, 2, NGD_SEEDS)
+    terms = [(1.0, ts.slot((1, 0, 0)), 0), (-1.0, ts.slot((0, 2, 0)), 0),
+             (-1.0, ts.slot((0, 0, 2)), 0)]
+    w = xavier(NGD_DIMS, 20260805)
+    X = np.random.default_rng(20260806).uniform(0.0, 1.0, (NGD_POINTS, 3))
+    return ts, terms, w, X
+
+
+def ngd_cpu_baseline(nsample_rows=24):
+    """The oracle on the box's host: the Jacobian rows of every point (all
+    host threads) and the metric build of app/optimizer_module.f90:310-321
+    in the reference's loop order, one thread, on nsample_rows of the rows
+    and scaled to all of them (its cost is linear in the rows).  The O(nw^3)
+    Gaussian elimination is left out: in the reference's loop order it takes
+    minutes at nw = 4481, so the figure is an upper bound on the CPU's
+    step rate."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    tab = po.Tables(3, 2, NGD_SEEDS)
+    slot = {tuple(int(v) for v in tab.alpha[i]): i + 1 for i in range(tab.na)}
+    terms = [(1.0, slot[(1, 0, 0)], 0), (-1.0, slot[(0, 2, 0)], 0), (-1.0, slot[(0, 0, 2)], 0)]
+    w = xavier(NGD_DIMS, 20260805)
+    X = np.random.default_rng(20260806).uniform(0.0, 1.0, (NGD_POINTS, 3))
+    t0 = time.perf_counter()
+    _, _, _, rows = po.grad_batch(tab, NGD_DIMS, w, X, kind=po.SEED_JROW, terms=terms,
+                                  want_t=False)
+    t_rows = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    po.ngd_metric(rows[:nsample_rows])
+    t_met = (time.perf_counter() - t0) * NGD_POINTS / nsample_rows
+    return {"value": 1.0 / (t_rows + t_met), "unit": "steps/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": f"Jacobian rows of all {NGD_POINTS} points ({t_rows:.2f} s, all host threads) + "
+                      f"the metric build on {nsample_rows} rows, one thread, scaled x"
+                      f"{NGD_POINTS // nsample_rows} ({t_met:.1f} s); the O(nw^3) solve is left "
+                      "out, so this overstates the CPU's rate"}
+
+
+def ngd_bench(args):
+    import torch
+
+    from dnnf90_b200 import api
+
+    ws, rank, local = dist_init()
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        ngd_cpu_baseline(4)                       # warm
+        times = []
+        for s in range(args.warmup + args.steps):
+            c = ngd_cpu_baseline(8)
+            if s >= args.warmup:
+                times.append(1.0 / c["value"])
+        v = len(times) / sum(times)
+        c["value"] = v
+        print(json.dumps({
+            "impl": "reference", "metric": NGD_METRIC, "value": v, "unit": "steps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": NGD_WORKLOAD, "parallelism": f"replicas ({ws})"},
+            "cpu_baseline": c,
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
+    dev = torch.device("cuda", local)
+    ts, terms, w, Xh = ngd_case(api)
+    net = api.Net(ts, NGD_DIMS, weights=w, precision=api.PREC_SPLIT)
+    nw, npts = net.nw, NGD_POINTS
+    rj = api.SeedRule(api.SEED_JROW, terms)
+    rp = api.SeedRule(api.SEED_PINN, terms)
+    X = torch.tensor(Xh, device=dev)
+    rows = torch.empty((npts, nw), dtype=torch.float64, device=dev)
+    G = torch.empty((nw, nw), dtype=torch.float64, device=dev)
+    b = torch.empty(nw, dtype=torch.float64, device=dev)
+    u = torch.empty(nw, dtype=torch.float64, device=dev)
+    loss = torch.empty(1, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    st = stream.cuda_stream
+
+    def step():
+        b.zero_()
+        loss.zero_()
+        api.call("dnnf90_grad_rule_dev", net.nid, net.tid, npts, X.data_ptr(), rp.rid,
+                 b.data_ptr(), loss.data_ptr(), None, st)
+        api.call("dnnf90_jrow_dev", net.nid, net.tid, npts, X.data_ptr(), rj.rid,
+                 rows.data_ptr(), None, st)
+        api.call("dnnf90_ngd_gram_dev", npts, nw, rows.data_ptr(), api.PREC_SPLIT,
+                 G.data_ptr(), st)
+        api.call("dnnf90_ngd_solve_dev", nw, G.data_ptr(), b.data_ptr(), npts, NGD_MU,
+                 u.data_ptr(), st)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ck = Clocks(local)
+    ck.__enter__()
+    ck.wait_first()
+    ck.mark()
+    n0 = api.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    launches = api.launch_count() - n0
+    ms = e0.elapsed_time(e1) / args.steps
+    ck.__exit__()
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # per-kernel device times of one more step
+    api.profile_read()
+    api.profile_enable(True)
+    step()
+    torch.cuda.synchronize(dev)
+    api.profile_enable(False)
+    prof = api.profile_read()
+    _, tc, src = peaks()
+    gram_n, gram_ms = prof.get("k_tc_gemm_dw", (0, 0.0))
+    roof = None
+    if gram_n:
+        flops = 2.0 * npts * nw * (nw + 1) / 2       # the lower triangle of J^T J
+        ach = flops / (gram_ms / gram_n * 1e-3) / 1e12
+        roof = {"bound": "tensor", "kernel": "k_tc_gemm_dw (J^T J)", "achieved": ach, "peak": tc,
+                "unit": "TFLOP/s", "frac": ach / tc, "peak_source": src, "traffic": None,
+                "useful_flops_per_launch": flops, "launch_ms": gram_ms / gram_n,
+                "note": "useful flops of the lower triangle; the split products run 6 bf16 "
+                        "MMAs per useful one"}
+    # end to end through the host entries: points in, rows out and back in
+    gh = net.grad()
+    Xpin = torch.tensor(Xh).pin_memory().numpy()
+
+    def e2e_step():
+        gh.zero()
+        gh.rule_batch(Xpin, rp)
+        bh = gh.read()
+        rh, _, _ = api.jacobian_rows(net, Xpin, rj)
+        return api.ngd_step(net, rh, bh, npts, NGD_MU, api.PREC_SPLIT)
+
+    e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / max(1, args.steps)
+    gh.free()
+    cpu = ngd_cpu_baseline() if (rank == 0 and ws == 1) else None
+    if rank == 0:
+        print(json.dumps({
+            "metric": NGD_METRIC, "value": ws * 1000.0 / ms, "unit": "steps/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 rows and solve, split-bf16 metric (fp32 accumulate)",
+            "data": "synthetic (seeded uniform points, Xavier-normal weights)",
+            "config": {"workload": NGD_WORKLOAD, "parallelism": f"replicas ({ws})",
+                       "l2": "the 147 MB rows exceed L2; no flush"},
+            "kernel_ms_per_step": {k: round(v[1], 3) for k, v in
+                                   sorted(prof.items(), key=lambda kv: -kv[1][1])},
+            "e2e": {"value": ws / e2e_s, "unit": "steps/s",
+                    "h2d_bytes_per_step": ws * (2 * npts * 3 * 8 + npts * nw * 8 + nw * 8),
+                    "d2h_bytes_per_step": ws * (npts * nw * 8 + 2 * nw * 8 + npts * 8 * 6 + 8),
+                    "note": "host entries: dnnf90_grad_rule_batch, dnnf90_grad_read, "
+                            "dnnf90_jrow_batch (rows to the host), dnnf90_ngd_step (rows back)"},
+            "gpu_launches": launches, "roofline": roof, "clocks": ck.summary(),
+            "cpu_baseline": cpu}), flush=True)
+    rj.free()
+    rp.free()
+    net.free()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def relaunch_cmd(n, argv, port):
+    """The torchrun command that runs this script as n ranks on this node
+    (one per GPU), with the rendezvous on the loopback address."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={n}", "--master-addr=127.0.0.1", f"--master-port={port}",
+            os.path.abspath(__file__)] + list(argv)
+
+
+def relaunch(n):
+    """--gpus n > 1 run directly: start the n ranks under torch.distributed.run
+    and return its status (rank 0 prints the line)."""
+    import socket
+    import subprocess
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    return subprocess.call(relaunch_cmd(n, sys.argv[1:], port))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -502,7 +755,6 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--points", type=int, default=65536, help="points per GPU")
     ap.add_argument("--f64-steps", type=int, default=2)
-    ap.add_argument("--ref-points", type=int, default=24)
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--committee-steps", type=int, default=3,
                     help="timed steps of the 64-network committee (0 skips it)")
@@ -512,10 +764,9 @@ def main():
                          "launches upset the autotuner's timings")
     ap.add_argument("--prof-steps", type=int, default=1,
                     help="steps of the per-kernel event-profiled pass (untimed)")
-    ap.add_argument("--no-kalman", action="store_true",
-                    help="leave the Kalman filter's line out of the default run")
-    ap.add_argument("--workload", default="zk7", choices=["zk7", "kalman"],
-                    help="zk7: the collocation training step (default); kalman: the "
+    ap.add_argument("--workload", default="zk7", choices=["zk7", "ngd", "kalman"],
+                    help="zk7: the collocation training step (default); ngd: the heat "
+                         "configuration's natural-gradient step; kalman: the "
                          "extended Kalman filter's rank-one updates")
     ap.add_argument("--kf-obs", type=int, default=16, help="Kalman updates per step")
     ap.add_argument("--kf-dims", default=None, help="Kalman network widths, e.g. 3,32,32,1")
@@ -524,6 +775,14 @@ def main():
                     help="Kalman update path: -1 by size, 0 two launches per update, "
                          "1 one launch per call")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch(args.gpus)
+    if "WORLD_SIZE" in os.environ and int(os.environ["WORLD_SIZE"]) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={os.environ['WORLD_SIZE']}",
+              file=sys.stderr)
+        return 2
+    if args.workload == "ngd":
+        return ngd_bench(args)
     if args.workload == "kalman":
         if args.kf_dims:
             KF_DIMS[:] = [int(v) for v in args.kf_dims.split(",")]
@@ -766,55 +1025,37 @@ def main():
     if rank == 0 and not args.no_accuracy:
         acc = accuracy(api, ts, w, terms)
     committee = committee_bench(api, dev, args.committee_steps) if args.committee_steps > 0 else None
-    cpu = cpu_baseline(args.ref_points, 1) if (rank == 0 and ws == 1) else None
-    # the Kalman filter's own line (bench.py --workload kalman), measured in a
-    # child process on the same GPU and carried here
-    kalman = None
-    if rank == 0 and ws == 1 and not args.no_kalman:
-        import subprocess
-
-        try:
-            out = subprocess.run([sys.executable, os.path.abspath(__file__), "--workload", "kalman",
-                                  "--steps", "3", "--warmup", "2"],
-                                 capture_output=True, text=True, timeout=600)
-            if out.returncode == 0:
-                d = json.loads(out.stdout.strip().splitlines()[-1])
-                kalman = {k: d.get(k) for k in ("metric", "value", "unit", "ms_per_step", "steps",
-                                                "warmup", "e2e", "roofline", "clocks",
-                                                "cpu_baseline", "gpu_launches", "config")}
-            else:
-                kalman = {"error": out.stderr[-400:]}
-        except Exception as e:  # the headline line is printed whatever happens here
-            kalman = {"error": str(e)[:400]}
+    cpu = cpu_baselines() if (rank == 0 and ws == 1) else None
 
     if rank == 0:
+        def r3(v):
+            return None if v is None else float(f"{v:.4g}")
+
+        cfg = config_of(ws, npts)
+        cfg.update({"hbm_free_gib_at_start": round(hbm_free0, 1),
+                    "launches_per_step": launches / max(args.steps, 1),
+                    "timing": ("one step captured as a CUDA graph, replayed per timed step"
+                               if ws == 1 else "plain calls per step")})
         line = {
             "metric": METRIC, "value": value, "unit": "pts/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "step_ms_each": each[0], "settle_steps": each[1],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "fp32 planes + 3-term split-bf16 GEMMs (fp32 accumulate), fp64 sigma/reductions",
             "data": "synthetic (seeded uniform points, Xavier-normal weights)",
-            "config": {"workload": WORKLOAD, "points_per_gpu": npts, "global_points": ws * npts,
-                       "parallelism": f"dp{ws}: points sharded, dL/dw all-reduced (NCCL)",
-                       "l2": "inputs larger than L2 (126 MB): a work chunk's planes are ~48 GB, so no flush",
-                       "hbm_free_gib_at_start": round(hbm_free0, 1),
-                       "launches_per_step": launches / max(args.steps, 1),
-                       "timing": ("one step captured as a CUDA graph, replayed per timed step"
-                                  if ws == 1 else "plain calls per step")},
-            "f64": {"value": value64, "unit": "pts/s", "ms_per_step": ms64,
-                    "step_ms_each": each64[0], "settle_steps": each64[1], "steps": args.f64_steps, "split_speedup": value / value64,
-                    "kernel_ms_per_step": per_step_ms(prof64)},
-            "kernel_ms_per_step": per_step_ms(prof),
+            # the north-star comparison: split path against the plain FP64
+            # GPU path on the same points, and the split path's error
+            "split_vs_f64": {"speedup": r3(value / value64), "target": 4.0,
+                             "f64_value": r3(value64), "f64_ms_per_step": r3(ms64)},
             "accuracy": acc,
-            "committee": committee,
-            "kalman": kalman,
-            "autotuner": [list(t) for t in api.tune_report()],
+            "config": cfg,
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": roof,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "kernel_ms_per_step": {"split": per_step_ms(prof), "f64": per_step_ms(prof64)},
+            "step_ms_each": each[0], "settle_steps": each[1],
+            "committee": committee,
         }
         print(json.dumps(line), flush=True)
     rule.free()

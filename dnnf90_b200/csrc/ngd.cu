@@ -439,7 +439,11 @@ static __device__ __align__(256) double
 int ngd_noalloc_maxw() { return NGD_NOALLOC_MAXW; }
 
 // Device address of the scratch on the current device, looked up once per
-// device (host code cannot use the array's name as a device address).
+// device (host code cannot use the array's name as a device address) and
+// kept for the life of the process: it does not survive cudaDeviceReset.
+// With lazy module loading (the CUDA 12 default) the array is backed when
+// this file's module first loads on a device, which the lookup itself
+// triggers, so that first call may take the 8 MiB from the device.
 static double *ngd_scratch_ptr() {
   static std::mutex mu;
   static double *ptr[256] = {};
@@ -464,6 +468,18 @@ int ngd_device_noalloc(const double *rows, int nrow, int nw, const double *b, in
     set_error("dnnf90_ngd_step_noalloc: nweights " + std::to_string(nw) +
               " is above the fixed scratch limit of " + std::to_string(NGD_NOALLOC_MAXW));
     return RC_BAD_ARG;
+  }
+  if (!(mu > 0.0)) {
+    set_error("dnnf90_ngd_step_noalloc: the damping mu must be positive");
+    return RC_BAD_ARG;
+  }
+  // the call reads the pivot flag back into host memory and waits for its
+  // stream, neither of which a stream being captured allows
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    set_error("dnnf90_ngd_step_noalloc cannot be captured into a CUDA graph (it waits for "
+              "its stream and reads a status back)");
+    return RC_UNSUPPORTED;
   }
   double *G = ngd_scratch_ptr();
   if (!G) return RC_DEVICE;

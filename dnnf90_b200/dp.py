@@ -106,6 +106,9 @@ def ngd_step_sharded(rows, b, mu: float, nb: int | None = None, route: str = "pr
     ops = ops or DeviceNGD()
     world = dist.get_world_size(group) if dist.is_initialized() else 1
     dev = rows.device
+    # the device entries read rows with stride nw: views are copied first
+    rows = rows.contiguous()
+    b = b.contiguous()
     nloc, nw = rows.shape
     if world > 1:
         cnt = torch.tensor([nloc], dtype=torch.int64, device=dev)

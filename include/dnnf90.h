@@ -43,7 +43,7 @@ int dnnf90_net_create_ts(int tid, int nlayer, const int *dims);
 int dnnf90_net_load(const char *filename);
 /* replaces dnnf90_tabset_activation, lib/c_api_module.f90:480-493.
  * Codes: 0 TANH, 1 SIN, 2 ERF, 3 BESSEL (J_0), 4 BESSEL1 (J_1); the device
- * path evaluates 0, 1 and 2 and answers -5 for 3 and 4. */
+ * path evaluates all five. */
 int dnnf90_tabset_activation(int tid, int iact);
 /* replaces dnnf90_net_load_ts, lib/c_api_module.f90:500-528 */
 int dnnf90_net_load_ts(int tid, const char *filename);

@@ -272,11 +272,17 @@ int dnnf90_committee_info(int *policy, float *graph_ms);
  * arrays).  The call allocates nothing: the nw x nw metric sits in a fixed
  * 8 MiB area inside the library that every GPU loading the library keeps
  * until the process exits, so nw <= 1024; larger nw is refused (-1) with a
- * message in dnnf90_last_error().  The first call on a device looks up the
- * area's device address; make that first call before any stream capture.
- * Every call shares the area: calls that overlap on the GPU (other
- * threads, other streams) race and must be serialised by the caller.  The
- * call synchronises stream (NULL: the legacy default stream). */
+ * message in dnnf90_last_error(); mu <= 0 is refused (-1) as well.  The
+ * first call on a device looks up the area's device address and, under
+ * CUDA's lazy module loading, loads the library's module on that device,
+ * which is when the 8 MiB area is taken from device memory: make one call
+ * before the host pools its device memory.  The address is kept for the
+ * life of the process and does not survive cudaDeviceReset.  Every call
+ * shares the area: calls that overlap on the GPU (other threads, other
+ * streams) race and must be serialised by the caller.  The call waits for
+ * stream (NULL: the legacy default stream) and reads a status back, so it
+ * cannot be captured into a CUDA graph: on a capturing stream it returns -5
+ * without doing anything. */
 int dnnf90_ngd_step_noalloc(int nrow, int nw, const double *rows_dev,
                             const double *b_dev, int nb, double mu,
                             double *u_dev, void *stream);

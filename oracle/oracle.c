@@ -1059,6 +1059,19 @@ void orc_adam_step(int nw, double *w, const double *grad, double *m,
   }
 }
 
+/* The metric build of ngd_apply_inv alone (app/optimizer_module.f90:
+ * 310-321): G(i,j) += jr(ib,i) jr(ib,j) row by row, in the reference's loop
+ * order; G[nw][nw] is overwritten.  The CPU baseline times it. */
+void orc_ngd_metric(int nw, int nrow, const double *rows, double *G) {
+  memset(G, 0, sizeof(double) * (size_t)nw * nw);
+  for (int ib = 0; ib < nrow; ++ib) {
+    const double *r = rows + (size_t)ib * nw;
+    for (int j = 0; j < nw; ++j)
+      for (int i = 0; i < nw; ++i)
+        G[(size_t)j * nw + i] = G[(size_t)j * nw + i] + r[i] * r[j];
+  }
+}
+
 int orc_ngd_step(int nw, int nrow, const double *rows, const double *b,
                  int nb, double mu, double *u) {
   double *G = (double *)calloc((size_t)nw * nw, sizeof(double));

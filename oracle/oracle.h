@@ -190,6 +190,7 @@ void orc_adam_step(int nw, double *w, const double *grad, double *m,
  * pivoting).  The flat layout here is the weight layout above; the
  * reference's flatten order only permutes the unknowns. Returns 0, or -1
  * on a singular pivot. */
+void orc_ngd_metric(int nw, int nrow, const double *rows, double *G);
 int orc_ngd_step(int nw, int nrow, const double *rows, const double *b,
                  int nb, double mu, double *u);
 

@@ -64,6 +64,8 @@ def lib():
         L.orc_grad_sys_batch.argtypes = [vp, ci, P(ci), vp, ci, vp, vp, vp, vp, vp, vp, ci]
         L.orc_adam_step.argtypes = [ci, vp, vp, vp, vp, cd, cd, cd, cd, ci, ci]
         L.orc_ngd_step.argtypes = [ci, ci, vp, vp, ci, cd, vp]
+        L.orc_ngd_metric.argtypes = [ci, ci, vp, vp]
+        L.orc_ngd_metric.restype = None
         _lib = L
     return _lib
 
@@ -339,6 +341,15 @@ def ngd_step(rows, b, nb, mu):
     if rc != 0:
         raise ValueError("oracle ngd: singular metric")
     return u
+
+
+def ngd_metric(rows):
+    """G = J^T J in the reference's loop order (app/optimizer_module.f90:
+    310-321), undivided."""
+    rows = np.ascontiguousarray(rows, np.float64)
+    G = np.zeros((rows.shape[1], rows.shape[1]))
+    lib().orc_ngd_metric(rows.shape[1], rows.shape[0], _p(rows), _p(G))
+    return G
 
 
 def check_weights(dims) -> np.ndarray:

@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Generate tests/golden/golden.json from the reference tree.
 
-Run in a container where the reference is mounted (REF below); the output
+Run with DNNF90_REFERENCE set to the reference source tree; the output
 is committed, so the tests never read the reference at run time.
 
 Contents:
@@ -32,7 +32,10 @@ import subprocess
 import sys
 import tempfile
 
-REF = os.environ.get("DNNF90_REFERENCE", "/root/reference")
+REF = os.environ.get("DNNF90_REFERENCE")
+if not REF:
+    sys.exit("set DNNF90_REFERENCE to the reference source tree (its zwork/ goldens and "
+             "tools/make_hod_golden.py are read from there)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

@@ -10,7 +10,7 @@ from conftest import ROOT
 
 def test_reference_arm_prints_the_contract_line():
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                          "--steps", "1", "--warmup", "1", "--ref-points", "2"],
+                          "--steps", "1", "--warmup", "1"],
                          capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads(out.stdout.strip().splitlines()[-1])
@@ -19,6 +19,36 @@ def test_reference_arm_prints_the_contract_line():
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
     assert "ZK7" in line["config"]["workload"]
+    # every thread carries the same share of the sample
+    assert "32 per thread" in line["cpu_baseline"]["sample"]
+
+
+def test_gpus_flag_relaunches_one_rank_per_gpu():
+    """bench.py --gpus N started without a launcher re-runs itself as N
+    ranks under torch.distributed.run, rendezvous on the loopback address."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    cmd = bench.relaunch_cmd(4, ["--gpus", "4", "--steps", "3"], 29511)
+    assert cmd[1:4] == ["-m", "torch.distributed.run", "--nnodes=1"]
+    assert "--nproc-per-node=4" in cmd and "--master-addr=127.0.0.1" in cmd
+    assert "--master-port=29511" in cmd
+    assert cmd[-5:] == [os.path.join(ROOT, "bench.py"), "--gpus", "4", "--steps", "3"]
+    # a launcher whose world size disagrees with --gpus is refused
+    env = dict(os.environ, WORLD_SIZE="2", RANK="0", LOCAL_RANK="0")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "4"],
+                         capture_output=True, text=True, timeout=300, cwd=ROOT, env=env)
+    assert out.returncode == 2 and "WORLD_SIZE=2" in out.stderr
+
+
+def test_ngd_reference_arm_prints_the_contract_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--workload", "ngd",
+                          "--impl", "reference", "--steps", "1", "--warmup", "1"],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "steps/s" and line["value"] > 0
+    assert "heat" in line["config"]["workload"] and line["cpu_baseline"]["kind"] == "port"
 
 
 def test_kalman_reference_arm_prints_the_contract_line():

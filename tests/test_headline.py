@@ -1,0 +1,136 @@
+"""Parity at the configurations the throughput is quoted on, through the C ABI.
+
+- ZK7 exactly as benchmarked: D0 = 4, K = 7 dense (330 slots), MLP
+  4-128-128-128-1 tanh, residual = the 120 order-7 slots + u u_x, in both
+  precisions: per-order error of the carried derivatives, the weight
+  gradient and the loss against the oracle (the FP64 restatement of
+  lib/train_module.f90:241-450 with app/pinn_module.f90:32-65).
+- The same network over a work space whose chunk holds fewer points than
+  the batch, so that three chunks (the last one ragged) carry the points.
+- Three members of the benchmark's own 64-network uneven committee draw
+  (bench.committee_members), at their full point counts, trained in one
+  committee step (one CUDA graph) and checked member by member.
+
+Tolerances: 1e-12 for the plain FP64 path, 1e-5 for the split path (per
+derivative order, normwise; the reference's convention in
+app/hod_check_module.f90:216,302)."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import per_order_error, rel_err, xavier_weights
+from dnnf90_b200 import api
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOLSPLIT = 1e-5
+ZK7 = [4, 128, 128, 128, 1]
+
+
+def _zk7_terms(ts):
+    terms = [(1.0, i + 1, 0) for i in range(ts.na) if ts.alpha[i].sum() == 7]
+    return terms + [(1.0, ts.slot((0, 1, 0, 0)), 1)]
+
+
+def _zk7_case(npts, seed=20260803):
+    rng = np.random.default_rng(seed)
+    w = xavier_weights(ZK7, 20260801)
+    w[np.arange(len(w)) % 5 == 0] += 0.05          # nonzero biases
+    return w, rng.uniform(-1, 1, (npts, 4))
+
+
+@pytest.fixture(scope="module")
+def zk7_ref():
+    ts = api.TableSet(4, 7)
+    ref = po.Tables(4, 7)
+    terms = _zk7_terms(ts)
+    w, X = _zk7_case(128)
+    gref, Tref, lref, _ = po.grad_batch(ref, ZK7, w, X, kind=po.SEED_PINN, terms=terms)
+    return ts, ref, terms, w, X, gref, Tref, lref
+
+
+@pytest.mark.parametrize("prec", [api.PREC_F64, api.PREC_SPLIT])
+def test_zk7_as_benchmarked(zk7_ref, prec):
+    ts, ref, terms, w, X, gref, Tref, lref = zk7_ref
+    net = api.Net(ts, ZK7, weights=w, precision=prec)
+    g = net.grad()
+    rule = api.SeedRule(api.SEED_PINN, terms)
+    loss, T = g.rule_batch(X, rule, want_t=True)
+    gd = g.read()
+    errs = per_order_error(T, Tref, ref.deg)
+    eg = rel_err(gd, gref)
+    tol = TOL64 if prec == api.PREC_F64 else TOLSPLIT
+    worst = max(errs, key=errs.get)
+    print(f"ZK7 prec={prec}: worst order {worst} err {errs[worst]:.3e}, grad {eg:.3e}, "
+          f"per order {{{', '.join(f'{p}: {e:.2e}' for p, e in errs.items())}}}")
+    assert errs[worst] < tol, errs
+    assert eg < tol, eg
+    assert abs(loss - lref) <= tol * abs(lref), (loss, lref)
+    rule.free()
+    g.free()
+    net.free()
+
+
+@pytest.mark.parametrize("prec", [api.PREC_F64, api.PREC_SPLIT])
+def test_zk7_over_three_chunks(zk7_ref, prec):
+    """48 + 48 + 32 points: the work space carries the batch in chunks and
+    the gradient, loss and derivatives are the one-chunk results."""
+    ts, ref, terms, w, X, gref, Tref, lref = zk7_ref
+    net = api.Net(ts, ZK7, weights=w, precision=prec)
+    api.call("dnnf90_twork_set_chunk", net.tid, 48)
+    g = net.grad()
+    rule = api.SeedRule(api.SEED_PINN, terms)
+    loss, T = g.rule_batch(X, rule, want_t=True)
+    gd = g.read()
+    tol = TOL64 if prec == api.PREC_F64 else TOLSPLIT
+    assert max(per_order_error(T, Tref, ref.deg).values()) < tol
+    assert rel_err(gd, gref) < tol
+    assert abs(loss - lref) <= tol * abs(lref)
+    # the same network in one chunk gives the same sums up to the order of
+    # the chunk additions (FP64 atomics of the gradient)
+    net1 = api.Net(ts, ZK7, weights=w, precision=prec)
+    g1 = net1.grad()
+    loss1, T1 = g1.rule_batch(X, rule, want_t=True)
+    assert rel_err(T, T1) < 1e-13
+    assert rel_err(gd, g1.read()) < 1e-12
+    assert abs(loss - loss1) <= 1e-12 * abs(loss1)
+    rule.free()
+    for o in (g, g1, net, net1):
+        o.free()
+
+
+# members 1, 2 and 9 of the draw: a width-256 net of four hidden layers at
+# K = 4, a K = 7 net of four hidden layers, and a D0 = 3 width-256 net
+DRAW_MEMBERS = (1, 2, 9)
+
+
+def test_committee_draw_members_match_the_oracle():
+    import torch
+
+    import bench
+
+    draw = bench.committee_members(64)
+    dev = torch.device("cuda", 0)
+    rule = api.SeedRule(api.SEED_HALFSQ)
+    nets, xs, cases = [], [], []
+    for i in DRAW_MEMBERS:
+        d0, k, width, depth, X, wseed = draw[i]
+        dims = [d0] + [width] * depth + [1]
+        w = bench.xavier(dims, wseed)
+        nets.append(api.Net(api.TableSet(d0, k), dims, weights=w, precision=api.PREC_SPLIT))
+        xs.append(torch.tensor(X, device=dev))
+        cases.append((d0, k, dims, w, X))
+    grads = [torch.full((m.nw,), float("nan"), dtype=torch.float64, device=dev) for m in nets]
+    loss = torch.full((len(nets),), float("nan"), dtype=torch.float64, device=dev)
+    api.committee_step(nets, [rule] * len(nets), xs, grads, loss)
+    for j, (d0, k, dims, w, X) in enumerate(cases):
+        gref, _, lref, _ = po.grad_batch(po.Tables(d0, k), dims, w, X, kind=po.SEED_HALFSQ,
+                                         want_t=False)
+        e = rel_err(grads[j].cpu().numpy(), gref)
+        print(f"draw member {DRAW_MEMBERS[j]} {dims} K={k} {X.shape[0]} pts: grad err {e:.2e}")
+        assert e < TOLSPLIT, (DRAW_MEMBERS[j], e)
+        assert abs(float(loss[j]) - lref) <= TOLSPLIT * abs(lref)
+    for m in nets:
+        m.free()
+    rule.free()
