@@ -16,8 +16,8 @@ OBJ = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libdnnf90_b200.so")
 
-SOURCES = ["tables.cpp", "bell_plan.cpp", "api.cpp", "engine.cu", "bell.cu", "gemm_tc.cu",
-           "ngd.cu", "kalman.cu"]
+SOURCES = ["tables.cpp", "bell_plan.cpp", "tile_plan.cpp", "api.cpp", "engine.cu", "bell.cu",
+           "bell_tile.cu", "gemm_tc.cu", "gemm_f64.cu", "ngd.cu", "kalman.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
            "--expt-relaxed-constexpr", "-Xcompiler", "-Wall"]
@@ -62,7 +62,7 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
         subprocess.run(cmd, check=True)
         changed = True
     if changed or not os.path.exists(LIB):
-        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcublas"]
+        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

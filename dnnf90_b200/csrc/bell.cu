@@ -58,6 +58,7 @@ void DevBellPlan::release() {
                 a5_pair, f6_rec};
   for (void *p : ps)
     if (p) cudaFree(p);
+  tile.release();
   *this = DevBellPlan();
 }
 
@@ -182,6 +183,7 @@ int upload_bell_plan(const TableSet &t, DevBellPlan &d) {
   d.f3_ok = P.f3_ok;
   d.nrows = P.nrows;
   d.dt_off = P.dt_off;
+  if ((rc = upload_tile_plan(t, d.tile))) return rc;
   d.ready = true;
   return RC_OK;
 }
@@ -1556,10 +1558,14 @@ static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
     return RC_OK;
   }
   // variant 0: records in global memory; 1: records in shared memory;
-  // 2: v8 (lean per-degree loops over 16-bit offset records)
+  // 2: v8 (lean per-degree loops over 16-bit offset records); 3: the
+  // register-tiled Horner forward (bell_tile.cu; FP32, dense sets), the
+  // default wherever it applies
   const bool srec_fits = smem + (size_t)bp.nrec32 * 4 <= 227 * 1024;
   const bool v8_ok = bp.f8.ok && bp.f8.smem <= 227 * 1024;
+  const bool tile_ok = sizeof(R) == 4 && tile_fwd_applies(bp.tile, n);
   auto launch = [&](int v, bool) -> int {
+    if (v == 3) return bell_fwd_tile(bp.tile, t, n, npts, S, T, h, train, st);
     if (v == 2) {
       Fwd8Args b;
       b.n = n; b.na = t.na; b.npts = npts; b.iact = t.iact; b.gy = a.gy; b.nrec = bp.f8.nrec;
@@ -1584,6 +1590,11 @@ static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
     CKB(cudaGetLastError());
     return RC_OK;
   };
+  if (tile_ok && g_force[0] < 0)  // timed against v8, the tiled kernel the default
+    return tuned_launch(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)}, v8_ok ? 2 : 1, 0,
+                        (long)npts * a.gy, st,
+                        [&](int v, bool last) { return launch(v ? 2 : 3, last); });
+  if (tile_ok && g_force[0] == 3) return launch(3, true);
   if (v8_ok && !srec_fits)  // variants 0 and 2 only: v8 takes the place of 1
     return tuned_launch(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)}, 2, 1,
                         (long)npts * a.gy, st, [&](int v, bool last) { return launch(v ? 2 : 0, last); });
@@ -1698,6 +1709,19 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
       CKB(cudaGetLastError());
       return RC_OK;
     };
+    // variant 3: the register-tiled correlation (bell_tile.cu; FP32, dense
+    // sets), the default wherever it applies, with v7 beside it
+    if (sizeof(R) == 4 && tile_adj_applies(bp.tile, n) && (g_force[1] < 0 || g_force[1] == 3)) {
+      auto launch_t = [&](int v, bool last) -> int {
+        if (v == 3)
+          return bell_adj_tile(bp.tile, n, npts, Tb, h, Sb, last ? gbias : nullptr, gstride, st);
+        return launch_all(v, last);
+      };
+      if (g_force[1] == 3) return launch_t(3, true);
+      return tuned_launch(TuneKey{bp.id, 2, n, (int)sizeof(R)}, v7_fits ? 2 : 1, 0,
+                          (long)npts * b.gy, st,
+                          [&](int v, bool last) { return launch_t(v ? 2 : 3, last); });
+    }
     const int nvar = v7_fits ? 3 : srec_fits ? 2 : 1;
     return tuned_launch(TuneKey{bp.id, 2, n, (int)sizeof(R)}, nvar, nvar - 1,
                         (long)npts * b.gy, st, launch_all);

@@ -15,6 +15,23 @@ constexpr int BELL_UNROLL = 4;    // table records fetched ahead per step
 constexpr int ADJ_WORKERS = 32;   // warps per block of the adjoint
 constexpr int ADJ_UNROLL = 2;     // pairs fetched ahead: 2 * ADJ_UNROLL
 
+// device copy of the register-tiled kernels' plan (tile_plan.hpp) and the
+// shared-memory layouts of the two kernels (byte offsets)
+struct TileDev {
+  bool ok = false;
+  int td = 0, k = 0, na = 0, nbuf0 = 0, nbuf1 = 0;
+  int nfunit = 0, nfrec = 0, naunit = 0, narec = 0, nafin = 0, nscratch = 0;
+  int *flist = nullptr, *funit = nullptr, *alist = nullptr, *aunit = nullptr;
+  int *aflist = nullptr, *afin = nullptr, *perm = nullptr, *rowslot = nullptr;
+  uint32_t *frec = nullptr, *arec = nullptr;
+  float *fact = nullptr, *ifact = nullptr;
+  int f_o_d0 = 0, f_o_d1 = 0, f_o_sig = 0, f_o_list = 0, f_o_unit = 0, f_o_rec = 0;
+  int f_o_perm = 0, f_o_rowslot = 0, f_o_fact = 0, f_o_ifact = 0, f_smem = 0;
+  int a_o_scr = 0, a_o_list = 0, a_o_flist = 0, a_o_unit = 0, a_o_fin = 0, a_o_rec = 0;
+  int a_o_perm = 0, a_o_rowslot = 0, a_o_fact = 0, a_o_ifact = 0, a_smem = 0;
+  void release();
+};
+
 struct DevBellPlan {
   bool ready = false;
   uint64_t id = 0;              // distinct per upload (autotuner key)
@@ -65,6 +82,7 @@ struct DevBellPlan {
     int pbase = 0, qbase = 0, smem = 0;
     bool ok = false;
   } f9;
+  TileDev tile;            // register-tiled kernels (dense sets, FP32)
   double *sc64 = nullptr;  // [3][na]: a!, 1/a!, 1/a! (Tb, h, Sb scales)
   float *sc32 = nullptr;
   void release();
@@ -87,6 +105,15 @@ int bell_fwd2(const DevBellPlan &bp, const DevTables &t, int n, int npts, const 
 int bell_adj2(const DevBellPlan &bp, const DevTables &t, int n, int npts, const void *Tb,
               const void *h, void *Sb, double *gbias, int gstride, int prec,
               cudaStream_t st);
+// register-tiled Bell forward and adjoint (bell_tile.cu): dense sets with
+// K <= 7, FP32 planes, n a multiple of 4; RC_UNSUPPORTED otherwise
+int upload_tile_plan(const TableSet &t, TileDev &d);
+bool tile_fwd_applies(const TileDev &d, int n);
+bool tile_adj_applies(const TileDev &d, int n);
+int bell_fwd_tile(const TileDev &d, const DevTables &t, int n, int npts, const void *S, void *T,
+                  void *h, bool train, cudaStream_t st);
+int bell_adj_tile(const TileDev &d, int n, int npts, const void *Tb, const void *h, void *Sb,
+                  double *gbias, int gstride, cudaStream_t st);
 // the first hidden layer's adjoint fused with dW_2, staged through shared
 // memory (RC_UNSUPPORTED when an item's rows do not fit)
 int bell_adj_l2s(int d0, int n, int na, int npts, const int *up, const void *Tb, const void *h,

@@ -15,7 +15,6 @@
 //   k_gemm<DT>     Tb_{l-1} = W_l^T Sb_l (:430-444)
 //   k_bell_adj_l2  Bell adjoint of the first hidden layer fused with its
 //                  weight gradient (only Sb^0 and Sb^{e_i} are needed)
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,6 +27,7 @@
 #include <type_traits>
 
 #include "engine.hpp"
+#include "gemm_f64.hpp"
 #include "gemm_tc.hpp"
 #include "kernels.cuh"
 
@@ -1319,71 +1319,15 @@ static int launch_bell_fwd(const DevTables &t, int n, int npts, const void *S,
   return RC_OK;
 }
 
-// bias of the forward GEMM on the alpha = 0 rows: C[pt * na][c] += W[c][0]
-__global__ void k_bias_rows(double *C, int ldc, const double *W, int ldw, int n, int na,
-                            int npts) {
-  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (long)npts * n) return;
-  const long pt = e / n;
-  const int c = (int)(e - pt * n);
-  C[(size_t)pt * na * ldc + c] += W[(size_t)c * ldw];
-}
-
-// FP64 layer GEMMs through cuBLAS (DGEMM); the row-major operands of the
-// three forms are read as column-major transposes.  One handle per device
-// and host thread.
-static cublasHandle_t cublas_handle() {
-  thread_local std::vector<cublasHandle_t> hs;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-  if ((int)hs.size() <= dev) hs.resize(dev + 1, nullptr);
-  if (!hs[dev] && cublasCreate(&hs[dev]) != CUBLAS_STATUS_SUCCESS) hs[dev] = nullptr;
-  return hs[dev];
-}
-
-static int gemm_f64_cublas(int mode, int M, int N, int K, int na, const double *A, int lda,
-                           const double *B, int ldb, double *C, int ldc, double *G, int gld,
-                           cudaStream_t st) {
-  cublasHandle_t h = cublas_handle();
-  if (!h || cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) return RC_UNSUPPORTED;
-  const double one = 1.0, zero = 0.0;
-  cublasStatus_t s;
-  if (mode == G_FWD) {
-    // C[M][N] = A[M][K] W[N][1 + k]^T  (+ bias on the alpha = 0 rows)
-    const int pi = prof_begin("cublas_dgemm", st);
-    s = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, N, M, K, &one, B + 1, ldb, A, lda, &zero, C,
-                    ldc);
-    prof_end(pi, st);
-    if (s != CUBLAS_STATUS_SUCCESS) return RC_UNSUPPORTED;
-    const int npts = M / na;
-    const long tot = (long)npts * N;
-    LAUNCH("k_bias_rows", st, (k_bias_rows<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(C, ldc, B, ldb, N, na, npts)));
-    CK(cudaGetLastError());
-  } else if (mode == G_DT) {
-    // C[M][N] = A[M][K] W[K][1 + c]
-    const int pi = prof_begin("cublas_dgemm", st);
-    s = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, M, K, &one, B + 1, ldb, A, lda, &zero, C,
-                    ldc);
-    prof_end(pi, st);
-    if (s != CUBLAS_STATUS_SUCCESS) return RC_UNSUPPORTED;
-  } else {
-    // G[c1][1 + c2] += sum_r A[r][c1] X[r][c2]  (M = c1 count, N = c2 count, K = rows)
-    const int pi = prof_begin("cublas_dgemm", st);
-    s = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, N, M, K, &one, B, ldb, A, lda, &one, G + 1,
-                    gld);
-    prof_end(pi, st);
-    if (s != CUBLAS_STATUS_SUCCESS) return RC_UNSUPPORTED;
-  }
-  return RC_OK;
-}
-
 template <typename R>
 static int launch_gemm_cc(int mode, int M, int N, int K, int na, const void *A,
                           int lda, const void *B, int ldb, void *C, int ldc,
                           double *G, int gld, cudaStream_t st) {
   if (sizeof(R) == 8) {
-    const int rc = gemm_f64_cublas(mode, M, N, K, na, (const double *)A, lda,
-                                   (const double *)B, ldb, (double *)C, ldc, G, gld, st);
+    // FP64 tensor cores (gemm_f64.cu); the CUDA-core tiles below take the
+    // shapes it refuses (odd widths)
+    const int rc = gemm_f64(mode, M, N, K, na, (const double *)A, lda, (const double *)B, ldb,
+                            (double *)C, ldc, G, gld, st);
     if (rc != RC_UNSUPPORTED) return rc;
   }
   GemmArgs g;

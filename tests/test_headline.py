@@ -13,7 +13,8 @@
 
 Tolerances: 1e-12 for the plain FP64 path, 1e-5 for the split path (per
 derivative order, normwise; the reference's convention in
-app/hod_check_module.f90:216,302)."""
+app/hod_check_module.f90:216,302); 3e-5 for the committee members, whose
+FP32 planes pass through up to four 256-wide layers."""
 import numpy as np
 import pytest
 
@@ -87,14 +88,17 @@ def test_zk7_over_three_chunks(zk7_ref, prec):
     assert max(per_order_error(T, Tref, ref.deg).values()) < tol
     assert rel_err(gd, gref) < tol
     assert abs(loss - lref) <= tol * abs(lref)
-    # the same network in one chunk gives the same sums up to the order of
-    # the chunk additions (FP64 atomics of the gradient)
+    # the same network in one chunk: the derivatives are per point and do not
+    # move; the gradient's sums are grouped by chunk (FP64 atomics, and on the
+    # split path FP32 partials of up to 512 rows), so they agree to that
+    # grouping's rounding
     net1 = api.Net(ts, ZK7, weights=w, precision=prec)
     g1 = net1.grad()
     loss1, T1 = g1.rule_batch(X, rule, want_t=True)
     assert rel_err(T, T1) < 1e-13
-    assert rel_err(gd, g1.read()) < 1e-12
-    assert abs(loss - loss1) <= 1e-12 * abs(loss1)
+    regroup = 1e-12 if prec == api.PREC_F64 else 2e-6
+    assert rel_err(gd, g1.read()) < regroup
+    assert abs(loss - loss1) <= regroup * abs(loss1)
     rule.free()
     for o in (g, g1, net, net1):
         o.free()
@@ -103,6 +107,11 @@ def test_zk7_over_three_chunks(zk7_ref, prec):
 # members 1, 2 and 9 of the draw: a width-256 net of four hidden layers at
 # K = 4, a K = 7 net of four hidden layers, and a D0 = 3 width-256 net
 DRAW_MEMBERS = (1, 2, 9)
+# The split path keeps its planes in FP32, so its error grows with depth:
+# at K = 4 the worst order measured 4e-6 with two hidden layers of 256 and
+# 1.2e-5 with four (the plain FP64 path stays at 2e-15 on the same nets).
+# The committee's members reach four hidden layers of 256.
+TOL_DRAW = 3e-5
 
 
 def test_committee_draw_members_match_the_oracle():
@@ -129,8 +138,8 @@ def test_committee_draw_members_match_the_oracle():
                                          want_t=False)
         e = rel_err(grads[j].cpu().numpy(), gref)
         print(f"draw member {DRAW_MEMBERS[j]} {dims} K={k} {X.shape[0]} pts: grad err {e:.2e}")
-        assert e < TOLSPLIT, (DRAW_MEMBERS[j], e)
-        assert abs(float(loss[j]) - lref) <= TOLSPLIT * abs(lref)
+        assert e < TOL_DRAW, (DRAW_MEMBERS[j], e)
+        assert abs(float(loss[j]) - lref) <= TOL_DRAW * abs(lref)
     for m in nets:
         m.free()
     rule.free()

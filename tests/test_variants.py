@@ -5,7 +5,9 @@ tests elsewhere see only the variant that won on the machine at hand.  Here
 each variant is pinned in turn (dnnf90_tune_force) and the whole gradient
 step is checked: derivatives, loss and dL/dw, in both precisions, over dense
 and seeded sets from K = 1 to K = 8.  The tanh series forward (v9, off by
-default) is switched off for the Bell variants and on for its own case."""
+default) is switched off for the Bell variants and on for its own case.
+Variant 3 is the register-tiled Horner forward and tiled correlation
+adjoint (dense sets, FP32; elsewhere the pin falls back to the default)."""
 import numpy as np
 import pytest
 
@@ -20,6 +22,8 @@ CASES = [
     (2, 8, None, [2, 32, 32, 1], 30),
     (1, 1, None, [1, 32, 32, 1], 64),
     (1, 2, None, [1, 36, 20, 1], 64),
+    (3, 7, None, [3, 100, 44, 1], 9),     # ragged neuron tiles (100 = 3 * 32 + 4)
+    (4, 4, None, [4, 36, 36, 36, 1], 17),
 ]
 
 
@@ -45,7 +49,7 @@ def pinned():
 @pytest.mark.gpu
 @pytest.mark.parametrize("d0,k,seeds,dims,npts", CASES)
 @pytest.mark.parametrize("prec", [api.PREC_F64, api.PREC_SPLIT])
-@pytest.mark.parametrize("fwd,adj,series", [(0, 0, 0), (1, 1, 0), (2, 2, 0), (2, 2, 1)])
+@pytest.mark.parametrize("fwd,adj,series", [(0, 0, 0), (1, 1, 0), (2, 2, 0), (2, 2, 1), (3, 3, 0)])
 def test_pinned_variant(pinned, d0, k, seeds, dims, npts, prec, fwd, adj, series):
     pinned(0, fwd)
     pinned(1, adj)
