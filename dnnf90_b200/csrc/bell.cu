@@ -1438,6 +1438,7 @@ struct TuneKey {
 };
 static std::map<TuneKey, int> g_tune;
 static std::map<TuneKey, std::vector<float>> g_tune_ms;  // timed trial per variant
+static std::map<TuneKey, std::vector<int>> g_tune_id;   // variant ids of the trials
 static std::mutex g_tune_mu;
 
 // "kernel width prec chosen ms0 ms1 ..." lines, one per tuned launch shape
@@ -1447,8 +1448,12 @@ std::string tune_report() {
   std::string out;
   char b[64];
   for (auto &kv : g_tune) {
+    auto ids = g_tune_id.find(kv.first);
+    const int chosen = ids != g_tune_id.end() && kv.second < (int)ids->second.size()
+                           ? ids->second[kv.second]
+                           : kv.second;
     std::snprintf(b, sizeof b, "%s %d %s %d", names[kv.first.which], kv.first.n,
-                  kv.first.prec == 8 ? "f64" : "f32", kv.second);
+                  kv.first.prec == 8 ? "f64" : "f32", chosen);
     out += b;
     auto it = g_tune_ms.find(kv.first);
     if (it != g_tune_ms.end())
@@ -1527,6 +1532,29 @@ static int tuned_launch(const TuneKey &key, int nvar, int dflt, long items, cuda
   return RC_OK;  // every variant wrote the same values
 }
 
+// tuned_launch over a list of variant ids (launch(id, last)); a pinned
+// variant runs if it applies, else the default; the record keeps the ids
+template <typename L>
+static int tuned_ids(const TuneKey &key, const std::vector<int> &ids, int dflt, long items,
+                     cudaStream_t st, L launch) {
+  const int f = g_force[key.which == 2 ? 1 : 0];
+  if (f >= 0) {
+    for (int id : ids)
+      if (id == f) return launch(f, true);
+    return launch(ids[dflt], true);
+  }
+  const int rc = tuned_launch(key, (int)ids.size(), dflt, items, st,
+                              [&](int i, bool last) { return launch(ids[i], last); });
+  if (rc == RC_OK) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end() && it->second < (int)ids.size() && g_tune_id.count(key) == 0) {
+      g_tune_id[key] = ids;
+    }
+  }
+  return rc;
+}
+
 template <typename R, int KK>
 static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int npts,
                          const void *S, void *T, void *h, bool train, cudaStream_t st) {
@@ -1590,17 +1618,15 @@ static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
     CKB(cudaGetLastError());
     return RC_OK;
   };
-  if (tile_ok && g_force[0] < 0)  // timed against v8, the tiled kernel the default
-    return tuned_launch(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)}, v8_ok ? 2 : 1, 0,
-                        (long)npts * a.gy, st,
-                        [&](int v, bool last) { return launch(v ? 2 : 3, last); });
-  if (tile_ok && g_force[0] == 3) return launch(3, true);
-  if (v8_ok && !srec_fits)  // variants 0 and 2 only: v8 takes the place of 1
-    return tuned_launch(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)}, 2, 1,
-                        (long)npts * a.gy, st, [&](int v, bool last) { return launch(v ? 2 : 0, last); });
-  return tuned_launch(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)},
-                      v8_ok ? 3 : srec_fits ? 2 : 1, v8_ok ? 2 : srec_fits ? 1 : 0,
-                      (long)npts * a.gy, st, launch);
+  // every variant that applies is timed; the default (the choice under
+  // graph capture, and for launches too small to time) is the tiled
+  // kernel, else v8, else v5
+  std::vector<int> ids{0};
+  if (srec_fits) ids.push_back(1);
+  if (v8_ok) ids.push_back(2);
+  if (tile_ok) ids.push_back(3);
+  return tuned_ids(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)}, ids, (int)ids.size() - 1,
+                   (long)npts * a.gy, st, launch);
 }
 
 template <typename R, int KK>
@@ -1710,21 +1736,21 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
       return RC_OK;
     };
     // variant 3: the register-tiled correlation (bell_tile.cu; FP32, dense
-    // sets), the default wherever it applies, with v7 beside it
-    if (sizeof(R) == 4 && tile_adj_applies(bp.tile, n) && (g_force[1] < 0 || g_force[1] == 3)) {
-      auto launch_t = [&](int v, bool last) -> int {
-        if (v == 3)
-          return bell_adj_tile(bp.tile, n, npts, Tb, h, Sb, last ? gbias : nullptr, gstride, st);
-        return launch_all(v, last);
-      };
-      if (g_force[1] == 3) return launch_t(3, true);
-      return tuned_launch(TuneKey{bp.id, 2, n, (int)sizeof(R)}, v7_fits ? 2 : 1, 0,
-                          (long)npts * b.gy, st,
-                          [&](int v, bool last) { return launch_t(v ? 2 : 3, last); });
-    }
-    const int nvar = v7_fits ? 3 : srec_fits ? 2 : 1;
-    return tuned_launch(TuneKey{bp.id, 2, n, (int)sizeof(R)}, nvar, nvar - 1,
-                        (long)npts * b.gy, st, launch_all);
+    // sets).  Every variant that applies is timed; the default is v7 (the
+    // faster at the headline sizes), else the last that applies
+    auto launch_t = [&](int v, bool last) -> int {
+      if (v == 3)
+        return bell_adj_tile(bp.tile, n, npts, Tb, h, Sb, last ? gbias : nullptr, gstride, st);
+      return launch_all(v, last);
+    };
+    std::vector<int> ids{0};
+    if (srec_fits) ids.push_back(1);
+    if (v7_fits) ids.push_back(2);
+    if (sizeof(R) == 4 && tile_adj_applies(bp.tile, n)) ids.push_back(3);
+    int dflt = (int)ids.size() - 1;
+    if (v7_fits) dflt = srec_fits ? 2 : 1;
+    return tuned_ids(TuneKey{bp.id, 2, n, (int)sizeof(R)}, ids, dflt, (long)npts * b.gy, st,
+                     launch_t);
   }
   Adj2Args a;
   a.n = n; a.na = t.na; a.npts = npts; a.gstride = gstride; a.list = bp.aj_list;

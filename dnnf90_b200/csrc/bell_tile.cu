@@ -248,8 +248,18 @@ __global__ void __launch_bounds__(TWF * 32, 1) k_bell_fwd10(Fwd10Args a) {
                  (int)((it + 1) / a.npts) * 32);
     cp_commit();
     float *Sb = (float *)(sm + (buf ? a.o_s1 : 0)) + lane;
-    // S_a -> S_a / a! (the origin row keeps S_0: 0! = 1)
-    for (int r = warp; r < na; r += TWF) Sb[r * 32] *= sifact[r];
+    // S_a -> S_a / a!, 16 bytes per thread at a time; the origin row keeps
+    // S_0 (0! = 1) and is left alone, since warp 0 reads it next
+    {
+      unsigned char *sb0 = sm + (buf ? a.o_s1 : 0);
+      for (int c = threadIdx.x + 8; c < na * 8; c += blockDim.x) {
+        float4 *p = (float4 *)(sb0 + c * 16);
+        const float f = sifact[c >> 3];
+        float4 v = *p;
+        v.x *= f; v.y *= f; v.z *= f; v.w *= f;
+        *p = v;
+      }
+    }
     if (warp == 0) {
       double d[TILE_KMAX + 2];
       sigma_derivs(a.iact, a.tpc, K, (double)Sb[0], d);
@@ -363,27 +373,26 @@ __device__ __forceinline__ void tile_adj(const float *tb, const float *hh,
   AdjRows<TD, 0, NT>::run(tb, hv, acc);
 }
 
-// one run of records of tile side L from record i on; small tiles four
-// records at a time, so that their shared loads are in flight together
-template <int TD, int LO, int L>
-__device__ __forceinline__ void adj_run(const float *tbb, const float *hb, const uint32_t *rec,
-                                        int &i, int end, float (&acc)[tsize(TD, LO)]) {
-  if constexpr (tsize(TD, L) <= 10) {
-    while (i + 4 <= end && (rec[i + 3] >> 28) == (uint32_t)L) {
-      const uint32_t r0 = rec[i], r1 = rec[i + 1], r2 = rec[i + 2], r3 = rec[i + 3];
-      tile_adj<TD, LO, L>(tbb + ((r0 >> 14) & 0x3fffu) * 32, hb + (r0 & 0x3fffu) * 32, acc);
-      tile_adj<TD, LO, L>(tbb + ((r1 >> 14) & 0x3fffu) * 32, hb + (r1 & 0x3fffu) * 32, acc);
-      tile_adj<TD, LO, L>(tbb + ((r2 >> 14) & 0x3fffu) * 32, hb + (r2 & 0x3fffu) * 32, acc);
-      tile_adj<TD, LO, L>(tbb + ((r3 >> 14) & 0x3fffu) * 32, hb + (r3 & 0x3fffu) * 32, acc);
-      i += 4;
+// a unit's records, E = 0 .. LO-1 in turn: (cw >> 4E) & 15 records of tile
+// side LO - E each, so that no record is dispatched at run time
+template <int TD, int LO, int E>
+struct AdjE {
+  static __device__ __forceinline__ void run(const float *tbb, const float *hb,
+                                             const uint32_t *rec, int i, uint32_t cw,
+                                             float (&acc)[tsize(TD, LO)]) {
+    const int cnt = (cw >> (4 * E)) & 15u;
+    for (int k = 0; k < cnt; ++k) {
+      const uint32_t r = rec[i + k];
+      tile_adj<TD, LO, LO - E>(tbb + ((r >> 14) & 0x3fffu) * 32, hb + (r & 0x3fffu) * 32, acc);
     }
+    AdjE<TD, LO, E + 1>::run(tbb, hb, rec, i + cnt, cw, acc);
   }
-  while (i < end && (rec[i] >> 28) == (uint32_t)L) {
-    const uint32_t r = rec[i];
-    tile_adj<TD, LO, L>(tbb + ((r >> 14) & 0x3fffu) * 32, hb + (r & 0x3fffu) * 32, acc);
-    ++i;
-  }
-}
+};
+template <int TD, int LO>
+struct AdjE<TD, LO, LO> {
+  static __device__ __forceinline__ void run(const float *, const float *, const uint32_t *, int,
+                                             uint32_t, float (&)[tsize(TD, LO)]) {}
+};
 
 // tbb, hb: this lane's word of the current buffer's Tb rows and h rows
 template <int TD, int LO>
@@ -395,21 +404,7 @@ __device__ __forceinline__ void adj_unit(const float *tbb, const float *hb, cons
   float acc[NT];
 #pragma unroll
   for (int e = 0; e < NT; ++e) acc[e] = 0.f;
-  // the records of a unit come in runs of one tile side (descending)
-  int i = u.y;
-  const int end = u.y + u.z;
-  while (i < end) {
-    switch (rec[i] >> 28) {
-#define A10(LL)                                                             \
-  case LL:                                                                  \
-    if constexpr (LL <= LO) adj_run<TD, LO, LL>(tbb, hb, rec, i, end, acc); \
-    else i = end;                                                           \
-    break;
-      A10(1) A10(2) A10(3) A10(4) A10(5) A10(6) A10(7) A10(8)
-#undef A10
-      default: i = end; break;
-    }
-  }
+  AdjE<TD, LO, 0>::run(tbb, hb, rec, u.y, (uint32_t)u.z, acc);
   if (u.x >> 8) {  // one part of a split output tile: into its scratch rows
 #pragma unroll
     for (int e = 0; e < NT; ++e) scr[(u.w + e) * 32] = acc[e];
@@ -484,9 +479,16 @@ __global__ void __launch_bounds__(TWA * 32, 1) k_bell_adj10(Adj10Args a) {
     cp_commit();
     // Tb_a -> a! Tb_a, h_g -> h_g / g!
     float *rb = (float *)(sm + buf * a.o_b1) + lane;
-    for (int r = warp; r < 2 * na; r += TWA) {
-      const int rr = r < na ? r : r - na;
-      rb[r * 32] *= r < na ? sfact[rr] : sifact[rr];
+    {
+      unsigned char *b0 = sm + buf * a.o_b1;  // 16 bytes per thread at a time
+      for (int c = threadIdx.x; c < 2 * na * 8; c += blockDim.x) {
+        const int r = c >> 3;
+        const float f = r < na ? sfact[r] : sifact[r - na];
+        float4 *p = (float4 *)(b0 + c * 16);
+        float4 v = *p;
+        v.x *= f; v.y *= f; v.z *= f; v.w *= f;
+        *p = v;
+      }
     }
     __syncthreads();
     float *Sb = a.Sb + pt * plane + j;

@@ -157,31 +157,38 @@ __global__ void __launch_bounds__(NTH) k_gemm_f64(F64Args g) {
   const int n0 = blockIdx.y * BN;
   const int r8 = lane >> 2, c2 = (lane & 3) * 2;
   if (MODE != MODE_F64_DW) {
+    // this block's M tiles blockIdx.x, + gridDim.x, ...; one cp.async ring
+    // runs through all their k-blocks, so no tile waits for its ring to fill
     const int tiles = (g.M + BM - 1) / BM;
     const int nkb = (g.K + BK - 1) / BK;
-    for (int tm = blockIdx.x; tm < tiles; tm += gridDim.x) {
-      const int m0 = tm * BM;
-      double acc[4][4][2];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-      __syncthreads();  // the last tile's stages are free
-#pragma unroll
-      for (int s = 0; s < NST - 1; ++s) {
-        if (s < nkb) load_stage<MODE>(g, sm + s * STAGE_WORDS, m0, n0, s * BK, g.K);
-        commit();
+    const int mine = blockIdx.x < tiles ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int total = mine * nkb;
+    auto issue = [&](int s) {
+      if (s < total) {
+        const int t = s / nkb, kb = s - t * nkb;
+        load_stage<MODE>(g, sm + (s % NST) * STAGE_WORDS, (blockIdx.x + t * gridDim.x) * BM, n0,
+                         kb * BK, g.K);
       }
-      for (int kb = 0; kb < nkb; ++kb) {
-        wait_group<NST - 2>();
-        __syncthreads();
-        const int nx = kb + NST - 1;
-        if (nx < nkb) load_stage<MODE>(g, sm + (nx % NST) * STAGE_WORDS, m0, n0, nx * BK, g.K);
-        commit();
-        compute_stage<MODE>(sm + (kb % NST) * STAGE_WORDS, wm, wn, lane, acc);
+      commit();
+    };
+#pragma unroll
+    for (int s = 0; s < NST - 1; ++s) issue(s);
+    double acc[4][4][2];
+    for (int s = 0; s < total; ++s) {
+      wait_group<NST - 2>();
+      __syncthreads();  // stage s is in; every warp is done with stage s - 1
+      issue(s + NST - 1);
+      const int t = s / nkb, kb = s - t * nkb;
+      if (kb == 0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
       }
-      wait_group<0>();
+      compute_stage<MODE>(sm + (s % NST) * STAGE_WORDS, wm, wn, lane, acc);
+      if (kb != nkb - 1) continue;
       // epilogue: rows m0 + wm + i*8 + r8, columns n0 + wn + j*8 + c2 (+0, +1)
+      const int m0 = (blockIdx.x + t * gridDim.x) * BM;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int m = m0 + wm + i * 8 + r8;
@@ -205,6 +212,7 @@ __global__ void __launch_bounds__(NTH) k_gemm_f64(F64Args g) {
         }
       }
     }
+    wait_group<0>();
   } else {
     // rows [r0, r1) of the reduction for output tile (blockIdx.z, blockIdx.y)
     const int m0 = blockIdx.z * BM;

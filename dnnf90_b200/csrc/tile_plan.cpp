@@ -223,7 +223,7 @@ TilePlan build_tile_plan(const TableSet &t, int fwarps, int awarps) {
       const int L = K - gd - deg_of(eps) + 1;
       const int hrow = P.tbase[o2], tbrow = P.tbase[oidx.at(sum)];
       a.rec.push_back((uint32_t)hrow | (uint32_t)tbrow << 14 | (uint32_t)L << 28);
-      const long c = tile_pairs(td, L) + 2 * tile_size(td, L) + 8;
+      const long c = tile_pairs(td, L) + 2 * tile_size(td, L) + 40;
       a.rcost.push_back(c);
       a.cost += c;
       P.adj_fma += tile_pairs(td, L);
@@ -283,9 +283,16 @@ TilePlan build_tile_plan(const TableSet &t, int fwarps, int awarps) {
       int cnt = 0;
       for (size_t i = 0; i < parts.size(); ++i) {
         if (own[i] != w) continue;
+        // records per degree of eps (tile side Lout - E): 4 bits each
+        uint32_t cw = 0;
+        for (int r = parts[i].rec0; r < parts[i].rec0 + parts[i].nrec; ++r) {
+          const int E = parts[i].Lout - (int)(P.arec[r] >> 28);
+          if (E < 0 || E > 7 || ((cw >> (4 * E)) & 15u) == 15u) return TilePlan();
+          cw += 1u << (4 * E);
+        }
         P.aunit.push_back(parts[i].Lout | parts[i].split << 8);
         P.aunit.push_back(parts[i].rec0);
-        P.aunit.push_back(parts[i].nrec);
+        P.aunit.push_back((int)cw);
         P.aunit.push_back(parts[i].out);
         ++cnt;
       }

@@ -60,8 +60,10 @@ struct TilePlan {
                                 //   record is the one whose s~ tile holds the origin
   // adjoint: one phase of units, then one of split outputs
   std::vector<int> alist;       // [awarps][2]
-  std::vector<int> aunit;       // [*][4]: Lout | split << 8, first record, records,
-                                //   first output row (full layout) or scratch row
+  std::vector<int> aunit;       // [*][4]: Lout | split << 8, first record, record
+                                //   counts (4 bits per E: records of tile side
+                                //   Lout - E, in that order), first output row
+                                //   (full layout) or scratch row
   std::vector<uint32_t> arec;   // h tile row | Tb tile row << 14 | L << 28
   std::vector<int> afin;        // [*][4]: Lout, first output row, parts, first scratch row
   std::vector<int> aflist;      // [awarps][2] into afin

@@ -163,11 +163,16 @@ static int check(int d0, int k) {
   for (int w = 0; w < P.awarps; ++w) {
     for (int u = P.alist[2 * w]; u < P.alist[2 * w] + P.alist[2 * w + 1]; ++u) {
       const int Lout = P.aunit[4 * u] & 0xff, split = P.aunit[4 * u] >> 8;
-      const int r0 = P.aunit[4 * u + 1], rn = P.aunit[4 * u + 2], out = P.aunit[4 * u + 3];
+      const int r0 = P.aunit[4 * u + 1], out = P.aunit[4 * u + 3];
+      const uint32_t cw = (uint32_t)P.aunit[4 * u + 2];
       const int NT = tile_size(td, Lout);
       std::vector<double> acc(NT, 0.0);
-      for (int r = r0; r < r0 + rn; ++r) {
+      // the kernel's order: for E = 0 .. Lout-1, the unit's records of tile side Lout - E
+      int r = r0;
+      for (int E = 0; E < Lout; ++E)
+      for (int cnt = (cw >> (4 * E)) & 15; cnt > 0; --cnt, ++r) {
         const int hr = P.arec[r] & 0x3fff, tr = (P.arec[r] >> 14) & 0x3fff, L = P.arec[r] >> 28;
+        if (L != Lout - E) { printf("adj record side\n"); return 1; }
         if (L > Lout || hr + tile_size(td, L) > na || tr + tile_size(td, L) > na) { printf("adj rec\n"); return 1; }
         for (int a = 0; a < tile_size(td, L); ++a) {
           int a1, a2;
