@@ -373,39 +373,39 @@ __device__ __forceinline__ void tile_adj(const float *tb, const float *hh,
   AdjRows<TD, 0, NT>::run(tb, hv, acc);
 }
 
-// a unit's records, E = 0 .. LO-1 in turn: (cw >> 4E) & 15 records of tile
-// side LO - E each, so that no record is dispatched at run time
-template <int TD, int LO, int E>
-struct AdjE {
+// Every unit keeps the accumulators of the largest output tile (side LMAX),
+// so that the record code is one body per record tile side, shared by all
+// output tile sides: the units run their records of side LMAX, LMAX - 1,
+// ..., 1 in turn, (cw >> 4 (LO - L)) & 15 of side L (the plan orders them
+// so), where LO is the unit's output tile side.
+constexpr int LMAX = TILE_KMAX + 1;
+template <int TD, int L>
+struct AdjL {
   static __device__ __forceinline__ void run(const float *tbb, const float *hb,
-                                             const uint32_t *rec, int i, uint32_t cw,
-                                             float (&acc)[tsize(TD, LO)]) {
-    const int cnt = (cw >> (4 * E)) & 15u;
+                                             const uint32_t *rec, int i, uint32_t cw, int lo,
+                                             float (&acc)[tsize(TD, LMAX)]) {
+    const int cnt = lo >= L ? (int)((cw >> (4 * (lo - L))) & 15u) : 0;
     for (int k = 0; k < cnt; ++k) {
       const uint32_t r = rec[i + k];
-      tile_adj<TD, LO, LO - E>(tbb + ((r >> 14) & 0x3fffu) * 32, hb + (r & 0x3fffu) * 32, acc);
+      tile_adj<TD, LMAX, L>(tbb + ((r >> 14) & 0x3fffu) * 32, hb + (r & 0x3fffu) * 32, acc);
     }
-    AdjE<TD, LO, E + 1>::run(tbb, hb, rec, i + cnt, cw, acc);
+    AdjL<TD, L - 1>::run(tbb, hb, rec, i + cnt, cw, lo, acc);
   }
 };
-template <int TD, int LO>
-struct AdjE<TD, LO, LO> {
+template <int TD>
+struct AdjL<TD, 0> {
   static __device__ __forceinline__ void run(const float *, const float *, const uint32_t *, int,
-                                             uint32_t, float (&)[tsize(TD, LO)]) {}
+                                             uint32_t, int, float (&)[tsize(TD, LMAX)]) {}
 };
 
-// tbb, hb: this lane's word of the current buffer's Tb rows and h rows
+// the first tsize(TD, LO) accumulators of a unit: into its scratch rows
+// (one part of a split output tile), or scaled by 1/b! and stored
 template <int TD, int LO>
-__device__ __forceinline__ void adj_unit(const float *tbb, const float *hb, const uint32_t *rec,
-                                         int4 u, float *scr, const int *rowslot,
-                                         const float *ifact, float *Sb, int n, bool act,
-                                         double &gb) {
+__device__ __forceinline__ void adj_store(const float (&acc)[tsize(TD, LMAX)], int4 u, float *scr,
+                                          const int *rowslot, const float *ifact, float *Sb,
+                                          int n, bool act, double &gb) {
   constexpr int NT = tsize(TD, LO);
-  float acc[NT];
-#pragma unroll
-  for (int e = 0; e < NT; ++e) acc[e] = 0.f;
-  AdjE<TD, LO, 0>::run(tbb, hb, rec, u.y, (uint32_t)u.z, acc);
-  if (u.x >> 8) {  // one part of a split output tile: into its scratch rows
+  if (u.x >> 8) {
 #pragma unroll
     for (int e = 0; e < NT; ++e) scr[(u.w + e) * 32] = acc[e];
   } else {
@@ -416,6 +416,26 @@ __device__ __forceinline__ void adj_unit(const float *tbb, const float *hb, cons
       if (act) Sb[(size_t)rowslot[row] * n] = v;
       if (row == 0) gb += (double)v;
     }
+  }
+}
+
+// tbb, hb: this lane's word of the current buffer's Tb rows and h rows
+template <int TD>
+__device__ __forceinline__ void adj_unit(const float *tbb, const float *hb, const uint32_t *rec,
+                                         int4 u, float *scr, const int *rowslot,
+                                         const float *ifact, float *Sb, int n, bool act,
+                                         double &gb) {
+  float acc[tsize(TD, LMAX)];
+#pragma unroll
+  for (int e = 0; e < tsize(TD, LMAX); ++e) acc[e] = 0.f;
+  const int lo = u.x & 0xff;
+  AdjL<TD, LMAX>::run(tbb, hb, rec, u.y, (uint32_t)u.z, lo, acc);
+  switch (lo) {
+#define ST10(LL) \
+  case LL: adj_store<TD, LL>(acc, u, scr, rowslot, ifact, Sb, n, act, gb); break;
+    ST10(1) ST10(2) ST10(3) ST10(4) ST10(5) ST10(6) ST10(7) ST10(8)
+#undef ST10
+    default: break;
   }
 }
 
@@ -495,15 +515,7 @@ __global__ void __launch_bounds__(TWA * 32, 1) k_bell_adj10(Adj10Args a) {
     const float *tbb = rb, *hb = rb + na * 32;  // Tb rows, then h rows
     for (int u = u0; u < u0 + un; ++u) {
       const int4 U = sunit[u];
-      switch (U.x & 0xff) {
-#define U10(LL)                                                                   \
-  case LL:                                                                        \
-    adj_unit<TD, LL>(tbb, hb, srec, U, scr, srowslot, sifact, Sb, n, act, gb);    \
-    break;
-        U10(1) U10(2) U10(3) U10(4) U10(5) U10(6) U10(7) U10(8)
-#undef U10
-        default: break;
-      }
+      adj_unit<TD>(tbb, hb, srec, U, scr, srowslot, sifact, Sb, n, act, gb);
     }
     __syncthreads();
     // split output tiles: the parts summed in a fixed order

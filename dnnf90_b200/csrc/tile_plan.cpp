@@ -234,7 +234,11 @@ TilePlan build_tile_plan(const TableSet &t, int fwarps, int awarps) {
   }
   long maxrec = 0;
   for (auto &a : as) maxrec = std::max(maxrec, *std::max_element(a.rcost.begin(), a.rcost.end()));
-  const long cap = std::max(maxrec, (total + awarps - 1) / awarps);
+  // split an output tile when it holds more than a twelfth of the work (at
+  // most: more splits would need more scratch rows than fit beside the two
+  // item buffers)
+  const int ways = std::min(awarps, 12);
+  const long cap = std::max(maxrec, (total + ways - 1) / ways);
   struct Part {
     int Lout, split, rec0, nrec, out;
     long cost;

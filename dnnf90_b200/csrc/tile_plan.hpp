@@ -36,11 +36,10 @@
 
 namespace dnnf90 {
 
-// warps per block of the tiled forward (at most 128 registers each) and of the
-// tiled adjoint (at most 168 registers; 16 warps would split more outputs and
-// the scratch rows would no longer fit beside the two item buffers)
+// warps per block of the tiled forward and of the tiled adjoint (at most 128
+// registers each)
 constexpr int TILE_WARPS_F = 16;
-constexpr int TILE_WARPS_A = 12;
+constexpr int TILE_WARPS_A = 16;
 constexpr int TILE_KMAX = 7;    // longest tile side is K + 1 <= 8
 
 struct TilePlan {
