@@ -1736,8 +1736,8 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
       return RC_OK;
     };
     // variant 3: the register-tiled correlation (bell_tile.cu; FP32, dense
-    // sets).  Every variant that applies is timed; the default is v7 (the
-    // faster at the headline sizes), else the last that applies
+    // sets).  Every variant that applies is timed; the default is the tiled
+    // kernel where it applies, else v7, else the last that applies
     auto launch_t = [&](int v, bool last) -> int {
       if (v == 3)
         return bell_adj_tile(bp.tile, n, npts, Tb, h, Sb, last ? gbias : nullptr, gstride, st);
@@ -1748,7 +1748,7 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
     if (v7_fits) ids.push_back(2);
     if (sizeof(R) == 4 && tile_adj_applies(bp.tile, n)) ids.push_back(3);
     int dflt = (int)ids.size() - 1;
-    if (v7_fits) dflt = srec_fits ? 2 : 1;
+    if (v7_fits && ids.back() != 3) dflt = srec_fits ? 2 : 1;
     return tuned_ids(TuneKey{bp.id, 2, n, (int)sizeof(R)}, ids, dflt, (long)npts * b.gy, st,
                      launch_t);
   }

@@ -62,6 +62,7 @@ __host__ __device__ constexpr int tadd(int td, int e, int c) {
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
+
 __device__ __forceinline__ void cp16(void *dst, const void *src, int src_bytes) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src),
                "r"(src_bytes)
@@ -71,8 +72,10 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Rows of a [na][n] plane slice (neurons j0 .. j0+31) into shared rows
-// perm[r] of dst (128 bytes each); columns at or beyond n read as zero.
-// n is a multiple of 4, so a 16-byte piece is wholly in or out of the row.
+// perm[r] of dst (128 bytes each), 16-byte pieces; columns at or beyond n
+// read as zero.  n is a multiple of 4, so a piece is wholly in or out of the
+// row.  (One 128-byte bulk copy per row measured slower: the rows queue
+// through the SM's bulk-copy unit one request at a time.)
 __device__ __forceinline__ void stage_perm(unsigned char *dst, const float *src, const int *perm,
                                            int na, int n, int j0) {
   for (int c = threadIdx.x; c < na * 8; c += blockDim.x) {
@@ -252,6 +255,7 @@ __global__ void __launch_bounds__(TWF * 32, 1) k_bell_fwd10(Fwd10Args a) {
     // S_0 (0! = 1) and is left alone, since warp 0 reads it next
     {
       unsigned char *sb0 = sm + (buf ? a.o_s1 : 0);
+#pragma unroll 4
       for (int c = threadIdx.x + 8; c < na * 8; c += blockDim.x) {
         float4 *p = (float4 *)(sb0 + c * 16);
         const float f = sifact[c >> 3];
@@ -260,7 +264,22 @@ __global__ void __launch_bounds__(TWF * 32, 1) k_bell_fwd10(Fwd10Args a) {
         *p = v;
       }
     }
-    if (warp == 0) {
+    if (a.iact == 0) {
+      // tanh: warp q forms sigma_q = P_q(tanh S_0) (lib/multi_index_bell_module.f90:
+      // 406-429, the polynomials of sigma_derivs, in the same order), so that no
+      // warp evaluates them all; warps K and K+1 also fill D_K = sigma_K,
+      // E_K = sigma_{K+1} (row 0 of buffer K & 1)
+      if (warp <= K + 1) {
+        const double t = tanh((double)Sb[0]);
+        const double *row = a.tpc + warp * (K + 3);
+        double v = __ldg(row + warp + 1);
+        for (int i = warp; i >= 0; --i) v = v * t + __ldg(row + i);
+        sig[warp * 32] = (float)v;
+        float2 *dk = (float2 *)(sm + ((K & 1) ? a.o_d1 : a.o_d0)) + lane;
+        if (warp == K) dk[0].x = (float)v;
+        if (warp == K + 1) dk[0].y = (float)v;
+      }
+    } else if (warp == 0) {
       double d[TILE_KMAX + 2];
       sigma_derivs(a.iact, a.tpc, K, (double)Sb[0], d);
       float dk0 = 0.f, dk1 = 0.f;
@@ -501,6 +520,7 @@ __global__ void __launch_bounds__(TWA * 32, 1) k_bell_adj10(Adj10Args a) {
     float *rb = (float *)(sm + buf * a.o_b1) + lane;
     {
       unsigned char *b0 = sm + buf * a.o_b1;  // 16 bytes per thread at a time
+#pragma unroll 4
       for (int c = threadIdx.x; c < 2 * na * 8; c += blockDim.x) {
         const int r = c >> 3;
         const float f = r < na ? sfact[r] : sifact[r - na];
@@ -518,18 +538,15 @@ __global__ void __launch_bounds__(TWA * 32, 1) k_bell_adj10(Adj10Args a) {
       adj_unit<TD>(tbb, hb, srec, U, scr, srowslot, sifact, Sb, n, act, gb);
     }
     __syncthreads();
-    // split output tiles: the parts summed in a fixed order
+    // split output tiles: each element's parts summed in a fixed order; the
+    // elements are dealt over all warps
     for (int f = f0; f < f0 + fn; ++f) {
-      const int4 F = sfin[f];
-      const int nt = tsize(TD, F.x);
-      for (int e = 0; e < nt; ++e) {
-        float v = 0.f;
-        for (int p = 0; p < F.z; ++p) v += scr[(F.w + p * nt + e) * 32];
-        const int row = F.y + e;
-        v *= sifact[row];
-        if (act) Sb[(size_t)srowslot[row] * n] = v;
-        if (row == 0) gb += (double)v;
-      }
+      const int4 F = sfin[f];  // row, parts, first scratch row, part stride
+      float v = 0.f;
+      for (int p = 0; p < F.y; ++p) v += scr[(F.z + p * F.w) * 32];
+      v *= sifact[F.x];
+      if (act) Sb[(size_t)srowslot[F.x] * n] = v;
+      if (F.x == 0) gb += (double)v;
     }
     buf ^= 1;
   }

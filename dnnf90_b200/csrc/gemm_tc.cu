@@ -745,12 +745,6 @@ static int sm_count_t() {
   return n;
 }
 
-static int check_flag(int *flag, cudaStream_t st, const char *what) {
-  (void)flag;
-  (void)st;
-  (void)what;
-  return RC_OK;
-}
 
 // cuTensorMapEncodeTiled from the driver the runtime has loaded, looked up
 // once: the library itself does not link libcuda, so it loads (and answers
@@ -924,7 +918,7 @@ int gemm_tc_flag(const DevNet *net, cudaStream_t st) {
     set_error("tensor-core GEMM: an mbarrier wait timed out (code " + std::to_string(h) + ")");
     return RC_DEVICE;
   }
-  return check_flag(w->flag, st, "");
+  return RC_OK;
 }
 
 }  // namespace dnnf90

@@ -302,15 +302,29 @@ TilePlan build_tile_plan(const TableSet &t, int fwarps, int awarps) {
       }
       P.alist[w * 2 + 1] = cnt;
     }
-    // finishing phase: split outputs, round robin
+    // finishing phase: every element of a split output tile is one entry
+    // (its row, parts, first scratch row, part stride), dealt round robin, so
+    // that all warps share the sums
+    std::vector<int> elems;
+    const int ntiles = (int)P.afin.size() / 4;
+    for (int f = 0; f < ntiles; ++f) {
+      const int lo = P.afin[4 * f], out = P.afin[4 * f + 1], np = P.afin[4 * f + 2];
+      const int s0 = P.afin[4 * f + 3], nt = tile_size(td, lo);
+      for (int e = 0; e < nt; ++e) {
+        elems.push_back(out + e);
+        elems.push_back(np);
+        elems.push_back(s0 + e);
+        elems.push_back(nt);
+      }
+    }
     P.aflist.assign((size_t)awarps * 2, 0);
     std::vector<int> fin;
-    const int nfin = (int)P.afin.size() / 4;
+    const int nfin = (int)elems.size() / 4;
     for (int w = 0; w < awarps; ++w) {
       P.aflist[w * 2] = (int)fin.size() / 4;
       int cnt = 0;
       for (int f = w; f < nfin; f += awarps) {
-        fin.insert(fin.end(), P.afin.begin() + 4 * f, P.afin.begin() + 4 * f + 4);
+        fin.insert(fin.end(), elems.begin() + 4 * f, elems.begin() + 4 * f + 4);
         ++cnt;
       }
       P.aflist[w * 2 + 1] = cnt;

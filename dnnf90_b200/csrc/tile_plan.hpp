@@ -64,7 +64,8 @@ struct TilePlan {
                                 //   Lout - E, in that order), first output row
                                 //   (full layout) or scratch row
   std::vector<uint32_t> arec;   // h tile row | Tb tile row << 14 | L << 28
-  std::vector<int> afin;        // [*][4]: Lout, first output row, parts, first scratch row
+  std::vector<int> afin;        // [*][4] per element of a split output tile: its row
+                                //   (full layout), parts, first scratch row, part stride
   std::vector<int> aflist;      // [awarps][2] into afin
   int nscratch = 0;             // scratch rows of the split outputs
   // work model (diagnostic): multiply-adds and shared loads per item

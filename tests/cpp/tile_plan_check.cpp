@@ -195,14 +195,14 @@ static int check(int d0, int k) {
   }
   for (int w = 0; w < P.awarps; ++w)
     for (int f = P.aflist[2 * w]; f < P.aflist[2 * w] + P.aflist[2 * w + 1]; ++f) {
-      const int Lout = P.afin[4 * f], out = P.afin[4 * f + 1], np = P.afin[4 * f + 2], s0 = P.afin[4 * f + 3];
-      const int NT = tile_size(td, Lout);
-      for (int e = 0; e < NT; ++e) {
-        double v = 0;
-        for (int p = 0; p < np; ++p) v += scr[s0 + p * NT + e];
-        const int ib = P.rowslot[out + e];
-        So[ib] = v / fact[ib];
+      const int row = P.afin[4 * f], np = P.afin[4 * f + 1], s0 = P.afin[4 * f + 2], st = P.afin[4 * f + 3];
+      double v = 0;
+      for (int p = 0; p < np; ++p) {
+        if (s0 + p * st >= P.nscratch) { printf("fin scratch\n"); return 1; }
+        v += scr[s0 + p * st];
       }
+      const int ib = P.rowslot[row];
+      So[ib] = v / fact[ib];
     }
   double es = 0, ms = 0;
   for (int ia = 0; ia < na; ++ia) {
