@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(TWF * 32, 1) k_bell_fwd10(Fwd10Args a) {
 // ------------------------------------------------------------ adjoint
 struct Adj10Args {
   int n, na, npts, gy, gstride;
-  int nunit, nrec, nfin;
+  int nunit, nrec, nfin, nscr;
   int o_b1, o_scr, o_list, o_unit, o_rec, o_flist, o_fin, o_perm, o_rowslot, o_fact, o_ifact;
   const int *list;       // [TWA][2]
   const int4 *unit;      // [nunit]: Lout | split << 8, first record, records, out row
@@ -483,7 +483,10 @@ __global__ void __launch_bounds__(TWA * 32, 1) k_bell_adj10(Adj10Args a) {
   copy_words(sfact, a.fact, na);
   copy_words(sifact, a.ifact, na);
   __syncthreads();
-  float *scr = (float *)(sm + a.o_scr) + lane;
+  // two sets of scratch rows: an item's split tiles are summed while the
+  // next item is computed, so no barrier separates the two
+  float *scr0 = (float *)(sm + a.o_scr) + lane;
+  const int scr_words = a.nscr * 32;
   const size_t plane = (size_t)na * n;
   const long nitem = (long)a.npts * a.gy;
   long it0, it1;
@@ -500,18 +503,39 @@ __global__ void __launch_bounds__(TWA * 32, 1) k_bell_adj10(Adj10Args a) {
   cp_commit();
   const int u0 = slist[warp * 2], un = slist[warp * 2 + 1];
   const int f0 = sflist[warp * 2], fn = sflist[warp * 2 + 1];
-  double gb = 0.0;
-  int gj = -1;
+  // the bias gradient: Sb_0 of this lane's neuron summed over the block's
+  // items, added once per neuron tile; gb for the units' outputs, gbp for
+  // the split tiles' (summed one item later)
+  double gb = 0.0, gbp = 0.0;
+  int gj = -1, gjp = -1;
+  auto flush = [&](double &g, int &jj, int jn) {
+    if (jj != jn) {
+      if (a.gbias && jj >= 0 && jj < n && g != 0.0) atomicAdd(a.gbias + (size_t)jj * a.gstride, g);
+      g = 0.0;
+      jj = jn;
+    }
+  };
+  // split output tiles of item itp from scratch set sc: each element's parts
+  // summed in a fixed order, the elements dealt over all warps
+  auto finish = [&](long itp, const float *sc) {
+    const int jp = (int)(itp / a.npts) * 32 + lane;
+    flush(gbp, gjp, jp);
+    float *Sbp = a.Sb + (itp % a.npts) * plane + jp;
+    for (int f = f0; f < f0 + fn; ++f) {
+      const int4 F = sfin[f];  // row, parts, first scratch row, part stride
+      float v = 0.f;
+      for (int p = 0; p < F.y; ++p) v += sc[(F.z + p * F.w) * 32];
+      v *= sifact[F.x];
+      if (jp < n) Sbp[(size_t)srowslot[F.x] * n] = v;
+      if (F.x == 0) gbp += (double)v;
+    }
+  };
   int buf = 0;
   for (long it = it0; it < it1; ++it) {
     const int pt = (int)(it % a.npts);
     const int j = (int)(it / a.npts) * 32 + lane;
     const bool act = j < n;
-    if (j != gj) {
-      if (a.gbias && gj >= 0 && gj < n && gb != 0.0) atomicAdd(a.gbias + (size_t)gj * a.gstride, gb);
-      gb = 0.0;
-      gj = j;
-    }
+    flush(gb, gj, j);
     cp_wait_all();
     __syncthreads();  // this item's rows are in; every warp is done with the last item
     if (it + 1 < it1) stage(buf ^ 1, it + 1);
@@ -530,28 +554,22 @@ __global__ void __launch_bounds__(TWA * 32, 1) k_bell_adj10(Adj10Args a) {
         *p = v;
       }
     }
-    __syncthreads();
+    __syncthreads();  // the rows are scaled; the last item's split parts are in
+    if (it > it0) finish(it - 1, scr0 + ((it - 1 - it0) & 1) * scr_words);
     float *Sb = a.Sb + pt * plane + j;
+    float *scr = scr0 + ((it - it0) & 1) * scr_words;
     const float *tbb = rb, *hb = rb + na * 32;  // Tb rows, then h rows
     for (int u = u0; u < u0 + un; ++u) {
       const int4 U = sunit[u];
       adj_unit<TD>(tbb, hb, srec, U, scr, srowslot, sifact, Sb, n, act, gb);
     }
-    __syncthreads();
-    // split output tiles: each element's parts summed in a fixed order; the
-    // elements are dealt over all warps
-    for (int f = f0; f < f0 + fn; ++f) {
-      const int4 F = sfin[f];  // row, parts, first scratch row, part stride
-      float v = 0.f;
-      for (int p = 0; p < F.y; ++p) v += scr[(F.z + p * F.w) * 32];
-      v *= sifact[F.x];
-      if (act) Sb[(size_t)srowslot[F.x] * n] = v;
-      if (F.x == 0) gb += (double)v;
-    }
     buf ^= 1;
   }
   cp_wait_all();
-  if (a.gbias && gj >= 0 && gj < n && gb != 0.0) atomicAdd(a.gbias + (size_t)gj * a.gstride, gb);
+  __syncthreads();  // the last item's split parts are in
+  if (it0 < it1) finish(it1 - 1, scr0 + ((it1 - 1 - it0) & 1) * scr_words);
+  flush(gb, gj, -1);
+  flush(gbp, gjp, -1);
 }
 
 int grid_for(const void *k, int threads, size_t smem, long items) {
@@ -658,7 +676,7 @@ int upload_tile_plan(const TableSet &t, TileDev &d) {
   d.f_smem = o;
   o = 4 * na * 128;  // two buffers of Tb and h rows
   d.a_o_scr = o;
-  o += std::max(1, P.nscratch) * 128;
+  o += 2 * std::max(1, P.nscratch) * 128;  // two sets of scratch rows
   d.a_o_list = o;
   o += TWA * 2 * 4;
   d.a_o_flist = o;
@@ -722,7 +740,7 @@ int bell_adj_tile(const TileDev &d, int n, int npts, const void *Tb, const void 
   if (!tile_adj_applies(d, n)) return RC_UNSUPPORTED;
   Adj10Args a;
   a.n = n; a.na = d.na; a.npts = npts; a.gy = (n + 31) / 32; a.gstride = gstride;
-  a.nunit = d.naunit; a.nrec = d.narec; a.nfin = d.nafin;
+  a.nunit = d.naunit; a.nrec = d.narec; a.nfin = d.nafin; a.nscr = std::max(1, d.nscratch);
   a.o_b1 = 2 * d.na * 128; a.o_scr = d.a_o_scr; a.o_list = d.a_o_list; a.o_unit = d.a_o_unit;
   a.o_rec = d.a_o_rec; a.o_flist = d.a_o_flist; a.o_fin = d.a_o_fin; a.o_perm = d.a_o_perm;
   a.o_rowslot = d.a_o_rowslot; a.o_fact = d.a_o_fact; a.o_ifact = d.a_o_ifact;

@@ -73,6 +73,11 @@ std::vector<int> lpt(const std::vector<long> &cost, int w) {
 
 }  // namespace
 
+// fixed cost of a unit in the load balance, beside its multiply-adds and
+// loads (its accumulators, its record loop, its output stores)
+static const long ADJ_UNIT_COST = 1000;
+static const long FWD_UNIT_COST = 500;
+
 TilePlan build_tile_plan(const TableSet &t, int fwarps, int awarps) {
   TilePlan P;
   const int d = t.d0, K = t.k;
@@ -181,7 +186,7 @@ TilePlan build_tile_plan(const TableSet &t, int fwarps, int awarps) {
       us.push_back(std::move(u));
     }
     std::vector<long> cost;
-    for (auto &u : us) cost.push_back(u.cost);
+    for (auto &u : us) cost.push_back(u.cost + FWD_UNIT_COST);
     const auto own = lpt(cost, fwarps);
     for (int w = 0; w < fwarps; ++w) {
       P.flist[((size_t)q * fwarps + w) * 2] = (int)P.funit.size() / 4;
@@ -278,8 +283,10 @@ TilePlan build_tile_plan(const TableSet &t, int fwarps, int awarps) {
   P.arec = recs;
   P.nscratch = scratch;
   {
+    // a unit's fixed cost: measured per-warp times at C3 fit about 1000
+    // cycles a unit better than its multiply-adds, which overlap across warps
     std::vector<long> cost;
-    for (auto &p : parts) cost.push_back(p.cost);
+    for (auto &p : parts) cost.push_back(p.cost + ADJ_UNIT_COST);
     const auto own = lpt(cost, awarps);
     P.alist.assign((size_t)awarps * 2, 0);
     for (int w = 0; w < awarps; ++w) {
