@@ -168,6 +168,7 @@ int net_device(NetH &n, cudaStream_t st) {
       for (int l = 2; l <= n.nlayer; ++l) d.woff[l - 1] = layer_off(n, l);
       if ((rc = ck(cudaMalloc(&d.w64, n.w.size() * sizeof(double)), "cudaMalloc"))) return rc;
       if ((rc = ck(cudaMalloc(&d.w32, n.w.size() * sizeof(float)), "cudaMalloc"))) return rc;
+      if ((rc = ck(cudaMalloc(&d.wpk, 2 * n.w.size() * sizeof(double)), "cudaMalloc"))) return rc;
     }
     if ((rc = ck(cudaMemcpyAsync(d.w64, n.w.data(), n.w.size() * sizeof(double),
                                  cudaMemcpyHostToDevice, st), "weights H2D")))

@@ -275,6 +275,8 @@ int upload_tables(const TableSet &t, DevTables &d) {
 
 void DevNet::release() {
   if (w64) cudaFree(w64);
+  if (wpk) cudaFree(wpk);
+  wpk = nullptr;
   if (w32) cudaFree(w32);
   gemm_tc_release_weights(this);
   w64 = nullptr;
@@ -1322,12 +1324,12 @@ static int launch_bell_fwd(const DevTables &t, int n, int npts, const void *S,
 template <typename R>
 static int launch_gemm_cc(int mode, int M, int N, int K, int na, const void *A,
                           int lda, const void *B, int ldb, void *C, int ldc,
-                          double *G, int gld, cudaStream_t st) {
+                          double *G, int gld, cudaStream_t st, double *pack = nullptr) {
   if (sizeof(R) == 8) {
     // FP64 tensor cores (gemm_f64.cu); the CUDA-core tiles below take the
     // shapes it refuses (odd widths)
     const int rc = gemm_f64(mode, M, N, K, na, (const double *)A, lda, (const double *)B, ldb,
-                            (double *)C, ldc, G, gld, st);
+                            (double *)C, ldc, G, gld, st, pack);
     if (rc != RC_UNSUPPORTED) return rc;
   }
   GemmArgs g;
@@ -1489,6 +1491,8 @@ struct Chunk {
   const void *W(int l) const {
     return split() ? (const void *)(net.w32 + net.woff[l - 1]) : (const void *)W64(l);
   }
+  // the plain path's packed operands of layer l (null on the split path)
+  double *pack(int l) const { return split() || !net.wpk ? nullptr : net.wpk + 2 * net.woff[l - 1]; }
 };
 
 // Forward of one chunk: hidden layers, read-out, and (seed != null) the
@@ -1525,7 +1529,7 @@ static int fwd_chunk(Chunk<R> &c, const DevRule *rule, const double *X,
              : RC_UNSUPPORTED;
     if (rc == RC_UNSUPPORTED)
       rc = launch_gemm_cc<R>(G_FWD, M, n, m, na, p.T[l - 2], m, c.W(l), m + 1, p.S, n,
-                             nullptr, 0, c.st);
+                             nullptr, 0, c.st, c.pack(l));
     if (rc) return rc;
     rc = launch_bell_fwd<R>(t, n, np, p.S, p.T[l - 1], p.h[l - 1], train, p, c.st);
     if (rc) return rc;
@@ -1620,7 +1624,7 @@ static int adj_chunk(Chunk<R> &c, const double *X, const double *seed,
                                       : RC_UNSUPPORTED;
     if (rc == RC_UNSUPPORTED)
       rc = launch_gemm_cc<R>(G_DT, M, m, n, na, p.Sb, n, c.W(l), m + 1, p.Tb, m, nullptr,
-                             0, c.st);
+                             0, c.st, c.pack(l) ? c.pack(l) + (size_t)n * m : nullptr);
     if (rc) return rc;
   }
   AdjL2Args a2;

@@ -102,6 +102,9 @@ struct DevNet {
   std::vector<int> dims;
   std::vector<size_t> woff;  // offset of layer l (index l-1) in the flat array
   double *w64 = nullptr;     // flat [layer][j][0..m]
+  double *wpk = nullptr;     // 2 * nw: per layer (at 2 * woff) the plain path's GEMM
+                             // operands without the bias column, [n][m] then [m][n],
+                             // rewritten before each use (gemm_f64.cu)
   float *w32 = nullptr;      // FP32 copy for the split path
   void *tc = nullptr;        // pre-split tensor-core weight operands
   uint64_t uploaded = 0;     // host weight version on the device
