@@ -589,6 +589,315 @@ done:
                  : "memory");
 }
 
+// ---------------------------------------------------------------- DW by TMA
+// G[j][gcol0 + i] += sum_r A[r][j] B[r][i] (A = Sb [K][Mdw], B = T_{l-1}
+// [K][Ndw], FP32), one 128 x 128 output tile per block, the rows split
+// across the grid.  Warp roles:
+//   warp 0      TMA: one 2-D box of 32 rows x up to 128 columns of A and
+//               of B per block of rows into a raw FP32 ring (3 stages)
+//   warps 1-16  converters: split the raw values into three bf16 terms in
+//               the MN-major 128-byte-swizzled layout (2 stages), two
+//               16-byte pieces of each operand per thread
+//   warp 17     MMA: per block two 16-deep steps of the six cross terms of
+//               order <= 2 into an FP32 accumulator in tensor memory (two
+//               buffers of 128 columns)
+//   warps 18-21 epilogue: every 16 blocks (512 rows) the FP32 partial is
+//               added into an FP64 accumulator kept in tensor memory
+//               (columns 256-511, two cells per value), which is added into
+//               G with FP64 atomics at the end
+// Every wait is bounded; one that runs out sets the error flag, and every
+// role then waits (bounded) for its own copies and products in flight.
+constexpr int DW_RB = 32;           // rows per block
+constexpr int DW_NR = 3;            // raw stages
+constexpr int DW_NT = 2;            // term stages
+constexpr int DW_CHUNK = 16;        // blocks per FP32 partial
+constexpr int DW_CONV = 16;         // converter warps
+constexpr int DW_W_MMA = 1 + DW_CONV, DW_W_EPI = DW_W_MMA + 1, DW_WARPS = DW_W_EPI + 4;
+constexpr int DW_NTH = DW_WARPS * 32;
+constexpr uint32_t DW_RAW = 2 * DW_RB * 128 * 4;   // A and B boxes
+constexpr uint32_t DW_TT = DW_RB * 128 * 2;        // one bf16 term of one operand
+constexpr uint32_t DW_TERM = 6 * DW_TT;
+constexpr size_t DW_SMEM = 1024 + DW_NR * DW_RAW + DW_NT * DW_TERM + 256;
+
+struct DwArgs {
+  int Mdw, Ndw, K;       // output rows (A columns), output columns (B columns), rows reduced
+  int bwa, bwb;          // box widths: min(128, Mdw), min(128, Ndw)
+  int kb_per_cta;        // blocks of DW_RB rows per block of the grid
+  double *G;
+  int gld, gcol0;
+  int *flag;
+};
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)),
+               "r"(bytes)
+               : "memory");
+}
+// 2-D tiled TMA load (no multicast) completing on mbarrier b
+__device__ __forceinline__ void tma_load2(void *dst, const CUtensorMap *m, int x, int y,
+                                          uint64_t *b) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, "
+      "{%2, %3}], [%4];" ::"r"(su32(dst)),
+      "l"(m), "r"(x), "r"(y), "r"(su32(b))
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld32u(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld16u(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_st32u(uint32_t taddr, const uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]),
+      "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]),
+      "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+// bounded wait for copies or products still in flight, whatever the flag
+// says (the wait that gives up sets the flag; this one only ends)
+__device__ __forceinline__ void mbar_drain(uint64_t *b, uint32_t par) {
+  for (long it = 0; it < WAIT_LIMIT; ++it) {
+    if (mbar_try(b, par)) return;
+    if (it > 64) __nanosleep(64);
+  }
+}
+// mbar_wait agreed across the warp, for warps whose next steps are
+// warp-collective (tcgen05.ld / st, __syncwarp)
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t *b, uint32_t par, int *flag, int code) {
+  return __all_sync(0xffffffffu, mbar_wait(b, par, flag, code));
+}
+// add 16 FP32 partials p into the 16 FP64 values held as (low, high) word
+// pairs in d (zero first when fresh)
+__device__ __forceinline__ void add16(uint32_t (&d)[32], const uint32_t (&p)[16], bool fresh) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const double x = (fresh ? 0.0 : __hiloint2double((int)d[2 * i + 1], (int)d[2 * i])) +
+                     (double)__uint_as_float(p[i]);
+    d[2 * i] = (uint32_t)__double2loint(x);
+    d[2 * i + 1] = (uint32_t)__double2hiint(x);
+  }
+}
+
+__global__ void __launch_bounds__(DW_NTH, 1)
+    k_tc_dw(DwArgs g, const __grid_constant__ CUtensorMap amap,
+            const __grid_constant__ CUtensorMap bmap) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t *sm = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t *sRaw = sm, *sTerm = sm + DW_NR * DW_RAW;
+  uint64_t *bars = (uint64_t *)(sTerm + DW_NT * DW_TERM);
+  uint64_t *rfull = bars, *rempty = bars + DW_NR, *tfull_s = bars + 2 * DW_NR,
+           *tempty_s = bars + 2 * DW_NR + DW_NT, *afull = bars + 2 * DW_NR + 2 * DW_NT,
+           *aempty = afull + 2, *fin = afull + 4;
+  uint32_t *tmem_hold = (uint32_t *)(fin + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tn = blockIdx.y, tm = blockIdx.z;  // output tile: A columns tm*128.., B columns tn*128..
+  const int nkb_all = (g.K + DW_RB - 1) / DW_RB;
+  const int kb0 = blockIdx.x * g.kb_per_cta;
+  const int nb = max(0, min(nkb_all, kb0 + g.kb_per_cta) - kb0);
+  const int nch = (nb + DW_CHUNK - 1) / DW_CHUNK;
+  const int mnbB = (g.bwb + 63) / 64;
+  int *flag = g.flag;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < DW_NR; ++s) {
+      mbar_init(rfull + s, 1);
+      mbar_init(rempty + s, DW_CONV * 32);
+    }
+    for (int s = 0; s < DW_NT; ++s) {
+      mbar_init(tfull_s + s, DW_CONV * 32);
+      mbar_init(tempty_s + s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(afull + b, 1);
+      mbar_init(aempty + b, 128);
+    }
+    mbar_init(fin, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == DW_W_MMA) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                     su32(tmem_hold))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_hold;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ TMA
+    int issued = 0;
+    if (lane == 0) {
+      const uint32_t bytes = (uint32_t)DW_RB * (g.bwa + g.bwb) * 4;
+      for (int i = 0; i < nb; ++i) {
+        const int s = i % DW_NR;
+        const uint32_t ph = (uint32_t)(i / DW_NR) & 1u;
+        if (!mbar_wait(rempty + s, ph ^ 1u, flag, 11)) break;
+        mbar_expect_tx(rfull + s, bytes);
+        uint8_t *dst = sRaw + s * DW_RAW;
+        const int y = (kb0 + i) * DW_RB;
+        tma_load2(dst, &amap, tm * 128, y, rfull + s);
+        tma_load2(dst + DW_RB * g.bwa * 4, &bmap, tn * 128, y, rfull + s);
+        issued = i + 1;
+      }
+      // the copies still in flight land before the block exits
+      for (int i = max(0, issued - DW_NR); i < issued; ++i)
+        mbar_drain(rfull + i % DW_NR, (uint32_t)(i / DW_NR) & 1u);
+    }
+    __syncwarp();
+  } else if (warp < DW_W_MMA) {
+    // ------------------------------------------------------------ converters
+    // piece e = t + 512 p of an operand: row e / 32, columns 4 (e % 32) ..
+    // + 3 of the box (rows of bw floats), present when they lie inside it
+    const int t = threadIdx.x - 32;  // 0 .. 511
+    static_assert(DW_CONV * 32 * 2 == DW_RB * 32, "two pieces of each operand per thread");
+    for (int i = 0; i < nb; ++i) {
+      const int s = i % DW_NR, ts = i % DW_NT;
+      if (!mbar_wait(rfull + s, (uint32_t)(i / DW_NR) & 1u, flag, 13)) break;
+      if (!mbar_wait(tempty_s + ts, ((uint32_t)(i / DW_NT) & 1u) ^ 1u, flag, 14)) break;
+      const uint8_t *ra = sRaw + s * DW_RAW, *rb = ra + DW_RB * g.bwa * 4;
+      uint8_t *ta = sTerm + ts * DW_TERM, *tb = ta + 3 * DW_TT;
+      float4 xa[2], xb[2];
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        const int e = t + p * DW_CONV * 32, kr = e >> 5, j = (e & 31) * 4;
+        if (j < g.bwa) xa[p] = *(const float4 *)(ra + (kr * g.bwa + j) * 4);
+        if (j < g.bwb) xb[p] = *(const float4 *)(rb + (kr * g.bwb + j) * 4);
+      }
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        const int e = t + p * DW_CONV * 32, kr = e >> 5, j = (e & 31) * 4;
+        uint2 p1, p2, p3;
+        if (j < g.bwa) {
+          split4(xa[p], p1, p2, p3);
+          const uint32_t off = mnmaj_off(j, kr, 2);
+          *(uint2 *)(ta + off) = p1;
+          *(uint2 *)(ta + DW_TT + off) = p2;
+          *(uint2 *)(ta + 2 * DW_TT + off) = p3;
+        }
+        if (j < g.bwb) {
+          split4(xb[p], p1, p2, p3);
+          const uint32_t off = mnmaj_off(j, kr, mnbB);
+          *(uint2 *)(tb + off) = p1;
+          *(uint2 *)(tb + DW_TT + off) = p2;
+          *(uint2 *)(tb + 2 * DW_TT + off) = p3;
+        }
+      }
+      fence_proxy_async();
+      mbar_arrive(tfull_s + ts);
+      mbar_arrive(rempty + s);
+    }
+  } else if (warp == DW_W_MMA) {
+    // ------------------------------------------------------------ MMA issuer
+    const int pa[6] = {2, 1, 0, 1, 0, 0};
+    const int pb[6] = {0, 1, 2, 0, 1, 0};
+    const uint32_t id = idesc(g.bwb, 1, 1);
+    bool any = false;
+    for (int i = 0; i < nb; ++i) {
+      const int ts = i % DW_NT, ic = i % DW_CHUNK, buf = (i / DW_CHUNK) & 1;
+      if (ic == 0 &&
+          !mbar_wait_warp(aempty + buf, ((uint32_t)(i / DW_CHUNK / 2) & 1u) ^ 1u, flag, 15))
+        break;
+      if (!mbar_wait_warp(tfull_s + ts, (uint32_t)(i / DW_NT) & 1u, flag, 16)) break;
+      tc_fence_after();
+      if (lane == 0) {
+        const uint32_t sa = su32(sTerm + ts * DW_TERM), sb = sa + 3 * DW_TT;
+        const uint32_t dcol = tmem + (uint32_t)(buf * 128);
+#pragma unroll
+        for (int ks = 0; ks < DW_RB / 16; ++ks) {
+#pragma unroll
+          for (int p = 0; p < 6; ++p) {
+            // one 16-deep step spans two 8-row k atoms
+            const uint64_t ad = sdesc(sa + pa[p] * DW_TT + ks * 2 * (2 * 1024), 1024, 2 * 1024);
+            const uint64_t bd =
+                sdesc(sb + pb[p] * DW_TT + ks * 2 * (mnbB * 1024), 1024, mnbB * 1024);
+            mma(dcol, ad, bd, id, (ic | ks | p) ? 1u : 0u);
+          }
+        }
+        mma_commit(tempty_s + ts);
+        if (ic == DW_CHUNK - 1 || i + 1 == nb) mma_commit(afull + buf);
+      }
+      any = true;
+      __syncwarp();
+    }
+    // the products in flight complete before the block exits
+    if (any) {
+      if (lane == 0) mma_commit(fin);
+      __syncwarp();
+      mbar_drain(fin, 0u);
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3;          // tensor-memory lane quadrant of this warp
+    const int row = q * 32 + lane;   // accumulator row
+    const uint32_t la = tmem + ((uint32_t)(q * 32) << 16);
+    const int ncol = g.bwb;  // a multiple of 16
+    int ch = 0;
+    for (; ch < nch; ++ch) {
+      const int buf = ch & 1;
+      if (!mbar_wait_warp(afull + buf, (uint32_t)(ch / 2) & 1u, flag, 18)) break;
+      tc_fence_after();
+      for (int c0 = 0; c0 < ncol; c0 += 16) {
+        uint32_t p[16], d[32];
+        tmem_ld16u(la + (uint32_t)(buf * 128 + c0), p);
+        if (ch) tmem_ld32u(la + (uint32_t)(256 + 2 * c0), d);
+        tmem_wait_ld();
+        add16(d, p, ch == 0);
+        tmem_st32u(la + (uint32_t)(256 + 2 * c0), d);
+      }
+      tmem_wait_st();
+      tc_fence_before();
+      mbar_arrive(aempty + buf);
+    }
+    const int gr = tm * 128 + row;
+    if (ch == nch && nch > 0) {  // warp-uniform: the loads are warp-collective
+      const bool mine = row < g.bwa && gr < g.Mdw;
+      double *dst = g.G + (size_t)(mine ? gr : 0) * g.gld + g.gcol0 + tn * 128;
+      const int nval = mine ? min(g.bwb, g.Ndw - tn * 128) : 0;
+      for (int c0 = 0; c0 < ncol; c0 += 16) {
+        uint32_t d[32];
+        tmem_ld32u(la + (uint32_t)(256 + 2 * c0), d);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (c0 + i < nval)
+            atomicAdd(dst + c0 + i, __hiloint2double((int)d[2 * i + 1], (int)d[2 * i]));
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == DW_W_MMA)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
 // host-side split of one FP32 value into three bf16 terms (round to nearest
 // even, as __float2bfloat16_rn)
 static uint16_t bf16_rn(float f) {
@@ -844,26 +1153,70 @@ int gemm_tc_dt(const DevNet *net, int l, int M, int n, int m, const void *Sb, vo
                   w->flag, st);
 }
 
+// tensor map of an FP32 operand P[rows][cols] (row stride ld floats):
+// boxes of DW_RB rows x bw columns, no swizzle, zeros past the edges
+static int f32_box_map(CUtensorMap *m, const float *P, int rows, int cols, int ld, int bw) {
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)tc::DW_RB};
+  const cuuint32_t estr[2] = {1, 1};
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is not available from the CUDA driver");
+    return RC_DEVICE;
+  }
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)P, dims, strides, box,
+                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed for a weight-gradient operand (code " +
+              std::to_string((int)r) + ")");
+    return RC_DEVICE;
+  }
+  return RC_OK;
+}
+
+// G[j][gcol0 + i] += sum_r A[r][j] B[r][i], A [K][Mdw] (row stride lda), B
+// [K][Ndw] (ldb): k_tc_dw over one wave of blocks, each an output tile of
+// 128 x 128 and a contiguous run of rows.  Widths are multiples of 16 and
+// the leading dimensions multiples of 4 (16-byte rows for TMA).
+static int dw_tma(const float *A, int Mdw, int lda, const float *B, int Ndw, int ldb, int K,
+                  double *G, int gld, int gcol0, int *flag, cudaStream_t st) {
+  if (Mdw < 16 || Ndw < 16 || Mdw % 16 || Ndw % 16 || lda % 4 || ldb % 4 || lda < Mdw ||
+      ldb < Ndw || ((uintptr_t)A & 15) || ((uintptr_t)B & 15) || K < 1)
+    return RC_UNSUPPORTED;
+  const int ntm = (Mdw + 127) / 128, ntn = (Ndw + 127) / 128;
+  if (ntm > 65535 || ntn > 65535) return RC_UNSUPPORTED;
+  const int nkb_all = (K + tc::DW_RB - 1) / tc::DW_RB;
+  const long tiles = (long)ntm * ntn;
+  const int ctas_k =
+      (int)std::max<long>(1, std::min<long>(nkb_all, std::max<long>(1, grid_sms() / tiles)));
+  tc::DwArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.Mdw = Mdw; a.Ndw = Ndw; a.K = K;
+  a.bwa = std::min(128, Mdw); a.bwb = std::min(128, Ndw);
+  a.kb_per_cta = (nkb_all + ctas_k - 1) / ctas_k;
+  a.G = G; a.gld = gld; a.gcol0 = gcol0; a.flag = flag;
+  CUtensorMap amap, bmap;
+  std::memset(&amap, 0, sizeof amap);
+  std::memset(&bmap, 0, sizeof bmap);
+  int rc = f32_box_map(&amap, A, K, Mdw, lda, a.bwa);
+  if (!rc) rc = f32_box_map(&bmap, B, K, Ndw, ldb, a.bwb);
+  if (rc) return rc;
+  const dim3 grid((nkb_all + a.kb_per_cta - 1) / a.kb_per_cta, ntn, ntm);
+  CKT(cudaFuncSetAttribute(tc::k_tc_dw, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)tc::DW_SMEM));
+  LAUNCH("k_tc_gemm_dw", st, tc::k_tc_dw<<<grid, tc::DW_NTH, tc::DW_SMEM, st>>>(a, amap, bmap));
+  CKT(cudaGetLastError());
+  return RC_OK;
+}
+
 int gemm_tc_dw(const DevNet *net, int l, int M, int n, int m, const void *Sb, const void *Tm,
                double *G, cudaStream_t st) {
+  (void)l;
   TcWeights *w = (TcWeights *)net->tc;
-  if (!w || n % 16 || m % 16) return RC_UNSUPPORTED;
-  const int BN = 64;
-  const int ntn = (m + BN - 1) / BN, ntm = (n + tc::BM - 1) / tc::BM;  // output tiles
-  if (ntm > 65535) return RC_UNSUPPORTED;
-  const int nkb_all = (M + tc::BK - 1) / tc::BK;
-  const int ctas_k = std::max(1, std::min(nkb_all, grid_sms() / (ntn * ntm)));
-  tc::Args a;
-  std::memset(&a, 0, sizeof a);
-  a.mode = tc::MODE_DW; a.M = n; a.N = m; a.K = M; a.na = 1;
-  a.A = (const float *)Sb; a.lda = n; a.B = (const float *)Tm; a.ldb = m;
-  a.G = G; a.gld = m + 1; a.gcol0 = 1; a.BN = BN; a.ntn = ntn; a.kchunk = 8;
-  a.kblocks_per_cta = (nkb_all + ctas_k - 1) / ctas_k;
-  a.flag = w->flag;
-  const size_t stage = 3 * (8 * 2 * 1024) + 3 * (8 * 1 * 1024);
-  const size_t smem = 1024 + 3 * stage + 1024;
-  dim3 grid((nkb_all + a.kblocks_per_cta - 1) / a.kblocks_per_cta, ntn, ntm);
-  return launch(a, tc::MODE_DW, grid, smem, st);
+  if (!w) return RC_UNSUPPORTED;
+  return dw_tma((const float *)Sb, n, n, (const float *)Tm, m, m, M, G, m + 1, 1, w->flag, st);
 }
 
 // G[i][j] += sum_r J[r][i] J[r][j] over an FP32 copy J[nrow][ldj] (ldj a
