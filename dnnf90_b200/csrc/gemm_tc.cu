@@ -1,6 +1,6 @@
 // gemm_tc.cu - split-BF16 layer GEMMs on the tcgen05 tensor cores.
 //
-// One persistent kernel, warp-specialised (FWD/DT 672 threads, DW 416):
+// One persistent kernel, warp-specialised (FWD/DT 800 threads, DW 416):
 //   producers  warps 0-15 (FWD/DT; 0-7 for DW): read FP32 operand rows from
 //              HBM (coalesced 16-byte loads; FWD/DT keep the next two K
 //              blocks in flight in registers), split every value x into three bf16 terms
@@ -12,7 +12,9 @@
 //              a3b1, a2b2, a1b3, a2b1, a1b2, a1b1, smallest first, into an
 //              accumulator in tensor memory (two buffers, so the epilogue of
 //              one tile overlaps the products of the next)
-//   epilogue   4 warps after the producers: tcgen05.ld of the accumulator (lane = row), bias
+//   epilogue   the warps after the producers (FWD/DT 8, two per tensor-memory
+//              lane quadrant taking alternate 32-column boxes; DW 4):
+//              tcgen05.ld of the accumulator (lane = row), bias
 //              on the alpha = 0 rows, FP32 store; or, for the weight
 //              gradient, FP32 partials of 512 rows added into FP64
 //              registers and reduced to HBM with FP64 atomics
@@ -60,9 +62,10 @@ constexpr int MODE_FWD = 0, MODE_DT = 1, MODE_DW = 2;
 template <int MODE>
 struct Roles {
   static constexpr int PW = MODE == MODE_DW ? 8 : 16;  // producer warps
+  static constexpr int EW = MODE == MODE_DW ? 4 : 8;   // epilogue warps
   static constexpr int NPROD = PW * 32;
-  static constexpr int MMA = PW + 4;
-  static constexpr int NT = (PW + 5) * 32;
+  static constexpr int MMA = PW + EW;
+  static constexpr int NT = (PW + EW + 1) * 32;
 };
 constexpr int BM = 128;       // rows per tile (MMA M)
 constexpr int BK = 64;        // K per block: one 128-byte bf16 swizzle row
@@ -210,7 +213,7 @@ struct Args {
 // FWD/DT epilogue staging: per epilogue warp one 32 x 32 FP32 box, rows of
 // 128 bytes with the 16-byte pieces in the 128-byte swizzle the tensor map
 // of C names, stored to HBM by one TMA bulk tensor store per box
-constexpr int STG_BYTES = 4 * 32 * 32 * 4;
+constexpr int STG_BYTES = 8 * 32 * 32 * 4;
 
 template <int MODE>
 __global__ void __launch_bounds__(Roles<MODE>::NT, 1)
@@ -263,7 +266,7 @@ __global__ void __launch_bounds__(Roles<MODE>::NT, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(tfull + b, 1);
-      mbar_init(tempty + b, 128);
+      mbar_init(tempty + b, Roles<MODE>::EW * 32);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -517,8 +520,10 @@ __global__ void __launch_bounds__(Roles<MODE>::NT, 1)
         const int gr = mt * BM + row;
         const bool ok = gr < g.M;
         const bool brow = (MODE == MODE_FWD) && ok && (gr % g.na == 0);
-        uint8_t *stg = sStg + q * (32 * 32 * 4);
-        for (int c0 = 0; c0 < BN; c0 += 32) {
+        // the two warps of a lane quadrant take alternate 32-column boxes,
+        // each through its own staging box
+        uint8_t *stg = sStg + (warp - NPROD_WARPS) * (32 * 32 * 4);
+        for (int c0 = 32 * ((warp - NPROD_WARPS) >> 2); c0 < BN; c0 += 64) {
           float v[32];
           tmem_ld32(lane_addr + (uint32_t)(buf * BN + c0), v);
           if (brow) {
