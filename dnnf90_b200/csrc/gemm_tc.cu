@@ -92,12 +92,15 @@ __device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t par) {
       : "memory");
   return ok != 0;
 }
-// bounded wait; false (and the error flag set) when the limit runs out
+// bounded wait; false (and the error flag set) when the limit runs out.
+// The flag (a global read, an L2 round trip) is looked at once every 64
+// polls, and the thread backs off only after 1024: a hand-off is seen
+// within one try_wait of its phase completing.
 __device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t par, int *flag, int code) {
   for (long it = 0; it < WAIT_LIMIT; ++it) {
     if (mbar_try(b, par)) return true;
-    if (*(volatile int *)flag) return false;
-    if (it > 64) __nanosleep(32);
+    if ((it & 63) == 63 && *(volatile int *)flag) return false;
+    if (it > 1024) __nanosleep(32);
   }
   atomicCAS(flag, 0, code);
   return false;
