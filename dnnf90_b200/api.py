@@ -50,7 +50,7 @@ EXTENSION_SYMBOLS = [
     "dnnf90_kf_update_rows_dev", "dnnf90_kf_read", "dnnf90_kf_iekf_begin",
     "dnnf90_kf_iekf_iter", "dnnf90_ngd_gram_dev", "dnnf90_ngd_solve_dev",
     "dnnf90_ngd_step_dual_dev", "dnnf90_kf_pass", "dnnf90_kf_pass_iekf", "dnnf90_kf_pass_sys",
-    "dnnf90_kf_status",
+    "dnnf90_kf_status", "dnnf90_keep_fits",
 ]
 
 _lib = None
@@ -124,6 +124,7 @@ def lib():
         "dnnf90_grad_rule_dev": [i, i, i, p, i, p, p, p, p],
         "dnnf90_jrow_dev": [i, i, i, p, i, p, p, p],
         "dnnf90_twork_set_chunk": [i, i],
+        "dnnf90_keep_fits": [i, i, i, pi],
         "dnnf90_last_error": [],
         "dnnf90_device_available": [],
         "dnnf90_launch_count": [],

@@ -10,10 +10,15 @@ so no torch op sees them.  dL/dx is not formed (None).
 
 Two memory modes: ``keep=True`` keeps every plane of the forward on the
 device for the backward (store mode); ``keep=False`` recomputes the forward
-inside the backward (recompute mode), the choice for large K and carried
-sets, where the planes of all layers do not fit.
+inside the backward, chunk by chunk (recompute mode).  ``keep=None`` (the
+default) chooses: store mode when every layer's planes for all the points
+fit the work space's budget (``dnnf90_keep_fits``: their size follows from
+|A|, that is from D0 and K, the widths and the point count), recompute mode
+otherwise -- the case of large K and carried sets.
 """
 from __future__ import annotations
+
+import ctypes
 
 import torch
 
@@ -28,15 +33,25 @@ def _stream():
     return torch.cuda.current_stream().cuda_stream
 
 
+def keep_fits(net: "api.Net", npts: int) -> bool:
+    """Whether a store-mode forward of npts points fits net's work space."""
+    fits = ctypes.c_int(0)
+    api.call("dnnf90_keep_fits", net.nid, net.tid, npts, ctypes.byref(fits))
+    return fits.value == 1
+
+
 class HodFunction(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, x: torch.Tensor, w: torch.Tensor, net: "api.Net", keep: bool):
+    def forward(ctx, x: torch.Tensor, w: torch.Tensor, net: "api.Net", keep):
         if not (x.is_cuda and w.is_cuda):
             raise ValueError("HodFunction runs on CUDA tensors only")
         x = x.detach().to(torch.float64).contiguous()
         w = w.detach().to(torch.float64).contiguous()
         api.call("dnnf90_set_weights_dev", net.nid, _ptr(w), _stream())
         npts = x.shape[0]
+        if keep is None:
+            keep = keep_fits(net, npts)
+        ctx.keep = bool(keep)
         tm = torch.empty((npts, net.na, net.nout), dtype=torch.float64, device=x.device)
         api.call("dnnf90_forward_dev", net.nid, net.tid, npts, _ptr(x), _ptr(tm),
                  1 if keep else 0, _stream())
@@ -58,6 +73,8 @@ class HodFunction(torch.autograd.Function):
         return None, g.to(w.dtype), None, None
 
 
-def hod(x: torch.Tensor, w: torch.Tensor, net: "api.Net", keep: bool = True):
-    """Carried derivatives T[npts][nout][na] with an analytic adjoint in w."""
+def hod(x: torch.Tensor, w: torch.Tensor, net: "api.Net", keep=None):
+    """Carried derivatives T[npts][nout][na] with an analytic adjoint in w.
+    keep: True (store mode), False (recompute mode) or None (store mode when
+    it fits, see keep_fits)."""
     return HodFunction.apply(x, w, net, keep)

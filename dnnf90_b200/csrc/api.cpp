@@ -204,17 +204,25 @@ size_t plane_bytes_per_point(const NetH &n) {
   return per;
 }
 
-int work_planes(WorkH &w, NetH &n, int want, bool exact) {
+// points whose planes (every layer's T and h, the S / Sb / Tb scratch, the
+// seeds and outputs: plane_bytes_per_point, so set by |A| = f(D0, K) and
+// the widths) one chunk of work space w holds: at most 48 GiB, and at most
+// half of what is free with this work space's own planes counted as free
+// (so the cap does not grow by re-counting them on every call), and at most
+// the chunk set by dnnf90_twork_set_chunk
+int plane_cap(const WorkH &w, const NetH &n) {
   const size_t per = plane_bytes_per_point(n);
-  // at most 48 GiB, and at most half of what is free with this work
-  // space's own planes counted as free (so the cap does not grow by
-  // re-counting them on every call)
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
   const size_t avail = freeb + (w.p.base ? w.p.bytes : 0);
   const size_t budget = std::min<size_t>((size_t)48 << 30, avail / 2);
-  int cap = (int)std::max<size_t>(1, budget / per);
+  int cap = (int)std::min<size_t>(std::max<size_t>(1, budget / per), (size_t)INT32_MAX);
   if (w.chunk > 0) cap = std::min(cap, w.chunk);
+  return cap;
+}
+
+int work_planes(WorkH &w, NetH &n, int want, bool exact) {
+  const int cap = plane_cap(w, n);
   int need = std::min(want, cap);
   if (exact && want > cap) {
     set_error("the kept forward does not fit the device memory budget");
@@ -1244,6 +1252,16 @@ int dnnf90_forward_dev(int nid, int tid, int npts, const double *x_dev, double *
   BatchArgs a;
   a.npts = npts; a.X = x_dev; a.out = tm_dev; a.prec = n.prec;
   return dev_finish(n, st, run_batch(n.dt, n.dn, none, w.p, a, st));
+}
+
+int dnnf90_keep_fits(int nid, int tid, int npts, int *fits) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int rc = check_train(nid, tid, 0, false);
+  if (rc) return rc;
+  if (npts < 0 || !fits) return RC_BAD_ARG;
+  if ((rc = device_ready())) return rc;
+  *fits = npts <= plane_cap(g_twk[tid], g_net[nid]) ? 1 : 0;
+  return RC_OK;
 }
 
 int dnnf90_backward_dev(int nid, int tid, int npts, const double *x_dev,

@@ -209,6 +209,13 @@ int dnnf90_set_weights_dev(int nid, const double *w_dev, void *stream);
  * keeps every plane on work space tid for dnnf90_backward_dev. */
 int dnnf90_forward_dev(int nid, int tid, int npts, const double *x_dev,
                        double *tm_dev, int keep, void *stream);
+/* *fits = 1 when a keep=1 forward of npts points fits work space tid: every
+ * layer's planes for all the points (their size follows from |A|, that is
+ * from D0 and K, and the widths) within the work space's budget, the
+ * smaller of 48 GiB and half of the free device memory, and within its
+ * chunk (dnnf90_twork_set_chunk); 0 otherwise, when the backward recomputes
+ * the forward chunk by chunk instead. */
+int dnnf90_keep_fits(int nid, int tid, int npts, int *fits);
 /* adjoint from seedm_dev[npts][nout][na], added to grad_dev[nweights].  Uses
  * the planes kept by the last keep=1 forward of the same points and
  * weights on tid; otherwise recomputes the forward first. */

@@ -91,6 +91,26 @@ def test_keep_and_recompute_agree():
     net.free()
 
 
+def test_automatic_memory_mode():
+    """keep=None keeps the planes when every layer's planes for the points
+    fit the work space (here: 4096 points of this net, about 40 MB), and
+    recomputes when they do not (a 1000-point chunk; 10^9 points); both give
+    the store-mode gradient."""
+    from dnnf90_b200.autograd import keep_fits
+    X, w = _points(4096, 5), _weights()
+    ts, net, slots = _setup(api.PREC_F64)
+    assert keep_fits(net, 4096)
+    assert not keep_fits(net, 10 ** 9)
+    L1, g1, _ = _loss_and_grad(net, slots, X, w, keep=True)
+    L2, g2, _ = _loss_and_grad(net, slots, X, w, keep=None)
+    assert L1 == L2 and rel_err(g2, g1) < 1e-14
+    api.call("dnnf90_twork_set_chunk", net.tid, 1000)
+    assert not keep_fits(net, 4096)
+    L3, g3, _ = _loss_and_grad(net, slots, X, w, keep=None)
+    assert abs(L3 - L1) <= 1e-13 * abs(L1) and rel_err(g3, g1) < 1e-13
+    net.free()
+
+
 def test_finite_differences_of_the_full_loss():
     """Central differences of L along random unit directions (the
     directional form of the reference's Hod_check)."""
