@@ -37,6 +37,7 @@ baseline.
 from __future__ import annotations
 
 import argparse
+import collections
 import json
 import os
 import statistics
@@ -295,6 +296,23 @@ def committee_members(nnet=64):
         npts = int(np.exp(rng.uniform(np.log(1000.0), np.log(64000.0))))
         out.append((d0, k, width, depth, rng.uniform(-1.0, 1.0, (npts, d0)), 1000 + i))
     return out
+
+
+def autotuner_summary(api):
+    """The Bell kernels' autotuner choices, keyed on (kernel, D0, K, |A|,
+    width, precision): the ZK7 shapes by name, the others (the committee's
+    members) as counts per (kernel, precision, variant)."""
+    zk7, other = [], collections.Counter()
+    rows = api.tune_report()
+    for kern, d0, k, na, width, prec, chosen, _ in rows:
+        names = api.ADJ_VARIANTS if kern == "bell_adj" else api.FWD_VARIANTS
+        name = names.get(chosen, str(chosen))
+        if (d0, k, na, width) == (D0, K, 330, DIMS[1]):
+            zk7.append(f"{kern} {prec}: {name}")
+        else:
+            other[f"{kern} {prec} {name}"] += 1
+    return {"key": "(kernel, D0, K, |A|, width, precision)", "shapes": len(rows),
+            "zk7": sorted(zk7), "others": dict(sorted(other.items()))}
 
 
 def committee_bench(api, dev, nsteps, nnet=64):
@@ -1052,6 +1070,7 @@ def main():
             "cpu_baseline": cpu,
             "kernel_ms_per_step": {"split": per_step_ms(prof), "f64": per_step_ms(prof64)},
             "committee": committee,
+            "autotuner": autotuner_summary(api),
         }
         print(json.dumps(line), flush=True)
     rule.free()

@@ -197,16 +197,23 @@ def profile_enable(on: bool = True):
     lib().dnnf90_profile_enable(1 if on else 0)
 
 
+# names of the Bell kernel variants by id (the forward's, the adjoint's)
+FWD_VARIANTS = {0: "v5-global", 1: "v5-shared", 2: "v8", 3: "tiled"}
+ADJ_VARIANTS = {0: "v5-global", 1: "v5-shared", 2: "v7", 3: "tiled"}
+
+
 def tune_report() -> list:
-    """The Bell kernels' autotuner choices: (kernel, width, precision,
-    chosen variant, [trial ms per variant])."""
+    """The Bell kernels' autotuner choices, one per tuned launch shape:
+    (kernel, d0, k, |A|, width, precision, chosen variant id, [trial ms per
+    variant])."""
     n = lib().dnnf90_tune_report(None, 0)
     buf = ctypes.create_string_buffer(n + 64)
     lib().dnnf90_tune_report(buf, len(buf))
     out = []
     for line in buf.value.decode().splitlines():
         f = line.split()
-        out.append((f[0], int(f[1]), f[2], int(f[3]), [float(v) for v in f[4:]]))
+        out.append((f[0], int(f[1]), int(f[2]), int(f[3]), int(f[4]), f[5], int(f[6]),
+                    [float(v) for v in f[7:]]))
     return out
 
 

@@ -1432,6 +1432,7 @@ static int persistent_grid(const void *k, int threads, size_t smem, long items) 
 struct TuneKey {
   uint64_t plan;
   int which, n, prec;
+  int d0 = 0, k = 0, na = 0;  // the plan's table set, for the report only
   bool operator<(const TuneKey &o) const {
     return std::tie(plan, which, n, prec) < std::tie(o.plan, o.which, o.n, o.prec);
   }
@@ -1441,7 +1442,8 @@ static std::map<TuneKey, std::vector<float>> g_tune_ms;  // timed trial per vari
 static std::map<TuneKey, std::vector<int>> g_tune_id;   // variant ids of the trials
 static std::mutex g_tune_mu;
 
-// "kernel width prec chosen ms0 ms1 ..." lines, one per tuned launch shape
+// "kernel d0 k na width prec chosen ms0 ms1 ..." lines, one per tuned
+// launch shape (the chosen variant's id, then the trial time of each)
 std::string tune_report() {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   static const char *names[] = {"bell_fwd", "bell_fwd_train", "bell_adj"};
@@ -1452,8 +1454,9 @@ std::string tune_report() {
     const int chosen = ids != g_tune_id.end() && kv.second < (int)ids->second.size()
                            ? ids->second[kv.second]
                            : kv.second;
-    std::snprintf(b, sizeof b, "%s %d %s %d", names[kv.first.which], kv.first.n,
-                  kv.first.prec == 8 ? "f64" : "f32", chosen);
+    std::snprintf(b, sizeof b, "%s %d %d %d %d %s %d", names[kv.first.which], kv.first.d0,
+                  kv.first.k, kv.first.na, kv.first.n, kv.first.prec == 8 ? "f64" : "f32",
+                  chosen);
     out += b;
     auto it = g_tune_ms.find(kv.first);
     if (it != g_tune_ms.end())
@@ -1625,7 +1628,8 @@ static int fwd5_dispatch(const DevBellPlan &bp, const DevTables &t, int n, int n
   if (srec_fits) ids.push_back(1);
   if (v8_ok) ids.push_back(2);
   if (tile_ok) ids.push_back(3);
-  return tuned_ids(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R)}, ids, (int)ids.size() - 1,
+  return tuned_ids(TuneKey{bp.id, train ? 1 : 0, n, (int)sizeof(R), t.d0, t.k, t.na}, ids,
+                   (int)ids.size() - 1,
                    (long)npts * a.gy, st, launch);
 }
 
@@ -1749,7 +1753,8 @@ static int adj2_t(const DevBellPlan &bp, const DevTables &t, int n, int npts, co
     if (sizeof(R) == 4 && tile_adj_applies(bp.tile, n)) ids.push_back(3);
     int dflt = (int)ids.size() - 1;
     if (v7_fits && ids.back() != 3) dflt = srec_fits ? 2 : 1;
-    return tuned_ids(TuneKey{bp.id, 2, n, (int)sizeof(R)}, ids, dflt, (long)npts * b.gy, st,
+    return tuned_ids(TuneKey{bp.id, 2, n, (int)sizeof(R), t.d0, t.k, t.na}, ids, dflt,
+                     (long)npts * b.gy, st,
                      launch_t);
   }
   Adj2Args a;

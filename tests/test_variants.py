@@ -105,3 +105,28 @@ def test_series_forward_agrees_with_the_bell_recurrence(pinned, prec):
         r.free(); g.free(); net.free()
     tol = 1e-13 if prec == api.PREC_F64 else 1e-5
     assert rel_err(out[1][0], out[0][0]) < tol and rel_err(out[1][1], out[0][1]) < tol
+
+
+@pytest.mark.gpu
+def test_autotuner_report_names_the_launch_shape():
+    """Unpinned, a launch with several waves of work (2048 points x 4 neuron
+    tiles) is tuned once: the report names its kernel, table set (D0, K,
+    |A|), width and precision, the chosen variant is one of the variants'
+    ids, and every trial was timed."""
+    ts = api.TableSet(4, 7)
+    dims = [4, 128, 128, 1]
+    w = xavier_weights(dims, 3)
+    X = np.random.default_rng(3).uniform(-1, 1, (2048, 4))
+    net = api.Net(ts, dims, weights=w, precision=api.PREC_SPLIT)
+    g = net.grad()
+    rule = api.SeedRule(api.SEED_HALFSQ)
+    g.rule_batch(X, rule)
+    rows = [r for r in api.tune_report() if r[1:6] == (4, 7, 330, 128, "f32")]
+    assert {"bell_fwd_train", "bell_adj"} <= {r[0] for r in rows}, rows
+    for kern, _, _, _, _, _, chosen, trials in rows:
+        names = api.ADJ_VARIANTS if kern == "bell_adj" else api.FWD_VARIANTS
+        assert chosen in names
+        assert len(trials) >= 2 and all(t > 0 for t in trials)
+    rule.free()
+    g.free()
+    net.free()
