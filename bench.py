@@ -298,10 +298,11 @@ def committee_members(nnet=64):
     return out
 
 
-def autotuner_summary(api):
+def autotuner_summary(api, pinned=None):
     """The Bell kernels' autotuner choices, keyed on (kernel, D0, K, |A|,
     width, precision): the ZK7 shapes by name, the others (the committee's
-    members) as counts per (kernel, precision, variant)."""
+    members) as counts per (kernel, precision, variant).  Launches under
+    --pin-variants are not tuned (pinned names the pin)."""
     zk7, other = [], collections.Counter()
     rows = api.tune_report()
     for kern, d0, k, na, width, prec, chosen, _ in rows:
@@ -311,8 +312,11 @@ def autotuner_summary(api):
             zk7.append(f"{kern} {prec}: {name}")
         else:
             other[f"{kern} {prec} {name}"] += 1
-    return {"key": "(kernel, D0, K, |A|, width, precision)", "shapes": len(rows),
-            "zk7": sorted(zk7), "others": dict(sorted(other.items()))}
+    out = {"key": "(kernel, D0, K, |A|, width, precision)", "shapes": len(rows),
+           "zk7": sorted(zk7), "others": dict(sorted(other.items()))}
+    if pinned:
+        out["pinned"] = pinned
+    return out
 
 
 def committee_bench(api, dev, nsteps, nnet=64):
@@ -1070,7 +1074,7 @@ def main():
             "cpu_baseline": cpu,
             "kernel_ms_per_step": {"split": per_step_ms(prof), "f64": per_step_ms(prof64)},
             "committee": committee,
-            "autotuner": autotuner_summary(api),
+            "autotuner": autotuner_summary(api, args.pin_variants),
         }
         print(json.dumps(line), flush=True)
     rule.free()
