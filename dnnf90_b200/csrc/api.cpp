@@ -201,6 +201,7 @@ size_t plane_bytes_per_point(const NetH &n) {
   for (int l = 2; l < n.nlayer; ++l) per += 2 * (size_t)n.ts.na * n.dims[l - 1] * rsz;
   per += 3 * (size_t)n.ts.na * nmax * rsz;
   per += 2 * (size_t)n.ts.na * n.dims[n.nlayer - 1] * 8 + n.ts.d0 * 8 + 1024;
+  per += (size_t)(n.ts.k + 2) * n.dims[1] * rsz;  // the first layer's s^(q)
   return per;
 }
 

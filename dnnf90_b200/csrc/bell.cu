@@ -1785,11 +1785,19 @@ int bell_adj2(const DevBellPlan &bp, const DevTables &t, int n, int npts, const 
 struct AdjL2sArgs {
   int n, na, npts, gy;
   const int *up;           // [na][D0]: slot of g + e_i | (g_i + 1) << 16, or -1
-  const void *Tb, *h;      // [P][na][n]
+  const void *Tb, *h;      // [P][na][n] (h unused when h is formed in the kernel)
   const double *X;         // [P][D0]
   double *g;               // dW_2 [n][D0 + 1], accumulated (null in row mode)
   double *rows;            // [P][nw] (row mode)
   size_t nw, woff;
+  // h formed in the kernel (graded slots): the layer's weights [n][D0 + 1],
+  // s^(q)(S^0) [P][k + 2][n] kept by the forward, the order, the first slot
+  // of each degree and a - e_i | i << 16 per slot (k_layer2v's monomials)
+  const double *W;
+  const void *sig;
+  const int *par;
+  int k;
+  int ds[KMAX + 2];
 };
 
 // The first hidden layer's Bell adjoint fused with dW_2 (the k_adj_l2v sums)
@@ -1802,13 +1810,26 @@ struct AdjL2sArgs {
 // in once per tile; only the per-point rows (Jacobian mode) are summed over
 // the warps per item.  Every Tb row is read from HBM once instead of D0 + 1
 // times through the caches.
-template <typename R, int D0, int NPB>
+// AN: the first layer is analytic (S^0 = W x + b, S^{e_i} = W_i), so
+// h^g = s^(|g|+1)(S^0) W^g, formed here exactly as k_layer2v forms it (the
+// monomial W^g = prod_i W_i^{g_i} in R, built once per neuron tile along
+// unit steps; the s^(q) the forward kept, rounded to R, times it): no h
+// plane is written by the forward nor read here, only k + 2 rows of s^(q)
+// per item beside its Tb rows.  A warp's slots come in graded order, so it
+// steps its multiplier at each degree boundary.  (Summing each degree with
+// W^g and multiplying by s^(p+1) once was measured slower: the degree runs
+// are short, 1 to 4 slots per warp.)
+template <typename R, int D0, int NPB, bool AN>
 __global__ void __launch_bounds__(1024) k_adj_l2s(AdjL2sArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char *sm = smem_raw;
   const int na = a.na, n = a.n;
-  const uint32_t bsz = 2u * na * 128;  // one buffer: Tb rows, then h rows
-  const uint32_t upoff = 2 * bsz, redoff = upoff + ((uint32_t)na * D0 * 8 + 127) / 128 * 128;
+  // one buffer: Tb rows, then h rows (AN: the k + 2 rows of s^(q))
+  const uint32_t bsz = (AN ? (uint32_t)(na + KMAX + 2) : 2u * na) * 128;
+  // AN: the tile's monomials [na] rows, the degree starts
+  const uint32_t moff = 2 * bsz, dsoff = moff + (AN ? (uint32_t)na * 128 : 0u);
+  const uint32_t upoff = dsoff + (AN ? 128u : 0u);
+  const uint32_t redoff = upoff + ((uint32_t)na * D0 * 8 + 127) / 128 * 128;
   // (byte offset of the Tb row of g + e_i, multiplier g_i + 1) per (g, i);
   // a missing child reads row 0 with multiplier 0
   uint2 *up = (uint2 *)(sm + upoff);
@@ -1829,10 +1850,39 @@ __global__ void __launch_bounds__(1024) k_adj_l2s(AdjL2sArgs a) {
     const size_t pofs = (size_t)(it % a.npts) * plane;
     const int j0 = (int)(it / a.npts) * NPB;
     stage_rows<NPB, R>(sm + dst, (const R *)a.Tb + pofs, na, n, j0, 1024);
-    stage_rows<NPB, R>(sm + dst + na * 128, (const R *)a.h + pofs, na, n, j0, 1024);
+    if (AN)
+      stage_rows<NPB, R>(sm + dst + na * 128,
+                         (const R *)a.sig + (size_t)(it % a.npts) * (a.k + 2) * n, a.k + 2, n,
+                         j0, 1024);
+    else
+      stage_rows<NPB, R>(sm + dst + na * 128, (const R *)a.h + pofs, na, n, j0, 1024);
   };
   if (it0 < it1) stage(it0, 0);
   cp_async_commit();
+  // AN: the monomials W^g of tile tl's neurons (every thread; barriers inside)
+  const int *sds = (const int *)(sm + dsoff);
+  auto build_m = [&](int tl) {
+    const int j = tl * NPB + ln;
+    const double *wr = a.W + (size_t)(j < n ? j : n - 1) * (D0 + 1);
+    if (warp == 0 && lact) srow<R>(sm, moff + lo) = (R)1;
+    __syncthreads();
+    for (int p = 1; p <= a.k; ++p) {
+      for (int ia = sds[p] + warp; ia < sds[p + 1]; ia += 32) {
+        const int pk = __ldg(a.par + ia);
+        if (lact)
+          srow<R>(sm, moff + ia * 128 + lo) =
+              (R)((double)srow<R>(sm, moff + (pk & 0xffff) * 128 + lo) * wr[1 + (pk >> 16)]);
+      }
+      __syncthreads();
+    }
+  };
+  int mtile = -1;
+  if (AN && it0 < it1) {
+    if (threadIdx.x < KMAX + 2) ((int *)(sm + dsoff))[threadIdx.x] = a.ds[threadIdx.x];
+    __syncthreads();
+    mtile = (int)(it0 / a.npts);
+    build_m(mtile);
+  }
   double acc[D0 + 1];
 #pragma unroll
   for (int o = 0; o <= D0; ++o) acc[o] = 0.0;
@@ -1860,17 +1910,42 @@ __global__ void __launch_bounds__(1024) k_adj_l2s(AdjL2sArgs a) {
       flush(tile);
       tile = tl;
     }
+    if (AN && tl != mtile) {  // block-uniform: every warp is past the last item
+      build_m(tl);
+      mtile = tl;
+    }
     const uint32_t tb = buf + lo, hb = tb + na * 128;
     R s[D0 + 1];
 #pragma unroll
     for (int o = 0; o <= D0; ++o) s[o] = (R)0;
-    for (int g = warp; g < na; g += 32) {
-      const R hg = srow<R>(sm, hb + g * 128);
-      s[0] += srow<R>(sm, tb + g * 128) * hg;
+    if (AN) {
+      // h^g = (R)s^(p+1) * W^g, p = |g|: the slots of a warp rise in degree,
+      // so its multiplier steps at each degree boundary
+      int p = 0, pend = sds[1];
+      R dq = srow<R>(sm, hb + 128);  // this item's s^(1) row
+      for (int g = warp; g < na; g += 32) {
+        while (g >= pend) {
+          ++p;
+          pend = sds[p + 1];
+          dq = srow<R>(sm, hb + (p + 1) * 128);
+        }
+        const R hg = dq * srow<R>(sm, moff + g * 128 + lo);
+        s[0] += srow<R>(sm, tb + g * 128) * hg;
 #pragma unroll
-      for (int i = 0; i < D0; ++i) {
-        const uint2 u = up[g * D0 + i];
-        s[1 + i] += (R)__uint_as_float(u.y) * srow<R>(sm, tb + u.x) * hg;
+        for (int i = 0; i < D0; ++i) {
+          const uint2 u = up[g * D0 + i];
+          s[1 + i] += (R)__uint_as_float(u.y) * srow<R>(sm, tb + u.x) * hg;
+        }
+      }
+    } else {
+      for (int g = warp; g < na; g += 32) {
+        const R hg = srow<R>(sm, hb + g * 128);
+        s[0] += srow<R>(sm, tb + g * 128) * hg;
+#pragma unroll
+        for (int i = 0; i < D0; ++i) {
+          const uint2 u = up[g * D0 + i];
+          s[1 + i] += (R)__uint_as_float(u.y) * srow<R>(sm, tb + u.x) * hg;
+        }
       }
     }
     const double *x = a.X + (size_t)pt * D0;
@@ -1903,15 +1978,30 @@ __global__ void __launch_bounds__(1024) k_adj_l2s(AdjL2sArgs a) {
   if (it0 < it1) flush(tile);
 }
 
+// shared memory of k_adj_l2s: two item buffers (Tb rows, then h rows, or
+// with h formed in the kernel the item's s^(q) rows), then (an) the
+// monomials and the degree starts, the (g, i) table and the per-warp row sums
+static size_t l2s_smem(int na, int d0, bool an) {
+  return (an ? (size_t)2 * (na + KMAX + 2) * 128 + (size_t)na * 128 + 128
+             : (size_t)4 * na * 128) +
+         ((size_t)na * d0 * 8 + 127) / 128 * 128 + (size_t)32 * (d0 + 1) * 128;
+}
+
+bool bell_adj_l2s_analytic(int d0, int na, int n, int prec) {
+  const int rsz = prec == PREC_F64 ? 8 : 4;
+  return d0 >= 1 && d0 <= 8 && na <= 65535 && n % (16 / rsz) == 0 &&
+         l2s_smem(na, d0, true) <= 227 * 1024;
+}
+
 template <typename R, int D0>
 static int adj_l2s_k(const AdjL2sArgs &a, cudaStream_t st) {
   constexpr int NPB = sizeof(R) == 8 ? 16 : 32;
-  const size_t smem = 4 * (size_t)a.na * 128 + ((size_t)a.na * D0 * 8 + 127) / 128 * 128 +
-                      (size_t)32 * (D0 + 1) * 128;
+  const bool an = a.W != nullptr;
+  const size_t smem = l2s_smem(a.na, D0, an);
   if (smem > 227 * 1024 || a.na > 65535 || a.n % (16 / (int)sizeof(R))) return RC_UNSUPPORTED;
   AdjL2sArgs b = a;
   b.gy = (a.n + NPB - 1) / NPB;
-  auto k = k_adj_l2s<R, D0, NPB>;
+  auto k = an ? k_adj_l2s<R, D0, NPB, true> : k_adj_l2s<R, D0, NPB, false>;
   CKB(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = persistent_grid((const void *)k, 1024, smem, (long)a.npts * b.gy);
   LAUNCH("k_bell_adj_l2", st, k<<<grid, 1024, smem, st>>>(b));
@@ -1936,11 +2026,18 @@ static int adj_l2s_t(int d0, const AdjL2sArgs &a, cudaStream_t st) {
 
 int bell_adj_l2s(int d0, int n, int na, int npts, const int *up, const void *Tb, const void *h,
                  const double *X, double *g, double *rows, size_t nw, size_t woff, int prec,
-                 cudaStream_t st) {
+                 cudaStream_t st, const L2Analytic *an) {
   if (npts <= 0) return RC_OK;
   AdjL2sArgs a;
   a.n = n; a.na = na; a.npts = npts; a.gy = 0; a.up = up; a.Tb = Tb; a.h = h; a.X = X;
   a.g = g; a.rows = rows; a.nw = nw; a.woff = woff;
+  a.W = nullptr; a.sig = nullptr; a.par = nullptr; a.k = 0;
+  for (int p = 0; p < KMAX + 2; ++p) a.ds[p] = na;
+  if (an) {
+    if (an->k < 1 || an->k > KMAX) return RC_UNSUPPORTED;
+    a.W = an->W; a.sig = an->sig; a.par = an->par; a.k = an->k;
+    for (int p = 0; p <= an->k + 1; ++p) a.ds[p] = an->dstart[p];
+  }
   return prec == PREC_F64 ? adj_l2s_t<double>(d0, a, st) : adj_l2s_t<float>(d0, a, st);
 }
 

@@ -114,10 +114,23 @@ int bell_fwd_tile(const TileDev &d, const DevTables &t, int n, int npts, const v
                   void *h, bool train, cudaStream_t st);
 int bell_adj_tile(const TileDev &d, int n, int npts, const void *Tb, const void *h, void *Sb,
                   double *gbias, int gstride, cudaStream_t st);
+// The first hidden layer is analytic: h^g = s^(|g|+1)(S^0) W^g.  With these
+// inputs the adjoint forms h itself (graded slots) from the s^(q) the
+// forward kept, and reads no h plane.
+struct L2Analytic {
+  const double *W;         // the layer's weights [n][d0 + 1]
+  const void *sig;         // [P][k + 2][n]: s^(q)(S^0), kept by the forward
+  const int *par;          // [na]: slot of g - e_i | i << 16 (the monomial recurrence)
+  int k;
+  const int *dstart;       // host [k + 2]: first slot of each degree
+};
+// whether the adjoint can form h itself for these sizes (its shared memory)
+bool bell_adj_l2s_analytic(int d0, int na, int n, int prec);
 // the first hidden layer's adjoint fused with dW_2, staged through shared
-// memory (RC_UNSUPPORTED when an item's rows do not fit)
+// memory (RC_UNSUPPORTED when an item's rows do not fit); an: h formed in
+// the kernel (null: read from the h plane)
 int bell_adj_l2s(int d0, int n, int na, int npts, const int *up, const void *Tb, const void *h,
                  const double *X, double *g, double *rows, size_t nw, size_t woff, int prec,
-                 cudaStream_t st);
+                 cudaStream_t st, const L2Analytic *an = nullptr);
 
 }  // namespace dnnf90

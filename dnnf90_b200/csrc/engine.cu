@@ -716,6 +716,7 @@ struct L2vArgs {
   const double *X;         // [P][d0]
   const double *W;         // [n][d0 + 1]
   void *T, *h;             // [P][na][n]
+  void *sig;               // [P][KK + 2][n]: s^(q)(S^0) (null: not kept)
 };
 
 // First hidden layer, analytic (see k_layer2): T^a = s^(|a|) W^a with the
@@ -747,6 +748,11 @@ __global__ void __launch_bounds__(256) k_layer2v(L2vArgs a) {
     sigma_derivs(a.iact, a.tpc, KK, s, d);
     R *T = (R *)a.T + pt * plane + j;
     R *H = TRAIN ? (R *)a.h + pt * plane + j : nullptr;
+    if (a.sig && act) {
+      R *G = (R *)a.sig + (size_t)pt * (KK + 2) * a.n + j;
+#pragma unroll
+      for (int q = 0; q <= KK + 1; ++q) G[(size_t)q * a.n] = (R)d[q];
+    }
 #pragma unroll
     for (int p = 0; p <= KK; ++p) {
       const R dp = (R)d[p], dq = (R)d[p + 1];
@@ -1246,6 +1252,7 @@ int ensure_planes(const DevTables &t, const DevNet &net, int prec, int cap_pts,
   size_t oSb = take(P * na * nmax * rsz);
   size_t oTb = take(P * na * nmax * rsz);
   size_t oSeed = take(P * na * net.dims[L - 1] * sizeof(double));
+  size_t oSig = take(P * (size_t)(t.k + 2) * net.dims[1] * rsz);
   size_t oX = take(P * t.d0 * sizeof(double));
   size_t oOut = take(P * na * net.dims[L - 1] * sizeof(double));
   size_t oLoss = take(sizeof(double) * 4);
@@ -1266,6 +1273,7 @@ int ensure_planes(const DevTables &t, const DevNet &net, int prec, int cap_pts,
   p.Sb = b + oSb;
   p.Tb = b + oTb;
   p.seed = b + oSeed;
+  p.sig = b + oSig;
   p.X = (double *)(b + oX);
   p.out = (double *)(b + oOut);
   p.loss = (double *)(b + oLoss);
@@ -1383,15 +1391,26 @@ static int layer2v_k(const L2vArgs &a, bool train, cudaStream_t st) {
   return RC_OK;
 }
 
+// whether the first hidden layer runs analytically in both directions:
+// k_layer2v forms T (and h would be s^(|g|+1) W^g), and the first-layer
+// adjoint forms h itself, so a training forward writes no h plane for it.
+// The forward and every adjoint of the same table set and width agree.
+template <typename R>
+static bool l2_analytic(const DevTables &t, int n) {
+  return t.graded && t.k >= 1 && t.k <= 8 && (size_t)t.na * 32 * sizeof(R) <= 200 * 1024 &&
+         (int)t.dstart.size() >= t.k + 2 &&
+         bell_adj_l2s_analytic(t.d0, t.na, n, sizeof(R) == 8 ? PREC_F64 : PREC_SPLIT);
+}
+
 // streaming first hidden layer; RC_UNSUPPORTED when the shape is outside it
 template <typename R>
 static int launch_layer2v(const DevTables &t, int n, int npts, const double *X, const double *W,
-                          void *T, void *h, bool train, cudaStream_t st) {
+                          void *T, void *h, bool train, cudaStream_t st, void *sig = nullptr) {
   if (!t.graded || t.k > 8 || (size_t)t.na * 32 * sizeof(R) > 200 * 1024) return RC_UNSUPPORTED;
   L2vArgs a;
   a.n = n; a.na = t.na; a.d0 = t.d0; a.npts = npts; a.iact = t.iact;
   for (int p = 0; p < KMAX + 2; ++p) a.ds[p] = p <= t.k + 1 ? t.dstart[std::min(p, t.k + 1)] : t.na;
-  a.par = t.l2par; a.tpc = t.tpc; a.X = X; a.W = W; a.T = T; a.h = h;
+  a.par = t.l2par; a.tpc = t.tpc; a.X = X; a.W = W; a.T = T; a.h = h; a.sig = sig;
   switch (t.k) {
     case 1: return layer2v_k<R, 1>(a, train, st);
     case 2: return layer2v_k<R, 2>(a, train, st);
@@ -1511,7 +1530,11 @@ static int fwd_chunk(Chunk<R> &c, const DevRule *rule, const double *X,
     l2.n = net.dims[1]; l2.na = na; l2.d0 = t.d0; l2.k = t.k; l2.iact = t.iact;
     l2.npts = np; l2.alpha = t.alpha; l2.deg = t.deg; l2.tpc = t.tpc; l2.X = X;
     l2.W = c.W64(2); l2.T = p.T[1]; l2.h = p.h[1];
-    rc = launch_layer2v<R>(t, l2.n, np, X, l2.W, l2.T, l2.h, train, c.st);
+    // the analytic adjoint forms the first layer's h itself from s^(q),
+    // which the forward keeps instead of the h plane
+    const bool an = train && l2_analytic<R>(t, l2.n);
+    rc = launch_layer2v<R>(t, l2.n, np, X, l2.W, l2.T, l2.h, train && !an, c.st,
+                           an ? p.sig : nullptr);
     if (rc == RC_UNSUPPORTED) {
       dim3 grid(std::min(np, smc * 8), (l2.n + 127) / 128);
       if (train) { LAUNCH("k_layer2", c.st, k_layer2<R, true><<<grid, 128, 0, c.st>>>(l2)); }
@@ -1634,8 +1657,15 @@ static int adj_chunk(Chunk<R> &c, const double *X, const double *seed,
   a2.Tb = p.Tb; a2.h = p.h[1]; a2.X = X;
   a2.g = rows || !grad ? nullptr : grad + net.woff[1];
   a2.rows = rows; a2.nw = net.nw; a2.woff = net.woff[1];
+  L2Analytic an{c.W64(2), p.sig, t.l2par, t.k, t.dstart.data()};
   rc = bell_adj_l2s(t.d0, a2.n, na, np, t.l2up, p.Tb, p.h[1], X, a2.g, rows, net.nw,
-                    net.woff[1], split ? PREC_SPLIT : PREC_F64, c.st);
+                    net.woff[1], split ? PREC_SPLIT : PREC_F64, c.st,
+                    l2_analytic<R>(t, a2.n) ? &an : nullptr);
+  if (rc == RC_UNSUPPORTED && l2_analytic<R>(t, a2.n)) {
+    // the forward wrote no h plane for this layer, so no other kernel may run
+    set_error("first-layer adjoint: the analytic kernel refused a shape it was chosen for");
+    return RC_DEVICE;
+  }
   if (rc != RC_UNSUPPORTED) return rc;
   {
     AdjL2vArgs v;

@@ -119,6 +119,7 @@ struct Planes {
   void *base = nullptr;      // one allocation, carved below
   std::vector<void *> T, h;  // per layer (index l-1), hidden layers only
   void *S = nullptr, *Sb = nullptr, *Tb = nullptr, *seed = nullptr;
+  void *sig = nullptr;       // [P][k + 2][n_1]: s^(q)(S^0) of the first hidden layer
   void *scratch = nullptr;   // Bell state spill when it does not fit smem
   size_t scratch_bytes = 0;
   double *X = nullptr;       // [P][d0] staged inputs
