@@ -313,7 +313,7 @@ def autotuner_summary(api, pinned=None):
         else:
             other[f"{kern} {prec} {name}"] += 1
     out = {"key": "(kernel, D0, K, |A|, width, precision)", "shapes": len(rows),
-           "zk7": sorted(zk7), "others": dict(sorted(other.items()))}
+           "zk7": sorted(set(zk7)), "others": dict(sorted(other.items()))}
     if pinned:
         out["pinned"] = pinned
     return out
