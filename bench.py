@@ -1061,7 +1061,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "fp32 planes, 3-term split-bf16 GEMMs (fp32 acc), fp64 sigma/reductions",
             "data": "synthetic (seeded points, Xavier-normal weights)",
-            # the north-star comparison: split path against the plain FP64
+            # the headline comparison: split path against the plain FP64
             # GPU path on the same points, and the split path's error
             "split_vs_f64": {"speedup": r3(value / value64), "target": 4.0,
                              "f64_value": r3(value64), "f64_ms_per_step": r3(ms64)},
