@@ -63,3 +63,34 @@ def test_kalman_reference_arm_prints_the_contract_line():
         assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["value"] == line["value"]
         assert ("decoupled" in line["metric"]) == bool(extra)
         assert "EKF" in line["config"]["workload"]
+
+
+def test_autotuner_summary_of_the_report():
+    """The bench line's autotuner field from the library's report rows
+    (kernel, D0, K, |A|, width, precision, chosen id, trial times): the ZK7
+    shapes by variant name without repeats, the others counted, a pin named."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from dnnf90_b200 import api
+
+    rows = [("bell_adj", 4, 7, 330, 128, "f32", 3, [1.0, 0.5]),
+            ("bell_adj", 4, 7, 330, 128, "f32", 3, [1.0, 0.5]),   # a second ZK7 net
+            ("bell_fwd_train", 4, 7, 330, 128, "f64", 2, [2.0, 1.0]),
+            ("bell_fwd_train", 3, 4, 35, 256, "f32", 2, [1.0, 2.0]),
+            ("bell_adj", 3, 4, 35, 256, "f32", 1, [1.0, 0.9]),
+            ("bell_adj", 2, 5, 21, 64, "f32", 1, [1.0, 0.9])]
+
+    class Stub:
+        FWD_VARIANTS = api.FWD_VARIANTS
+        ADJ_VARIANTS = api.ADJ_VARIANTS
+
+        @staticmethod
+        def tune_report():
+            return rows
+
+    out = bench.autotuner_summary(Stub)
+    assert out["shapes"] == 6
+    assert out["zk7"] == ["bell_adj f32: tiled", "bell_fwd_train f64: v8"]
+    assert out["others"] == {"bell_adj f32 v5-shared": 2, "bell_fwd_train f32 v8": 1}
+    assert "pinned" not in out
+    assert bench.autotuner_summary(Stub, "3,3")["pinned"] == "3,3"
