@@ -165,6 +165,11 @@ def test_no_device_fails_loudly():
         api.call("dnnf90_ngd_solve_dev", net.nw, 1, 1, 1, 1e-3, 1, None)
     assert e.value.rc == -3
     # argument checks come first
+    fits = ctypes.c_int(7)
+    assert api.lib().dnnf90_keep_fits(net.nid, net.tid, -1, ctypes.byref(fits)) == -1
+    assert api.lib().dnnf90_keep_fits(net.nid, net.tid, 10, None) == -1
+    assert api.lib().dnnf90_keep_fits(net.nid, net.tid, 10, ctypes.byref(fits)) == -3
+    assert fits.value == 7
     assert api.lib().dnnf90_kf_create(net.nid, 0.0, 0.98, 0.99, 0, 0.0, 0.0) == -1
     assert api.lib().dnnf90_kf_update_rows(1, 1, None, None, None) == -1
     net.free()
