@@ -249,9 +249,9 @@ int dnnf90_twork_set_chunk(int tid, int npts);
 int dnnf90_committee_step(int nnet, const int *nids, const int *tids, const int *rids,
                           const int *npts, const double *const *x_dev,
                           double *const *grad_dev, double *loss_dev, void *stream);
-/* the Bell kernels' autotuner: one line per tuned launch shape, "kernel
- * width precision chosen-variant ms-of-each-variant"; returns the length
- * (buf may be NULL); new */
+/* the Bell kernels' autotuner: one line per tuned launch shape, "kernel d0
+ * k na width precision chosen-variant ms-of-each-variant" (the table set's
+ * D0, K and |A|); returns the length (buf may be NULL); new */
 int dnnf90_tune_report(char *buf, int len);
 /* pin the variant of the Bell forward (which 0: 0 records in global memory,
  * 1 records in shared memory, 2 per-degree loops over 16-bit offset records)
