@@ -1,6 +1,10 @@
 // gemm_tc.cu - split-BF16 layer GEMMs on the tcgen05 tensor cores.
 //
-// One persistent kernel, warp-specialised (FWD/DT 800 threads, DW 416):
+// Two kernels: k_tc_gemm for the products with the weights (FWD, DT) and the
+// natural-gradient metric J^T J (its DW mode, gemm_tc_syrk), and k_tc_dw, the
+// layers' weight gradient, fed by TMA (further below).
+//
+// k_tc_gemm: one persistent kernel, warp-specialised (FWD/DT 800 threads, DW 416):
 //   producers  warps 0-15 (FWD/DT; 0-7 for DW): read FP32 operand rows from
 //              HBM (coalesced 16-byte loads; FWD/DT keep the next two K
 //              blocks in flight in registers), split every value x into three bf16 terms
@@ -27,8 +31,8 @@
 //   FWD  S[M][N]  = A[M][K] W^T  (+ bias[N] on rows r % na == 0),
 //        A = T_{l-1} plane (K-major), W pre-split and pre-swizzled
 //   DT   Tb[M][N] = A[M][K] W    (A = Sb plane, K = n, N = m)
-//   DW   G[j][1+i] += sum_r A[r][j] B[r][i]  (A = Sb, B = T_{l-1}, both
-//        MN-major tiles, K = rows split across blocks)
+//   DW   G[j][1+i] += sum_r A[r][j] B[r][i]  (both MN-major tiles, K = rows
+//        split across blocks): the metric J^T J (A = B = J)
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
