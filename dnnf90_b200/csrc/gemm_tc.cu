@@ -645,7 +645,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
                "r"(bytes)
                : "memory");
 }
-// 2-D tiled TMA load (no multicast) completing on mbarrier b
+// 2-D tiled TMA load into this block's own shared memory, completing on mbarrier b
 __device__ __forceinline__ void tma_load2(void *dst, const CUtensorMap *m, int x, int y,
                                           uint64_t *b) {
   asm volatile(
